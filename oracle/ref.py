@@ -1,0 +1,137 @@
+"""ctypes access to the reference's own compiled operators (oracle/_ref).
+
+TEST INFRASTRUCTURE ONLY (see oracle/restate.py).  The library is built from
+the reference sources by oracle/build_ref.sh; this module never builds it.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import tempfile
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_ref", "libmidapack_ref.so")
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise FileNotFoundError(f"{LIB_PATH} not built (run oracle/build_ref.sh)")
+        _lib = ct.CDLL(LIB_PATH)
+    return _lib
+
+
+def _p(a, ctype):
+    return a.ctypes.data_as(ct.POINTER(ctype))
+
+
+I32 = ct.c_int
+F64 = ct.c_double
+
+
+def local_shape(gindices: np.ndarray, m: int, nnz: int):
+    idx = np.ascontiguousarray(gindices, dtype=np.int32).copy()
+    vals = np.zeros(m * nnz)
+    cap = idx.size
+    lind = np.zeros(cap, dtype=np.int32)
+    trash = ct.c_int(0)
+    lc = lib().ref_local_shape(m, nnz, _p(idx, I32), _p(vals, F64), _p(lind, I32), cap, ct.byref(trash))
+    return idx, lind[:lc].copy(), trash.value
+
+
+def matvec(gindices, values, x, m, nnz=3):
+    idx = np.ascontiguousarray(gindices, dtype=np.int32).copy()
+    v = np.ascontiguousarray(values, dtype=np.float64).copy()
+    xx = np.ascontiguousarray(x, dtype=np.float64).copy()
+    y = np.zeros(m)
+    lib().ref_matvec(m, nnz, _p(idx, I32), _p(v, F64), _p(xx, F64), _p(y, F64))
+    return y
+
+
+def trmatvec(gindices, values, y, m, n, nnz=3):
+    idx = np.ascontiguousarray(gindices, dtype=np.int32).copy()
+    v = np.ascontiguousarray(values, dtype=np.float64).copy()
+    yy = np.ascontiguousarray(y, dtype=np.float64).copy()
+    x = np.zeros(max(n, 1))
+    lib().ref_trmatvec(m, nnz, _p(idx, I32), _p(v, F64), _p(yy, F64), _p(x, F64))
+    return x[:n]
+
+
+def stbmm(V, block_sizes, lam, invtt):
+    bs = np.ascontiguousarray(block_sizes, dtype=np.int32).copy()
+    tt = np.ascontiguousarray(invtt, dtype=np.float64).copy()
+    out = np.ascontiguousarray(V, dtype=np.float64).copy()
+    lib().ref_stbmm(len(bs), _p(bs, I32), lam, _p(tt, F64), _p(out, F64))
+    return out
+
+
+def pcg(gindices, values, signal, noise, block_sizes, lam, invtt, tol=1e-8, maxiter=500, nnz=3):
+    """Single-rank MLmap set-up + PCG_GLS_true. Returns (x, lstid, cond, hits, res_rel)."""
+    m = len(signal)
+    idx = np.ascontiguousarray(gindices, dtype=np.int32).copy()
+    v = np.ascontiguousarray(values, dtype=np.float64).copy()
+    sig = np.ascontiguousarray(signal, dtype=np.float64).copy()
+    noi = np.ascontiguousarray(noise, dtype=np.float64).copy()
+    bs = np.ascontiguousarray(block_sizes, dtype=np.int32).copy()
+    tt = np.ascontiguousarray(invtt, dtype=np.float64).copy()
+    cap = int(np.unique(idx).size)
+    x = np.zeros(cap)
+    lstid = np.zeros(cap, dtype=np.int32)
+    cond = np.zeros(cap // 3 + 1)
+    hits = np.zeros(cap // 3 + 1, dtype=np.int32)
+    with tempfile.TemporaryDirectory() as td:
+        n = lib().ref_pcg(m, nnz, _p(idx, I32), _p(v, F64), _p(sig, F64), _p(noi, F64), len(bs), _p(bs, I32), lam,
+                          _p(tt, F64), F64(tol), maxiter, td.encode(), b"oracle", _p(x, F64), _p(lstid, I32),
+                          _p(cond, F64), _p(hits, I32), cap)
+        res = np.fromfile(os.path.join(td, "pcg_residuals_oracle.dat"), dtype=np.float64)
+    return x[:n].copy(), lstid[:n].copy(), cond[:n // 3].copy(), hits[:n // 3].copy(), res
+
+
+def mlmap(nranks, data_size_proc, nb_blocks_proc, block_sizes, pix, weights, signal, noise, lam, invtt, nside,
+          tol=1e-8, maxiter=500, nnz=3):
+    """MLmap on `nranks` forked ranks; returns the I, Q, U, Cond, Hits maps."""
+    dsp = np.ascontiguousarray(data_size_proc, dtype=np.int32)
+    nbp = np.ascontiguousarray(nb_blocks_proc, dtype=np.int32)
+    bs = np.ascontiguousarray(block_sizes, dtype=np.int32)
+    px = np.ascontiguousarray(pix, dtype=np.int32)
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    s = np.ascontiguousarray(signal, dtype=np.float64)
+    nz = np.ascontiguousarray(noise, dtype=np.float64)
+    tt = np.ascontiguousarray(invtt, dtype=np.float64)
+    with tempfile.TemporaryDirectory() as td:
+        rc = lib().ref_mlmap(nranks, td.encode(), b"oracle", F64(tol), maxiter, nside, nnz, lam, _p(dsp, I32),
+                             _p(nbp, I32), _p(bs, I32), _p(px, I32), _p(w, F64), _p(s, F64), _p(nz, F64),
+                             _p(tt, F64))
+        if rc != 0:
+            raise RuntimeError(f"reference MLmap failed (status {rc})")
+        rd = lambda name, dt: np.fromfile(os.path.join(td, f"{name}_oracle.fits"), dtype=dt)  # noqa: E731
+        out = (rd("mapI", np.float64), rd("mapQ", np.float64), rd("mapU", np.float64), rd("Cond", np.float64),
+               rd("Hits", np.int32))
+        res = np.fromfile(os.path.join(td, "pcg_residuals_oracle.dat"), dtype=np.float64)
+    return out + (res,)
+
+
+def operator_time(nranks, data_size_proc, nb_blocks_proc, block_sizes, pix, weights, lam, invtt, reps=1, nnz=3):
+    """Seconds per P^T N^-1 P application (max over ranks), reference code on host cores."""
+    dsp = np.ascontiguousarray(data_size_proc, dtype=np.int32)
+    nbp = np.ascontiguousarray(nb_blocks_proc, dtype=np.int32)
+    bs = np.ascontiguousarray(block_sizes, dtype=np.int32)
+    px = np.ascontiguousarray(pix, dtype=np.int32)
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    tt = np.ascontiguousarray(invtt, dtype=np.float64)
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "t.bin")
+        rc = lib().ref_operator_time(nranks, nnz, lam, reps, _p(dsp, I32), _p(nbp, I32), _p(bs, I32), _p(px, I32),
+                                     _p(w, F64), _p(tt, F64), path.encode())
+        if rc != 0:
+            raise RuntimeError(f"reference operator timing failed (status {rc})")
+        return float(np.fromfile(path, dtype=np.float64)[0])

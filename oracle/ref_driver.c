@@ -1,0 +1,261 @@
+/*
+ * Test-oracle driver: thin C entry points around the reference's own
+ * operators, compiled together with the unmodified reference sources into
+ * oracle/_ref/libmidapack_ref.so by oracle/build_ref.sh.  NOT product code;
+ * only tests/, the smoke check and bench.py's CPU-baseline leg load it.
+ *
+ * Each entry point reproduces the call sequence of the reference caller it
+ * names, so a test compares against exactly what MAPPRAISER would compute:
+ *   ref_local_shape   MatInit -> MatLocalShape   (algebra/src/mapmat/mapmat.c:54-73,496-521)
+ *   ref_matvec        MatVecProd                 (mapmat.c:704-729)
+ *   ref_trmatvec      TrMatVecProd               (mapmat.c:819-859)
+ *   ref_stbmm         defineBlocks_avg/defineTpltz_avg + stbmmProd
+ *                     (mappraiser/src/create_toeplitz.c:10-47, toeplitz_wizard.c:80-111)
+ *   ref_pcg           MLmap's set-up (mappraiser.c:64-200) + PCG_GLS_true (pcg_true.c:20-241)
+ *   ref_mlmap         MLmap on n forked ranks (mappraiser.c:34-385)
+ *   ref_operator_time one A = P^T N^-1 P application, timed (CPU baseline)
+ */
+#include <mpi.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "mappraiser/create_toeplitz.h"
+#include "mappraiser/map.h"
+#include "mappraiser/pcg_true.h"
+#include "mappraiser/precond.h"
+#include "midapack.h"
+
+int apply_weights(Tpltz *Nm1, double *tod);
+
+/* indices: in = global, out = local (in place, as MatInit does). Returns lcount. */
+int ref_local_shape(int m, int nnz, int *indices, double *values, int *lindices_out, int cap, int *trash_pix) {
+    Mat A;
+    memset(&A, 0, sizeof(A));
+    A.trash_pix = 0;
+    MatInit(&A, m, nnz, indices, values, ALLREDUCE, MPI_COMM_WORLD);
+    int lc = A.lcount;
+    if (lindices_out) memcpy(lindices_out, A.lindices, sizeof(int) * (size_t) (lc < cap ? lc : cap));
+    *trash_pix = A.trash_pix;
+    MatFree(&A);
+    return lc;
+}
+
+static void build_mat(Mat *A, int m, int nnz, int *gindices, double *values) {
+    memset(A, 0, sizeof(*A));
+    A->trash_pix = 0;
+    MatInit(A, m, nnz, gindices, values, ALLREDUCE, MPI_COMM_WORLD);
+}
+
+/* y = P x; gindices are global and are rewritten in place to local indices */
+int ref_matvec(int m, int nnz, int *gindices, double *values, double *x, double *y) {
+    Mat A;
+    build_mat(&A, m, nnz, gindices, values);
+    MatVecProd(&A, x, y, 0);
+    MatFree(&A);
+    return 0;
+}
+
+/* x = P^T y */
+int ref_trmatvec(int m, int nnz, int *gindices, double *values, double *y, double *x) {
+    Mat A;
+    build_mat(&A, m, nnz, gindices, values);
+    TrMatVecProd(&A, y, x, 0);
+    MatFree(&A);
+    return 0;
+}
+
+static void build_tpltz(Tpltz *Nm1, Block **blocks, int nb_blocks, int *block_sizes, int lambda, double *invtt,
+                        int64_t nrow) {
+    Flag flag_stgy;
+    flag_stgy_init_auto(&flag_stgy);
+    flag_stgy.flag_verbose = 0;
+    *blocks = (Block *) malloc(sizeof(Block) * (size_t) nb_blocks);
+    defineBlocks_avg(*blocks, invtt, nb_blocks, block_sizes, lambda, 0);
+    defineTpltz_avg(Nm1, nrow, 1, 1, *blocks, nb_blocks, nb_blocks, 0, (int) nrow, flag_stgy, MPI_COMM_WORLD);
+}
+
+/* V <- N^-1 V in place (mean removal + banded Toeplitz per block), as apply_weights does */
+int ref_stbmm(int nb_blocks, int *block_sizes, int lambda, double *invtt, double *V) {
+    int64_t nrow = 0;
+    for (int i = 0; i < nb_blocks; i++) nrow += block_sizes[i];
+    Tpltz  Nm1;
+    Block *blocks;
+    build_tpltz(&Nm1, &blocks, nb_blocks, block_sizes, lambda, invtt, nrow);
+    apply_weights(&Nm1, V);
+    free(blocks);
+    return 0;
+}
+
+/* Replicates MLmap's pixel-to-time linked list (mappraiser.c:110-145). */
+static void build_ll(Mat *A, int m) {
+    int nvalid = A->lcount - (A->trash_pix ? A->nnz : 0);
+    A->id_last_pix = (int *) malloc(sizeof(int) * (size_t) (nvalid / A->nnz > 0 ? nvalid / A->nnz : 1));
+    A->ll = (int *) malloc(sizeof(int) * (size_t) (m > 0 ? m : 1));
+    for (int i = 0; i < m; i++) A->ll[i] = -1;
+    for (int j = 0; j < nvalid / A->nnz; j++) A->id_last_pix[j] = -1;
+    for (int i = 0; i < m; i++) {
+        if (!A->trash_pix || (A->trash_pix && (A->indices[i * A->nnz] != 0))) {
+            int vpix_i = A->indices[i * A->nnz] / A->nnz - A->trash_pix;
+            if (A->id_last_pix[vpix_i] == -1) A->id_last_pix[vpix_i] = i;
+            else {
+                A->ll[i]               = A->id_last_pix[vpix_i];
+                A->id_last_pix[vpix_i] = i;
+            }
+        }
+    }
+}
+
+/*
+ * Single-rank GLS solve exactly as MLmap drives it (solver 0, BJ precond).
+ * gindices/values/signal are modified in place like the reference does.
+ * Outputs: x_out (capacity 3*npix_cap unknowns), lstid_out (global ids of x),
+ * cond_out, hits_out; returns the number of unknowns n.
+ */
+int ref_pcg(int m, int nnz, int *gindices, double *values, double *signal, double *noise, int nb_blocks,
+            int *block_sizes, int lambda, double *invtt, double tol, int maxiter, const char *outpath,
+            const char *ref, double *x_out, int *lstid_out, double *cond_out, int *hits_out, int cap) {
+    Mat A;
+    build_mat(&A, m, nnz, gindices, values);
+    build_ll(&A, m);
+    int     nvalid = A.lcount - (A.trash_pix ? A.nnz : 0);
+    double *x      = (double *) calloc((size_t) nvalid, sizeof(double));
+    double *cond   = (double *) calloc((size_t) (nvalid / 3 + 1), sizeof(double));
+    int    *lhits  = (int *) calloc((size_t) (nvalid / 3 + 1), sizeof(int));
+    Tpltz   Nm1;
+    Block  *blocks;
+    build_tpltz(&Nm1, &blocks, nb_blocks, block_sizes, lambda, invtt, (int64_t) m);
+    PCG_GLS_true((char *) outpath, (char *) ref, &A, &Nm1, x, signal, noise, cond, lhits, tol, maxiter, 0, 0);
+    int n = A.lcount - A.nnz * A.trash_pix;
+    if (n > cap) n = cap;
+    memcpy(x_out, x, sizeof(double) * (size_t) n);
+    for (int i = 0; i < n; i++) lstid_out[i] = A.lindices[i + A.nnz * A.trash_pix];
+    memcpy(cond_out, cond, sizeof(double) * (size_t) (n / 3));
+    memcpy(hits_out, lhits, sizeof(int) * (size_t) (n / 3));
+    MatFree(&A);
+    free(x);
+    free(cond);
+    free(lhits);
+    free(blocks);
+    return n;
+}
+
+/* ---- MLmap over forked ranks ---- */
+typedef struct {
+    char   *outpath, *ref;
+    double  tol;
+    int     maxiter, nside, nnz, lambda, nranks;
+    int    *data_size_proc; /* [nranks] */
+    int    *nb_blocks_proc; /* [nranks] */
+    int    *block_sizes;    /* all blocks, rank-major */
+    int    *pix;            /* global arrays (rank-major) */
+    double *weights, *signal, *noise, *invtt;
+} mlmap_args;
+
+static void mlmap_rank(int rank, void *vp) {
+    mlmap_args *a = (mlmap_args *) vp;
+    int64_t     s0 = 0;
+    int         b0 = 0;
+    for (int r = 0; r < rank; r++) {
+        s0 += a->data_size_proc[r];
+        b0 += a->nb_blocks_proc[r];
+    }
+    int m = a->data_size_proc[rank];
+    /* MLmap rewrites its inputs in place; work on private copies */
+    int    *pix = (int *) malloc(sizeof(int) * (size_t) m * a->nnz);
+    double *w   = (double *) malloc(sizeof(double) * (size_t) m * a->nnz);
+    double *sig = (double *) malloc(sizeof(double) * (size_t) m);
+    double *noi = (double *) malloc(sizeof(double) * (size_t) m);
+    memcpy(pix, a->pix + s0 * a->nnz, sizeof(int) * (size_t) m * a->nnz);
+    memcpy(w, a->weights + s0 * a->nnz, sizeof(double) * (size_t) m * a->nnz);
+    memcpy(sig, a->signal + s0, sizeof(double) * (size_t) m);
+    memcpy(noi, a->noise + s0, sizeof(double) * (size_t) m);
+    MLmap(MPI_COMM_WORLD, a->outpath, a->ref, 0, 0, 0, ALLREDUCE, a->tol, a->maxiter, 0, 0, 0, a->nside,
+          a->data_size_proc, a->nb_blocks_proc[rank], a->block_sizes + b0, a->nnz, pix, w, sig, noi, a->lambda,
+          a->invtt + (size_t) b0 * a->lambda);
+    free(pix);
+    free(w);
+    free(sig);
+    free(noi);
+}
+
+int ref_mlmap(int nranks, const char *outpath, const char *ref, double tol, int maxiter, int nside, int nnz,
+              int lambda, int *data_size_proc, int *nb_blocks_proc, int *block_sizes, int *pix, double *weights,
+              double *signal, double *noise, double *invtt) {
+    mlmap_args a = {(char *) outpath, (char *) ref, tol,   maxiter, nside,  nnz,   lambda, nranks,
+                    data_size_proc,   nb_blocks_proc, block_sizes, pix,   weights, signal, noise, invtt};
+    return shim_mpi_run(nranks, mlmap_rank, &a);
+}
+
+/* ---- CPU baseline: time one operator application P^T N^-1 P on n ranks ---- */
+typedef struct {
+    int     nranks, nnz, lambda, reps;
+    int    *data_size_proc, *nb_blocks_proc, *block_sizes, *pix;
+    double *weights, *invtt;
+    double *seconds; /* shared result: max over ranks, written by rank 0 via Allreduce */
+    double *shared_out;
+} optime_args;
+
+static void optime_rank(int rank, void *vp) {
+    optime_args *a  = (optime_args *) vp;
+    int64_t      s0 = 0;
+    int          b0 = 0;
+    for (int r = 0; r < rank; r++) {
+        s0 += a->data_size_proc[r];
+        b0 += a->nb_blocks_proc[r];
+    }
+    int     m   = a->data_size_proc[rank];
+    int    *pix = (int *) malloc(sizeof(int) * (size_t) m * a->nnz);
+    memcpy(pix, a->pix + s0 * a->nnz, sizeof(int) * (size_t) m * a->nnz);
+    Mat A;
+    memset(&A, 0, sizeof(A));
+    MatInit(&A, m, a->nnz, pix, a->weights + s0 * a->nnz, ALLREDUCE, MPI_COMM_WORLD);
+    int64_t M = 0;
+    for (int r = 0; r < a->nranks; r++) M += a->data_size_proc[r];
+    int nb_tot = 0;
+    for (int r = 0; r < a->nranks; r++) nb_tot += a->nb_blocks_proc[r];
+    Flag flag_stgy;
+    flag_stgy_init_auto(&flag_stgy);
+    flag_stgy.flag_verbose = 0;
+    Block *blocks = (Block *) malloc(sizeof(Block) * (size_t) a->nb_blocks_proc[rank]);
+    defineBlocks_avg(blocks, a->invtt + (size_t) b0 * a->lambda, a->nb_blocks_proc[rank], a->block_sizes + b0,
+                     a->lambda, s0);
+    Tpltz Nm1;
+    defineTpltz_avg(&Nm1, M, 1, 1, blocks, a->nb_blocks_proc[rank], nb_tot, s0, m, flag_stgy, MPI_COMM_WORLD);
+    int     n   = A.lcount - A.nnz * A.trash_pix;
+    double *h   = (double *) malloc(sizeof(double) * (size_t) (n > 0 ? n : 1));
+    double *out = (double *) malloc(sizeof(double) * (size_t) (n > 0 ? n : 1));
+    double *tod = (double *) malloc(sizeof(double) * (size_t) m);
+    for (int i = 0; i < n; i++) h[i] = 1.0 + 1e-3 * (double) (i % 97);
+    MPI_Barrier(MPI_COMM_WORLD);
+    double t0 = MPI_Wtime();
+    for (int r = 0; r < a->reps; r++) {
+        MatVecProd(&A, h, tod, 0);
+        apply_weights(&Nm1, tod);
+        TrMatVecProd(&A, tod, out, 0);
+    }
+    double dt = (MPI_Wtime() - t0) / (double) a->reps, dmax;
+    MPI_Allreduce(&dt, &dmax, 1, MPI_DOUBLE, MPI_MAX, MPI_COMM_WORLD);
+    if (rank == 0) {
+        FILE *f = fopen((char *) a->shared_out, "wb");
+        if (f) {
+            fwrite(&dmax, sizeof(double), 1, f);
+            fclose(f);
+        }
+    }
+    MatFree(&A);
+    free(pix);
+    free(blocks);
+    free(h);
+    free(out);
+    free(tod);
+}
+
+/* writes max-over-ranks seconds per application to the file named by result_path */
+int ref_operator_time(int nranks, int nnz, int lambda, int reps, int *data_size_proc, int *nb_blocks_proc,
+                      int *block_sizes, int *pix, double *weights, double *invtt, const char *result_path) {
+    optime_args a = {nranks, nnz, lambda, reps, data_size_proc, nb_blocks_proc, block_sizes, pix, weights,
+                     invtt,  NULL, (double *) result_path};
+    return shim_mpi_run(nranks, optime_rank, &a);
+}

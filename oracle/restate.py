@@ -1,0 +1,323 @@
+"""CPU restatement of the reference's GLS map-making path (numpy / scipy).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check and by
+bench.py's CPU-baseline leg, always as the checker, never as the thing
+measured or shipped.  The product path (midapack_b200) never imports it.
+
+Each function restates one reference routine (file:line in its docstring,
+paths relative to the reference project root).  The restatement is pinned
+against the reference's own compiled C (oracle/_ref, built by
+oracle/build_ref.sh) in tests/test_oracle_pin.py.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+# --------------------------------------------------------------------------- pointing
+@dataclass
+class Pointing:
+    m: int
+    nnz: int
+    local: np.ndarray      # int32 [m*nnz] local indices (position in lindices)
+    values: np.ndarray     # f64  [m*nnz]
+    lindices: np.ndarray   # int32 sorted unique global indices
+    trash_pix: int
+
+    @property
+    def lcount(self) -> int:
+        return int(self.lindices.size)
+
+    @property
+    def n(self) -> int:
+        """Map-domain size: lcount - nnz*trash_pix (mappraiser.c:96-98)."""
+        return self.lcount - self.nnz * self.trash_pix
+
+
+def local_shape(gindices: np.ndarray, values: np.ndarray, m: int, nnz: int) -> Pointing:
+    """MatInit -> MatLocalShape (algebra/src/mapmat/mapmat.c:54-73, 496-521).
+
+    lindices = sorted unique global indices (counting_sort, csort.c:111-135);
+    each index becomes its position in lindices (sindex/dichotomy,
+    cindex.c:34-42, 102-116); trash_pix = 1 when lindices[0] < 0.
+    """
+    g = np.asarray(gindices, dtype=np.int32)
+    lind = np.unique(g)
+    local = np.searchsorted(lind, g).astype(np.int32)
+    trash = 1 if lind.size and lind[0] < 0 else 0
+    return Pointing(m, nnz, local, np.asarray(values, dtype=np.float64), lind.astype(np.int32), trash)
+
+
+def matvec(A: Pointing, x: np.ndarray) -> np.ndarray:
+    """y = P x, MatVecProd (mapmat.c:704-729), including the trash-row skip."""
+    idx = A.local.reshape(A.m, A.nnz).astype(np.int64)
+    val = A.values.reshape(A.m, A.nnz)
+    if A.trash_pix:
+        keep = idx[:, 0] != 0
+        y = np.zeros(A.m)
+        xi = x[np.where(keep[:, None], idx - A.nnz, 0)]
+        # accumulate in the reference's j order: ((0 + v0 x0) + v1 x1) + v2 x2
+        acc = np.zeros(A.m)
+        for j in range(A.nnz):
+            acc = acc + val[:, j] * xi[:, j]
+        y[keep] = acc[keep]
+        return y
+    acc = np.zeros(A.m)
+    for j in range(A.nnz):
+        acc = acc + val[:, j] * x[idx[:, j]]
+    return acc
+
+
+def trmatvec(A: Pointing, y: np.ndarray) -> np.ndarray:
+    """x = P^T y, TrMatVecProd (mapmat.c:819-859); single rank, so the
+    ALLREDUCE of greedyreduce (mapmat.c:1008-1141) is the identity.
+    np.add.at accumulates in sample order, like the reference loop."""
+    idx = A.local.reshape(A.m, A.nnz).astype(np.int64)
+    val = A.values.reshape(A.m, A.nnz)
+    x = np.zeros(A.n)
+    if A.trash_pix:
+        keep = idx[:, 0] != 0
+        ii = (idx[keep] - A.nnz)
+        contrib = val[keep] * y[keep][:, None]
+    else:
+        ii = idx
+        contrib = val * y[:, None]
+    np.add.at(x, ii.reshape(-1), contrib.reshape(-1))
+    return x
+
+
+# --------------------------------------------------------------------------- Toeplitz
+def block_offsets(block_sizes: np.ndarray) -> np.ndarray:
+    """idv of each block (create_toeplitz.c:27-47, id0 = 0)."""
+    off = np.zeros(len(block_sizes) + 1, dtype=np.int64)
+    off[1:] = np.cumsum(np.asarray(block_sizes, dtype=np.int64))
+    return off
+
+
+def banded_toeplitz_fft(v: np.ndarray, t: np.ndarray) -> np.ndarray:
+    """Exact (within a block, zero outside) symmetric banded Toeplitz product,
+    computed as one linear convolution by FFT of a padded length.  The
+    reference's overlap-save tiling (toeplitz.c:731-865) computes the same
+    product tile by tile."""
+    n = v.size
+    lam = t.size
+    if lam == 1:
+        return v * t[0]
+    h = np.concatenate([t[:0:-1], t])  # kernel, taps -(lam-1)..(lam-1)
+    L = n + h.size - 1
+    nfft = 1 << int(np.ceil(np.log2(L)))
+    full = np.fft.irfft(np.fft.rfft(v, nfft) * np.fft.rfft(h, nfft), nfft)[:L]
+    return full[lam - 1: lam - 1 + n]
+
+
+def banded_toeplitz_direct(v: np.ndarray, t: np.ndarray) -> np.ndarray:
+    """Same product by direct summation in long double: the exact arbiter for
+    small cases (the reference's no-FFT product, toeplitz_nofft.c:104-150,
+    computed here for the edges too)."""
+    n = v.size
+    lam = t.size
+    vl = v.astype(np.longdouble)
+    out = vl * np.longdouble(t[0])
+    for k in range(1, min(lam, n)):
+        tk = np.longdouble(t[k])
+        out[k:] += tk * vl[:-k]
+        out[:-k] += tk * vl[k:]
+    return out.astype(np.float64)
+
+
+def stbmm(V: np.ndarray, block_sizes: np.ndarray, lam: int, invtt: np.ndarray, exact: bool = False) -> np.ndarray:
+    """apply_weights (pcg_true.c:578-600) -> stbmmProd (toeplitz_wizard.c:80-111):
+    per block, subtract the block mean, then the banded Toeplitz product; with
+    lambda == 1 only the diagonal scaling (no mean removal)."""
+    out = np.array(V, dtype=np.float64, copy=True)
+    off = block_offsets(block_sizes)
+    for b in range(len(block_sizes)):
+        s, e = off[b], off[b + 1]
+        t = np.asarray(invtt[b * lam:(b + 1) * lam], dtype=np.float64)
+        if lam == 1:
+            out[s:e] = t[0] * out[s:e]
+            continue
+        seg = out[s:e]
+        seg = seg - seg.sum() / (e - s)
+        out[s:e] = banded_toeplitz_direct(seg, t) if exact else banded_toeplitz_fft(seg, t)
+    return out
+
+
+# --------------------------------------------------------------------------- block Jacobi
+def local_W(A: Pointing, block_sizes: np.ndarray, lam: int, invtt: np.ndarray):
+    """getlocalW (mappraiser/src/precond.c:42-161): per-pixel 3x3 blocks of
+    P^T diag(N^-1) P and hit counts; diag(N^-1) = T_block[0] inside a block."""
+    nnz = A.nnz
+    off = block_offsets(block_sizes)
+    diag = np.empty(A.m)
+    for b in range(len(block_sizes)):
+        diag[off[b]:off[b + 1]] = invtt[b * lam]
+    if off[-1] < A.m:
+        diag[off[-1]:] = 1.0
+    idx = A.local.reshape(A.m, nnz).astype(np.int64)
+    val = A.values.reshape(A.m, nnz)
+    keep = (idx[:, 0] != 0) if A.trash_pix else np.ones(A.m, dtype=bool)
+    npx = A.n // nnz
+    W = np.zeros(npx * nnz * nnz)
+    hits = np.zeros(npx, dtype=np.int64)
+    ik = idx[keep] - nnz * A.trash_pix
+    vk = val[keep]
+    dk = diag[keep]
+    np.add.at(hits, ik[:, 0] // nnz, 1)
+    for j in range(nnz):
+        for k in range(nnz):
+            np.add.at(W, nnz * ik[:, j] + k, vk[:, j] * vk[:, k] * dk)
+    return W.reshape(npx, nnz, nnz), hits
+
+
+def bj_blocks(W: np.ndarray):
+    """Per pixel: anorm = dlange('1'), LU = dgetrf, rcond = dgecon('1'); keep
+    the pixel when rcond > 0.1 and invert with dgetri
+    (precond.c:511-583).  Uses scipy's LAPACK, i.e. the real routines."""
+    from scipy.linalg import lapack
+
+    npx = W.shape[0]
+    rcond = np.zeros(npx)
+    inv = np.zeros_like(W)
+    for p in range(npx):
+        a = np.array(W[p], dtype=np.float64, order="F")
+        anorm = np.abs(a).sum(axis=0).max()
+        lu, piv, info = lapack.dgetrf(a)
+        rc, info2 = lapack.dgecon(lu, anorm, norm="1")
+        rcond[p] = rc
+        if rc > 1e-1:
+            ainv, info3 = lapack.dgetri(lu, piv)
+            inv[p] = ainv
+    return rcond, inv
+
+
+@dataclass
+class BJResult:
+    A: Pointing               # pointing after the cut (re-initialised)
+    signal: np.ndarray        # b with cut samples zeroed
+    inv: np.ndarray           # [n/3, 3, 3] inverse blocks of kept pixels
+    W: np.ndarray             # [n/3, 3, 3] blocks of kept pixels
+    cond: np.ndarray          # rcond of kept pixels
+    hits: np.ndarray          # hits of kept pixels
+    cut: np.ndarray           # bool per pre-cut pixel
+
+
+def precond_blockjacobi(A: Pointing, signal: np.ndarray, block_sizes, lam, invtt) -> BJResult:
+    """precondblockjacobilike (precond.c:456-702): cut pixels with rcond <= 0.1,
+    point their samples to the trash triplet (-3,-2,-1) with zero weights, zero
+    their signal samples, then MatInit again on the rewritten global indices."""
+    nnz = A.nnz
+    W, hits = local_W(A, block_sizes, lam, invtt)
+    rcond, inv = bj_blocks(W)
+    cut = ~(rcond > 1e-1)
+    gl = A.lindices[A.local.astype(np.int64)].astype(np.int32)  # back to global indices
+    vals = A.values.copy()
+    sig = np.array(signal, dtype=np.float64, copy=True)
+    if cut.any():
+        # The reference walks the pixel->samples linked list from
+        # id_last_pix[u + trash_pix] for the u-th pixel block
+        # (precond.c:521, 585-600), while MLmap indexes id_last_pix by
+        # u itself (mappraiser.c:130-142).  With flagged samples present the
+        # samples rewritten are therefore those of pixel u + 1; that is kept
+        # here as the reference behaves (a target past the last pixel rewrites
+        # nothing).
+        idx = A.local.reshape(A.m, nnz).astype(np.int64)
+        valid = (idx[:, 0] != 0) if A.trash_pix else np.ones(A.m, dtype=bool)
+        pixrow = np.where(valid, idx[:, 0] // nnz - A.trash_pix, -1)
+        npx = cut.size
+        target = np.zeros(npx, dtype=bool)
+        cu = np.nonzero(cut)[0] + A.trash_pix
+        target[cu[cu < npx]] = True
+        rows = valid & target[np.clip(pixrow, 0, None)]
+        g2 = gl.reshape(A.m, nnz)
+        g2[rows] = np.arange(nnz, dtype=np.int32) - nnz
+        vals.reshape(A.m, nnz)[rows] = 0.0
+        sig[rows] = 0.0
+        gl = g2.reshape(-1)
+    A2 = local_shape(gl, vals, A.m, nnz)
+    if cut.any():
+        A2.trash_pix = 1
+    keep = ~cut
+    return BJResult(A2, sig, inv[keep], W[keep], rcond[keep], hits[keep], cut)
+
+
+def apply_bj(inv: np.ndarray, g: np.ndarray) -> np.ndarray:
+    """apply_precond, precond = 0 (precond.c:1403-1409): MatVecProd(BJ_inv, g)."""
+    gp = g.reshape(-1, 3)
+    out = np.zeros_like(gp)
+    for j in range(3):
+        out = out + inv[:, :, j] * gp[:, j:j + 1]
+    return out.reshape(-1)
+
+
+# --------------------------------------------------------------------------- PCG
+@dataclass
+class PCGResult:
+    x: np.ndarray
+    iters: int
+    res_rel: list
+    bj: BJResult
+
+
+def pcg(gindices, values, signal, noise, block_sizes, lam, invtt, tol=1e-8, maxiter=500,
+        nnz: int = 3, exact_toeplitz: bool = False) -> PCGResult:
+    """PCG_GLS_true (mappraiser/src/pcg_true.c:20-241), single rank (pixpond = 1):
+    Polak-Ribiere PCG on (P^T N^-1 P) x = P^T N^-1 (b + noise), block-Jacobi
+    preconditioner, stop when sum(g^2) <= tol^2 * sum(g0^2)."""
+    m = len(signal)
+    A = local_shape(gindices, values, m, nnz)
+    bj = precond_blockjacobi(A, signal, block_sizes, lam, invtt)
+    A = bj.A
+    n = A.n
+    x = np.zeros(n)
+    N = lambda v: stbmm(v, block_sizes, lam, invtt, exact=exact_toeplitz)  # noqa: E731
+    _g = bj.signal + noise - matvec(A, x)
+    g = trmatvec(A, N(_g))
+    Cg = apply_bj(bj.inv, g)
+    h = Cg.copy()
+    g2pix = float(np.dot(Cg, g))
+    res = float(np.dot(g, g))
+    res0 = res
+    tol2rel = tol * tol * res
+    res_rel = [1.0]
+    k = 1
+    if res <= tol:
+        return PCGResult(x, 0, res_rel, bj)
+    while k < maxiter:
+        gp = g
+        Ah = matvec(A, h)
+        AtNm1Ah = trmatvec(A, N(Ah))
+        coeff = float(np.dot(h, AtNm1Ah))
+        ro = g2pix / coeff
+        x = x + ro * h
+        g = gp - ro * AtNm1Ah
+        Cg = apply_bj(bj.inv, g)
+        g2pixp = g2pix
+        g2pix = float(np.dot(Cg, g))
+        g2pix_polak = float(np.dot(Cg, g - gp))
+        res = float(np.dot(g, g))
+        res_rel.append(float(np.sqrt(res) / np.sqrt(res0)))
+        if res <= tol2rel:
+            break
+        gamma = g2pix_polak / g2pixp
+        h = h * gamma + Cg
+        k += 1
+    return PCGResult(x, k, res_rel, bj)
+
+
+def x2map_pol(x, lstid, cond, hits, npix):
+    """x2map_pol (mappraiser/src/mappraiser.c:836-853)."""
+    mapI = np.zeros(npix)
+    mapQ = np.zeros(npix)
+    mapU = np.zeros(npix)
+    Cond = np.zeros(npix)
+    Hits = np.zeros(npix, dtype=np.int32)
+    p = (np.asarray(lstid[0::3]) // 3).astype(np.int64)
+    mapI[p] = x[0::3]
+    mapQ[p] = x[1::3]
+    mapU[p] = x[2::3]
+    Cond[p] = cond
+    Hits[p] = hits
+    return mapI, mapQ, mapU, Cond, Hits
