@@ -1,0 +1,118 @@
+/*
+ * midapack_b200 device-level C API.
+ *
+ * The GLS map-making hot path (P^T N^-1 P) m = P^T N^-1 d on one B200, on
+ * device-resident data: every pointer named d_* is device memory owned by the
+ * caller, every h_* pointer is host memory.  The reference-compatible API
+ * (MatInit, MatVecProd, TrMatVecProd, stbmmProd, PCG_GLS_true, MLmap; host
+ * pointers) is declared in mapmat.h, toeplitz.h and mappraiser.h and is built
+ * on top of this one.
+ *
+ * All functions return 0 (MDP_OK) or an MDP_E* code; mdp_last_error() gives a
+ * one-line description of the last failure on the calling thread.  Work is
+ * queued on the context's stream; functions that return host-visible results
+ * synchronise that stream.
+ */
+#ifndef MIDAPACK_B200_H
+#define MIDAPACK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MDP_OK           0
+#define MDP_EINVAL       1 /* bad argument (size, pointer, index out of range) */
+#define MDP_ENOMEM       2 /* device or host allocation failed */
+#define MDP_ECUDA        3 /* CUDA runtime error */
+#define MDP_EUNSUPPORTED 4 /* valid input this build does not handle */
+#define MDP_ENAN         5 /* NaN/Inf met in a reduction */
+#define MDP_ETIMEOUT     6 /* a bounded device-side wait gave up */
+
+typedef struct mdp_context  mdp_context;
+typedef struct mdp_pointing mdp_pointing;
+typedef struct mdp_noise    mdp_noise;
+
+const char *mdp_strerror(int code);
+const char *mdp_last_error(void);
+
+/* ---- context: one device, one stream ---------------------------------- */
+int      mdp_context_create(int device, mdp_context **out);
+void     mdp_context_destroy(mdp_context *ctx);
+/* queue work on an existing cudaStream_t (e.g. the caller's); NULL = own stream */
+int      mdp_context_set_stream(mdp_context *ctx, void *cuda_stream);
+void    *mdp_context_stream(mdp_context *ctx);
+int      mdp_synchronize(mdp_context *ctx);
+/* number of kernels this library launched on ctx since creation */
+uint64_t mdp_launch_count(const mdp_context *ctx);
+
+/* ---- pointing matrix P (reference: Mat, algebra/include/mapmat/mapmat.h:46-69) ----
+ * m rows (time samples), nnz entries per row, global column indices d_gindices
+ * [m*nnz] (int32, e.g. 3*pixel+stokes, negative = flagged) and weights
+ * d_values [m*nnz].  Creation compresses the indices exactly as MatInit /
+ * MatLocalShape do (sorted unique set, position = local index, trash pixel
+ * when the smallest index is negative).  d_values is borrowed, not copied: it
+ * must stay valid while the pointing exists. */
+int  mdp_pointing_create(mdp_context *ctx, int64_t m, int nnz, const int32_t *d_gindices,
+                         const double *d_values, mdp_pointing **out);
+void mdp_pointing_destroy(mdp_pointing *A);
+/* lcount = #unique indices, n_map = lcount - nnz*trash_pix (map-domain size) */
+int  mdp_pointing_shape(const mdp_pointing *A, int64_t *lcount, int *trash_pix, int64_t *n_map,
+                        int *triplet_layout);
+int  mdp_pointing_lindices(mdp_context *ctx, const mdp_pointing *A, int32_t *d_lindices);
+int  mdp_pointing_local_indices(mdp_context *ctx, const mdp_pointing *A, int32_t *d_local);
+/* y[m] = P x[n_map]          (reference MatVecProd, mapmat.c:704-729) */
+int  mdp_matvec(mdp_context *ctx, const mdp_pointing *A, const double *d_x, double *d_y);
+/* x[n_map] = P^T y[m]        (reference TrMatVecProd, mapmat.c:819-859) */
+int  mdp_trmatvec(mdp_context *ctx, const mdp_pointing *A, const double *d_y, double *d_x);
+
+/* ---- inverse noise N^-1: block-diagonal banded symmetric Toeplitz --------
+ * (reference: Tpltz/Block, algebra/include/toeplitz/toeplitz.h:152-203)
+ * Block b covers rows [h_idv[b], h_idv[b] + h_n[b]) and its first row is
+ * h_T[b*lambda .. b*lambda+lambda).  Spectra are computed once here. */
+int  mdp_noise_create(mdp_context *ctx, int nb_blocks, const int64_t *h_idv, const int32_t *h_n,
+                      int lambda, const double *h_T, mdp_noise **out);
+void mdp_noise_destroy(mdp_noise *N);
+/* out = N^-1 in: per block, subtract the block mean then apply the banded
+ * Toeplitz block (reference stbmmProd, toeplitz_wizard.c:80-111; with
+ * lambda == 1 the diagonal scaling of apply_weights, pcg_true.c:578-600).
+ * in == out is allowed. */
+int  mdp_stbmm(mdp_context *ctx, const mdp_noise *N, const double *d_in, double *d_out);
+int  mdp_noise_tile(const mdp_noise *N, int *fft_size, int *cluster_ctas, int64_t *n_tiles);
+
+/* ---- GLS solve (reference PCG_GLS_true with block-Jacobi, pcg_true.c:20-241) ---- */
+typedef struct {
+    double tol;      /* relative residual: stop when sum(g^2) <= tol^2 sum(g0^2) */
+    int    maxiter;  /* K: at most K-1 iterations, as the reference */
+    int    verbose;  /* 1: print the reference's per-iteration line on stdout */
+} mdp_solve_params;
+
+typedef struct {
+    int     iterations;    /* k at exit (the reference's loop index) */
+    int     converged;
+    double  res0, res;     /* sum(g0^2) and final sum(g^2) */
+    int64_t n_map;         /* unknowns after the rcond cut */
+    int64_t n_cut;         /* pixels removed by the rcond cut */
+    double  precond_seconds, solve_seconds;
+} mdp_solve_info;
+
+/* Builds the block-Jacobi preconditioner (rcond > 0.1 cut, exactly as
+ * precondblockjacobilike, precond.c:456-702; A is updated in place to the
+ * post-cut pointing) and solves with x0 = 0.  Outputs (device, capacity
+ * n_map of A before the cut, i.e. mdp_pointing_shape's n_map):
+ *   d_x      solution, n_map entries after the cut
+ *   d_lstid  global index of each solution entry (lindices minus trash)
+ *   d_cond   rcond of each kept pixel (n_map/3)
+ *   d_hits   hit count of each kept pixel (n_map/3)
+ * h_res_rel (optional, maxiter+1 entries) receives sqrt(res/res0) per iteration. */
+int mdp_gls_solve(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *d_signal,
+                  const double *d_noise, const mdp_solve_params *params, double *d_x, int32_t *d_lstid,
+                  double *d_cond, int32_t *d_hits, double *h_res_rel, mdp_solve_info *info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MIDAPACK_B200_H */

@@ -1,0 +1,159 @@
+// Internal declarations shared by the midapack_b200 CUDA sources.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "midapack_b200.h"
+
+#define MDP_SM_COUNT_HINT 148
+
+// ---------------------------------------------------------------- errors
+void mdp_set_error(const char *fmt, ...);
+
+#define MDP_CUDA(call)                                                                       \
+    do {                                                                                     \
+        cudaError_t e__ = (call);                                                            \
+        if (e__ != cudaSuccess) {                                                            \
+            mdp_set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e__)); \
+            return MDP_ECUDA;                                                                \
+        }                                                                                    \
+    } while (0)
+
+#define MDP_CHECK_LAUNCH(ctx)                                                                \
+    do {                                                                                     \
+        (ctx)->launches++;                                                                   \
+        cudaError_t e__ = cudaGetLastError();                                                \
+        if (e__ != cudaSuccess) {                                                            \
+            mdp_set_error("%s:%d kernel launch: %s", __FILE__, __LINE__, cudaGetErrorString(e__)); \
+            return MDP_ECUDA;                                                                \
+        }                                                                                    \
+    } while (0)
+
+#define MDP_TRY(expr)                                                                        \
+    do {                                                                                     \
+        int rc__ = (expr);                                                                   \
+        if (rc__ != MDP_OK) return rc__;                                                     \
+    } while (0)
+
+// ---------------------------------------------------------------- device buffer
+struct DevBuf {
+    void  *p     = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p     = nullptr;
+        bytes = 0;
+    }
+    int alloc(size_t nbytes) {  // (re)allocate when too small; contents are not kept
+        if (nbytes <= bytes && p) return MDP_OK;
+        release();
+        if (nbytes == 0) nbytes = 16;
+        cudaError_t e = cudaMalloc(&p, nbytes);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            cudaGetLastError();
+            mdp_set_error("cudaMalloc(%zu bytes): %s", nbytes, cudaGetErrorString(e));
+            return MDP_ENOMEM;
+        }
+        bytes = nbytes;
+        return MDP_OK;
+    }
+    template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+// ---------------------------------------------------------------- context
+struct mdp_context {
+    int          device = 0;
+    int          sm_count = MDP_SM_COUNT_HINT;
+    cudaStream_t stream = nullptr;
+    bool         own_stream = false;
+    uint64_t     launches = 0;
+    // small reusable scratch
+    DevBuf       red;       // reduction partials
+    DevBuf       scalars;   // device scalars of the solver
+    DevBuf       scratch;   // large temporary (stbmm in place, scans)
+    DevBuf       scratch2;
+    double      *h_pinned = nullptr;  // pinned host scalars
+};
+
+// ---------------------------------------------------------------- pointing
+struct mdp_pointing {
+    int64_t       m = 0;
+    int           nnz = 0;
+    int           trash_pix = 0;
+    int64_t       lcount = 0;
+    int           triplet = 0;        // fast layout: one map offset per row
+    const double *values = nullptr;   // borrowed [m*nnz]
+    DevBuf        lindices;           // int32 [lcount]
+    DevBuf        local;              // int32 [m*nnz] (general layout only)
+    DevBuf        off;                // int32 [m]: map offset 3q, -1 trash row, -2 cut row (triplet layout)
+    int64_t n_map() const { return lcount - (int64_t) nnz * trash_pix; }
+};
+
+// ---------------------------------------------------------------- noise
+struct mdp_noise {
+    int                  nb = 0;
+    int                  lambda = 0;
+    int64_t              nrow_end = 0;   // max(idv+n)
+    std::vector<int64_t> h_idv;
+    std::vector<int32_t> h_n;
+    std::vector<double>  h_T0;           // diagonal of each block
+    // tile plan
+    int     log2_ml = 0;   // per-CTA complex points = 2^log2_ml
+    int     cluster = 1;   // CTAs per tile
+    int     fft_n = 0;     // real FFT size N = 2 * cluster * 2^log2_ml
+    int64_t n_tiles = 0;
+    DevBuf  tile_start;    // int64 [n_tiles] first output row (global)
+    DevBuf  tile_block;    // int32 [n_tiles]
+    DevBuf  blk_start;     // int64 [nb]
+    DevBuf  blk_len;       // int32 [nb]
+    DevBuf  blk_spec;      // int32 [nb] index of the block's spectrum
+    DevBuf  blk_t0;        // double [nb] T_block[0]
+    DevBuf  spectra;       // double [n_spec][N/2+1]
+    DevBuf  twiddle;       // double2 [N/2]: exp(-2 pi i k / N)
+    DevBuf  means;         // double [nb]
+    int     n_spec = 0;
+};
+
+// ---------------------------------------------------------------- block Jacobi state (solver.cu)
+// Kept blocks after the rcond cut, in their original order; block k pairs
+// with pixel k of the re-initialised pointing.
+struct BJState {
+    DevBuf  inv;    // [npix][9] inverse blocks, row-major
+    DevBuf  W;      // [npix][9] P^T diag(N^-1) P blocks
+    DevBuf  rcond;  // [npix]
+    DevBuf  hits;   // [npix]
+    int64_t npix = 0;
+    int64_t ncut = 0;
+};
+int mdp_bj_build(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, BJState *bj);
+int mdp_pcg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *inv, int64_t npix,
+                const double *d_signal, const double *d_noise, const mdp_solve_params *params, double *d_x,
+                double *h_res_rel, mdp_solve_info *info);
+int mdp_pointing_create_ex(mdp_context *ctx, int64_t m, int nnz, const int32_t *d_g, const double *d_values,
+                           int32_t *d_local_out, mdp_pointing **out);
+int mdp_matvec_launch(mdp_context *ctx, const mdp_pointing *A, const double *d_x, double *d_y);
+int mdp_trmatvec_launch(mdp_context *ctx, const mdp_pointing *A, const double *d_y, double *d_x);
+
+// ---------------------------------------------------------------- helpers (pointing.cu / reduce)
+int mdp_exclusive_scan_u32(mdp_context *ctx, const uint32_t *d_in, uint32_t *d_out, int64_t n,
+                           uint32_t *h_total);
+int mdp_stbmm_impl(mdp_context *ctx, const mdp_noise *N, const double *d_in, double *d_out,
+                   const double *d_means_or_null);
+int mdp_block_means(mdp_context *ctx, const mdp_noise *N, const double *d_v, double *d_means);
+
+inline int grid_for(int64_t n, int threads, int max_blocks = 148 * 16) {
+    int64_t b = (n + threads - 1) / threads;
+    if (b > max_blocks) b = max_blocks;
+    if (b < 1) b = 1;
+    return (int) b;
+}

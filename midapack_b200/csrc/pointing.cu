@@ -1,0 +1,565 @@
+// Pointing matrix P on the device: index compression (MatInit/MatLocalShape),
+// y = P x (MatVecProd) and x = P^T y (TrMatVecProd), plus the context, error
+// handling and the device-wide scan they use.
+//
+// Reference: algebra/src/mapmat/mapmat.c:54-73 (MatInit), 496-521
+// (MatLocalShape), 704-729 (MatVecProd), 819-859 (TrMatVecProd);
+// algebra/src/mapmat/csort.c:111-135 (counting_sort), cindex.c:34-42,102-116
+// (sindex/dichotomy).
+#include <cstdarg>
+#include <cstring>
+
+#include "mdp_internal.cuh"
+
+// ============================================================== errors
+static thread_local char g_err[512] = "";
+
+void mdp_set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+extern "C" const char *mdp_last_error(void) { return g_err; }
+
+extern "C" const char *mdp_strerror(int code) {
+    switch (code) {
+        case MDP_OK: return "ok";
+        case MDP_EINVAL: return "invalid argument";
+        case MDP_ENOMEM: return "out of memory";
+        case MDP_ECUDA: return "CUDA error";
+        case MDP_EUNSUPPORTED: return "unsupported input";
+        case MDP_ENAN: return "NaN or Inf in a reduction";
+        case MDP_ETIMEOUT: return "device wait timed out";
+        default: return "unknown error";
+    }
+}
+
+// ============================================================== context
+extern "C" int mdp_context_create(int device, mdp_context **out) {
+    if (!out) return MDP_EINVAL;
+    *out = nullptr;
+    int ndev = 0;
+    MDP_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) {
+        mdp_set_error("device %d not present (%d devices)", device, ndev);
+        return MDP_EINVAL;
+    }
+    MDP_CUDA(cudaSetDevice(device));
+    mdp_context *ctx = new mdp_context();
+    ctx->device = device;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) ctx->sm_count = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        mdp_set_error("cudaStreamCreate failed");
+        return MDP_ECUDA;
+    }
+    ctx->own_stream = true;
+    if (cudaMallocHost(&ctx->h_pinned, 4096) != cudaSuccess) {
+        cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        mdp_set_error("cudaMallocHost failed");
+        return MDP_ENOMEM;
+    }
+    *out = ctx;
+    return MDP_OK;
+}
+
+extern "C" void mdp_context_destroy(mdp_context *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    delete ctx;
+}
+
+extern "C" int mdp_context_set_stream(mdp_context *ctx, void *cuda_stream) {
+    if (!ctx) return MDP_EINVAL;
+    MDP_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    if (cuda_stream) {
+        ctx->stream     = (cudaStream_t) cuda_stream;
+        ctx->own_stream = false;
+    } else {
+        MDP_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        ctx->own_stream = true;
+    }
+    return MDP_OK;
+}
+
+extern "C" void *mdp_context_stream(mdp_context *ctx) { return ctx ? (void *) ctx->stream : nullptr; }
+
+extern "C" int mdp_synchronize(mdp_context *ctx) {
+    if (!ctx) return MDP_EINVAL;
+    MDP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return MDP_OK;
+}
+
+extern "C" uint64_t mdp_launch_count(const mdp_context *ctx) { return ctx ? ctx->launches : 0; }
+
+// ============================================================== device-wide exclusive scan (uint32)
+// Three phases: per-tile totals, scan of the totals (recursively), rescan of
+// each tile with its offset.  Tiles of SCAN_TILE elements, one CTA per tile.
+#define SCAN_THREADS 256
+#define SCAN_ITEMS 16
+#define SCAN_TILE (SCAN_THREADS * SCAN_ITEMS)
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *total) {
+    __shared__ uint32_t warp_tot[SCAN_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t  x    = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = (lane < SCAN_THREADS / 32) ? warp_tot[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < SCAN_THREADS / 32) warp_tot[lane] = w;
+    }
+    __syncthreads();
+    uint32_t before = (warp > 0 ? warp_tot[warp - 1] : 0u) + x - v;
+    if (total) *total = warp_tot[SCAN_THREADS / 32 - 1];
+    __syncthreads();
+    return before;
+}
+
+__global__ void scan_tile_sums(const uint32_t *__restrict__ in, uint32_t *__restrict__ sums, int64_t n) {
+    int64_t  base = (int64_t) blockIdx.x * SCAN_TILE + (int64_t) threadIdx.x * SCAN_ITEMS;
+    uint32_t s    = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++)
+        if (base + i < n) s += in[base + i];
+    uint32_t tot;
+    block_exclusive_scan(s, &tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void scan_tile_apply(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
+                                const uint32_t *__restrict__ offs, int64_t n) {
+    int64_t  base = (int64_t) blockIdx.x * SCAN_TILE + (int64_t) threadIdx.x * SCAN_ITEMS;
+    uint32_t v[SCAN_ITEMS];
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++) {
+        v[i] = (base + i < n) ? in[base + i] : 0u;
+        s += v[i];
+    }
+    uint32_t run = block_exclusive_scan(s, nullptr) + (offs ? offs[blockIdx.x] : 0u);
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++) {
+        if (base + i < n) out[base + i] = run;
+        run += v[i];
+    }
+}
+
+int mdp_exclusive_scan_u32(mdp_context *ctx, const uint32_t *d_in, uint32_t *d_out, int64_t n,
+                           uint32_t *h_total) {
+    if (n <= 0) {
+        if (h_total) *h_total = 0;
+        return MDP_OK;
+    }
+    int64_t ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (ntiles == 1) {
+        scan_tile_apply<<<1, SCAN_THREADS, 0, ctx->stream>>>(d_in, d_out, nullptr, n);
+        MDP_CHECK_LAUNCH(ctx);
+    } else {
+        DevBuf sums, sums_scan;
+        MDP_TRY(sums.alloc(sizeof(uint32_t) * ntiles));
+        MDP_TRY(sums_scan.alloc(sizeof(uint32_t) * ntiles));
+        scan_tile_sums<<<(unsigned) ntiles, SCAN_THREADS, 0, ctx->stream>>>(d_in, sums.as<uint32_t>(), n);
+        MDP_CHECK_LAUNCH(ctx);
+        MDP_TRY(mdp_exclusive_scan_u32(ctx, sums.as<uint32_t>(), sums_scan.as<uint32_t>(), ntiles, nullptr));
+        scan_tile_apply<<<(unsigned) ntiles, SCAN_THREADS, 0, ctx->stream>>>(d_in, d_out, sums_scan.as<uint32_t>(),
+                                                                              n);
+        MDP_CHECK_LAUNCH(ctx);
+        MDP_CUDA(cudaStreamSynchronize(ctx->stream));  // sums freed at scope exit
+    }
+    if (h_total) {
+        uint32_t last_out = 0, last_in = 0;
+        MDP_CUDA(cudaMemcpyAsync(&last_out, d_out + n - 1, 4, cudaMemcpyDeviceToHost, ctx->stream));
+        MDP_CUDA(cudaMemcpyAsync(&last_in, d_in + n - 1, 4, cudaMemcpyDeviceToHost, ctx->stream));
+        MDP_CUDA(cudaStreamSynchronize(ctx->stream));
+        *h_total = last_out + last_in;
+    }
+    return MDP_OK;
+}
+
+// ============================================================== index compression
+__global__ void minmax_kernel(const int32_t *__restrict__ g, int64_t n, int32_t *__restrict__ out_min,
+                              int32_t *__restrict__ out_max) {
+    int32_t mn = INT32_MAX, mx = INT32_MIN;
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+        int32_t v = g[i];
+        mn        = min(mn, v);
+        mx        = max(mx, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    __shared__ int32_t smn[32], smx[32];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        smn[warp] = mn;
+        smx[warp] = mx;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        int nw = blockDim.x >> 5;
+        mn     = lane < nw ? smn[lane] : INT32_MAX;
+        mx     = lane < nw ? smx[lane] : INT32_MIN;
+        for (int o = 16; o > 0; o >>= 1) {
+            mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+            mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        }
+        if (lane == 0) {
+            out_min[blockIdx.x] = mn;
+            out_max[blockIdx.x] = mx;
+        }
+    }
+}
+
+__global__ void mark_kernel(const int32_t *__restrict__ g, int64_t n, int32_t gmin, uint32_t *__restrict__ flags) {
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        flags[(int64_t) g[i] - gmin] = 1u;
+}
+
+__global__ void lindices_kernel(const uint32_t *__restrict__ flags, const uint32_t *__restrict__ rank, int64_t range,
+                                int32_t gmin, int32_t *__restrict__ lind) {
+    for (int64_t v = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; v < range; v += (int64_t) gridDim.x * blockDim.x)
+        if (flags[v]) lind[rank[v]] = (int32_t) (v + gmin);
+}
+
+__global__ void localize_kernel(const int32_t *__restrict__ g, int64_t n, int32_t gmin,
+                                const uint32_t *__restrict__ rank, int32_t *__restrict__ local) {
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        local[i] = (int32_t) rank[(int64_t) g[i] - gmin];
+}
+
+// one map offset per row when every row is a consecutive triplet (3q, 3q+1, 3q+2)
+// of local indices, or a trash row (first local index 0 with a trash pixel)
+__global__ void triplet_kernel(const int32_t *__restrict__ g, int64_t m, int32_t gmin, const uint32_t *__restrict__ rank,
+                               int trash, int32_t *__restrict__ off, int *__restrict__ bad) {
+    int local_bad = 0;
+    for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t) gridDim.x * blockDim.x) {
+        int32_t l0 = (int32_t) rank[(int64_t) g[3 * t] - gmin];
+        if (trash && l0 == 0) {
+            off[t] = -1;
+            continue;
+        }
+        int32_t l1 = (int32_t) rank[(int64_t) g[3 * t + 1] - gmin];
+        int32_t l2 = (int32_t) rank[(int64_t) g[3 * t + 2] - gmin];
+        if (l1 != l0 + 1 || l2 != l0 + 2 || (l0 % 3) != 0) local_bad = 1;
+        off[t] = l0 - 3 * trash;
+    }
+    if (local_bad) atomicOr(bad, 1);
+}
+
+int mdp_pointing_create_ex(mdp_context *ctx, int64_t m, int nnz, const int32_t *d_g, const double *d_values,
+                           int32_t *d_local_out, mdp_pointing **out) {
+    if (!ctx || !out || m < 0 || nnz <= 0 || (m > 0 && (!d_g || !d_values))) {
+        mdp_set_error("mdp_pointing_create: invalid arguments");
+        return MDP_EINVAL;
+    }
+    *out = nullptr;
+    if (m == 0) {
+        mdp_set_error("mdp_pointing_create: empty pointing (m == 0)");
+        return MDP_EINVAL;
+    }
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    const int64_t n = m * (int64_t) nnz;
+    // 1. min / max
+    const int nb = 2 * ctx->sm_count;
+    DevBuf    mm;
+    MDP_TRY(mm.alloc(sizeof(int32_t) * 2 * nb));
+    minmax_kernel<<<nb, 512, 0, ctx->stream>>>(d_g, n, mm.as<int32_t>(), mm.as<int32_t>() + nb);
+    MDP_CHECK_LAUNCH(ctx);
+    std::vector<int32_t> hmm(2 * nb);
+    MDP_CUDA(cudaMemcpyAsync(hmm.data(), mm.p, sizeof(int32_t) * 2 * nb, cudaMemcpyDeviceToHost, ctx->stream));
+    MDP_CUDA(cudaStreamSynchronize(ctx->stream));
+    int32_t gmin = INT32_MAX, gmax = INT32_MIN;
+    for (int i = 0; i < nb; i++) {
+        gmin = std::min(gmin, hmm[i]);
+        gmax = std::max(gmax, hmm[nb + i]);
+    }
+    const int64_t range = (int64_t) gmax - gmin + 1;
+    // 2. presence flags over [min, max] (the counting sort's bitmap) and their ranks
+    DevBuf flags, rank;
+    MDP_TRY(flags.alloc(sizeof(uint32_t) * range));
+    MDP_TRY(rank.alloc(sizeof(uint32_t) * range));
+    MDP_CUDA(cudaMemsetAsync(flags.p, 0, sizeof(uint32_t) * range, ctx->stream));
+    mark_kernel<<<grid_for(n, 256, ctx->sm_count * 32), 256, 0, ctx->stream>>>(d_g, n, gmin, flags.as<uint32_t>());
+    MDP_CHECK_LAUNCH(ctx);
+    uint32_t lcount = 0;
+    MDP_TRY(mdp_exclusive_scan_u32(ctx, flags.as<uint32_t>(), rank.as<uint32_t>(), range, &lcount));
+
+    mdp_pointing *A = new mdp_pointing();
+    A->m            = m;
+    A->nnz          = nnz;
+    A->values       = d_values;
+    A->lcount       = lcount;
+    int rc          = A->lindices.alloc(sizeof(int32_t) * (size_t) lcount);
+    if (rc) {
+        delete A;
+        return rc;
+    }
+    lindices_kernel<<<grid_for(range, 256, ctx->sm_count * 32), 256, 0, ctx->stream>>>(
+            flags.as<uint32_t>(), rank.as<uint32_t>(), range, gmin, A->lindices.as<int32_t>());
+    A->trash_pix = gmin < 0 ? 1 : 0;  // lindices[0] == gmin
+    ctx->launches++;
+    // 3. per-row map offsets (triplet layout) or full local indices (general layout)
+    bool triplet = false;
+    if (nnz == 3) {
+        DevBuf bad;
+        if ((rc = A->off.alloc(sizeof(int32_t) * m)) || (rc = bad.alloc(sizeof(int)))) {
+            delete A;
+            return rc;
+        }
+        cudaMemsetAsync(bad.p, 0, sizeof(int), ctx->stream);
+        triplet_kernel<<<grid_for(m, 256, ctx->sm_count * 32), 256, 0, ctx->stream>>>(
+                d_g, m, gmin, rank.as<uint32_t>(), A->trash_pix, A->off.as<int32_t>(), bad.as<int>());
+        ctx->launches++;
+        int hbad = 1;
+        cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+            delete A;
+            mdp_set_error("pointing compression failed: %s", cudaGetErrorString(cudaGetLastError()));
+            return MDP_ECUDA;
+        }
+        triplet = (hbad == 0);
+        if (!triplet) A->off.release();
+    }
+    A->triplet = triplet ? 1 : 0;
+    int32_t *local = d_local_out;
+    if (!triplet) {
+        if ((rc = A->local.alloc(sizeof(int32_t) * n))) {
+            delete A;
+            return rc;
+        }
+        localize_kernel<<<grid_for(n, 256, ctx->sm_count * 32), 256, 0, ctx->stream>>>(d_g, n, gmin, rank.as<uint32_t>(),
+                                                                                      A->local.as<int32_t>());
+        ctx->launches++;
+        if (d_local_out)
+            cudaMemcpyAsync(d_local_out, A->local.p, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, ctx->stream);
+    } else if (local) {
+        localize_kernel<<<grid_for(n, 256, ctx->sm_count * 32), 256, 0, ctx->stream>>>(d_g, n, gmin, rank.as<uint32_t>(),
+                                                                                      local);
+        ctx->launches++;
+    }
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        delete A;
+        mdp_set_error("pointing compression: %s", cudaGetErrorString(e));
+        return MDP_ECUDA;
+    }
+    *out = A;
+    return MDP_OK;
+}
+
+extern "C" int mdp_pointing_create(mdp_context *ctx, int64_t m, int nnz, const int32_t *d_gindices,
+                                   const double *d_values, mdp_pointing **out) {
+    return mdp_pointing_create_ex(ctx, m, nnz, d_gindices, d_values, nullptr, out);
+}
+
+extern "C" void mdp_pointing_destroy(mdp_pointing *A) { delete A; }
+
+extern "C" int mdp_pointing_shape(const mdp_pointing *A, int64_t *lcount, int *trash_pix, int64_t *n_map,
+                                  int *triplet_layout) {
+    if (!A) return MDP_EINVAL;
+    if (lcount) *lcount = A->lcount;
+    if (trash_pix) *trash_pix = A->trash_pix;
+    if (n_map) *n_map = A->n_map();
+    if (triplet_layout) *triplet_layout = A->triplet;
+    return MDP_OK;
+}
+
+extern "C" int mdp_pointing_lindices(mdp_context *ctx, const mdp_pointing *A, int32_t *d_lindices) {
+    if (!ctx || !A || !d_lindices) return MDP_EINVAL;
+    MDP_CUDA(cudaMemcpyAsync(d_lindices, A->lindices.p, sizeof(int32_t) * A->lcount, cudaMemcpyDeviceToDevice,
+                             ctx->stream));
+    return MDP_OK;
+}
+
+// local indices of the triplet layout: 3q+j for valid rows, 0,1,2 for trash rows
+__global__ void expand_local_kernel(const int32_t *__restrict__ off, int64_t m, int trash, int32_t *__restrict__ local) {
+    for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t) gridDim.x * blockDim.x) {
+        int32_t o  = off[t];
+        int32_t l0 = (o < 0) ? 0 : o + 3 * trash;
+        local[3 * t] = l0;
+        local[3 * t + 1] = l0 + 1;
+        local[3 * t + 2] = l0 + 2;
+    }
+}
+
+extern "C" int mdp_pointing_local_indices(mdp_context *ctx, const mdp_pointing *A, int32_t *d_local) {
+    if (!ctx || !A || !d_local) return MDP_EINVAL;
+    if (!A->triplet) {
+        MDP_CUDA(cudaMemcpyAsync(d_local, A->local.p, sizeof(int32_t) * A->m * A->nnz, cudaMemcpyDeviceToDevice,
+                                 ctx->stream));
+        return MDP_OK;
+    }
+    expand_local_kernel<<<grid_for(A->m, 256, ctx->sm_count * 32), 256, 0, ctx->stream>>>(A->off.as<int32_t>(), A->m,
+                                                                                          A->trash_pix, d_local);
+    MDP_CHECK_LAUNCH(ctx);
+    return MDP_OK;
+}
+
+// ============================================================== y = P x
+// Triplet layout: 2 rows per thread so the 6 weights load as 3 aligned double2.
+__global__ void __launch_bounds__(256) matvec_triplet_kernel(const int32_t *__restrict__ off,
+                                                             const double *__restrict__ w,
+                                                             const double *__restrict__ x, double *__restrict__ y,
+                                                             int64_t m) {
+    const int64_t npair = m >> 1;
+    for (int64_t p = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; p < npair; p += (int64_t) gridDim.x * blockDim.x) {
+        const int2    o  = reinterpret_cast<const int2 *>(off)[p];
+        const double2 a  = reinterpret_cast<const double2 *>(w)[3 * p];
+        const double2 b  = reinterpret_cast<const double2 *>(w)[3 * p + 1];
+        const double2 c  = reinterpret_cast<const double2 *>(w)[3 * p + 2];
+        double        y0 = 0.0, y1 = 0.0;
+        if (o.x >= 0) y0 = a.x * __ldg(x + o.x) + a.y * __ldg(x + o.x + 1) + b.x * __ldg(x + o.x + 2);
+        if (o.y >= 0) y1 = b.y * __ldg(x + o.y) + c.x * __ldg(x + o.y + 1) + c.y * __ldg(x + o.y + 2);
+        reinterpret_cast<double2 *>(y)[p] = make_double2(y0, y1);
+    }
+    if ((m & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        int64_t t = m - 1;
+        int32_t o = off[t];
+        y[t]      = (o >= 0) ? w[3 * t] * x[o] + w[3 * t + 1] * x[o + 1] + w[3 * t + 2] * x[o + 2] : 0.0;
+    }
+}
+
+// General layout: the reference loop, row by row (mapmat.c:711-727)
+__global__ void matvec_general_kernel(const int32_t *__restrict__ local, const double *__restrict__ w,
+                                      const double *__restrict__ x, double *__restrict__ y, int64_t m, int nnz,
+                                      int trash) {
+    for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t) gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        if (trash) {
+            if (local[t * nnz] != 0)
+                for (int j = 0; j < nnz; j++) acc += w[t * nnz + j] * x[local[t * nnz + j] - nnz];
+        } else {
+            for (int j = 0; j < nnz; j++) acc += w[t * nnz + j] * x[local[t * nnz + j]];
+        }
+        y[t] = acc;
+    }
+}
+
+// Triplet layout, one row per thread, any alignment of w / y.
+__global__ void matvec_triplet_scalar_kernel(const int32_t *__restrict__ off, const double *__restrict__ w,
+                                             const double *__restrict__ x, double *__restrict__ y, int64_t m) {
+    for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t) gridDim.x * blockDim.x) {
+        const int32_t o = off[t];
+        y[t] = (o >= 0) ? w[3 * t] * x[o] + w[3 * t + 1] * x[o + 1] + w[3 * t + 2] * x[o + 2] : 0.0;
+    }
+}
+
+__global__ void trmatvec_triplet_scalar_kernel(const int32_t *__restrict__ off, const double *__restrict__ w,
+                                               const double *__restrict__ y, double *__restrict__ x, int64_t m) {
+    for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t) gridDim.x * blockDim.x) {
+        const int32_t o = off[t];
+        if (o < 0) continue;
+        const double v = y[t];
+        atomicAdd(x + o, w[3 * t] * v);
+        atomicAdd(x + o + 1, w[3 * t + 1] * v);
+        atomicAdd(x + o + 2, w[3 * t + 2] * v);
+    }
+}
+
+static inline bool aligned16(const void *a, const void *b) {
+    return (((uintptr_t) a | (uintptr_t) b) & 15u) == 0;
+}
+
+int mdp_matvec_launch(mdp_context *ctx, const mdp_pointing *A, const double *d_x, double *d_y) {
+    if (A->triplet && !aligned16(A->values, d_y)) {
+        matvec_triplet_scalar_kernel<<<grid_for(A->m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+                A->off.as<int32_t>(), A->values, d_x, d_y, A->m);
+    } else if (A->triplet) {
+        int64_t npair = A->m >> 1;
+        matvec_triplet_kernel<<<grid_for(npair > 0 ? npair : 1, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+                A->off.as<int32_t>(), A->values, d_x, d_y, A->m);
+    } else {
+        matvec_general_kernel<<<grid_for(A->m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+                A->local.as<int32_t>(), A->values, d_x, d_y, A->m, A->nnz, A->trash_pix);
+    }
+    MDP_CHECK_LAUNCH(ctx);
+    return MDP_OK;
+}
+
+extern "C" int mdp_matvec(mdp_context *ctx, const mdp_pointing *A, const double *d_x, double *d_y) {
+    if (!ctx || !A || !d_x || !d_y) return MDP_EINVAL;
+    return mdp_matvec_launch(ctx, A, d_x, d_y);
+}
+
+// ============================================================== x = P^T y
+// FP64 atomics into the (L2-resident) map.
+__global__ void __launch_bounds__(256) trmatvec_triplet_kernel(const int32_t *__restrict__ off,
+                                                               const double *__restrict__ w,
+                                                               const double *__restrict__ y, double *__restrict__ x,
+                                                               int64_t m) {
+    const int64_t npair = m >> 1;
+    for (int64_t p = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; p < npair; p += (int64_t) gridDim.x * blockDim.x) {
+        const int2    o  = reinterpret_cast<const int2 *>(off)[p];
+        const double2 yy = reinterpret_cast<const double2 *>(y)[p];
+        const double2 a  = reinterpret_cast<const double2 *>(w)[3 * p];
+        const double2 b  = reinterpret_cast<const double2 *>(w)[3 * p + 1];
+        const double2 c  = reinterpret_cast<const double2 *>(w)[3 * p + 2];
+        if (o.x >= 0) {
+            atomicAdd(x + o.x, a.x * yy.x);
+            atomicAdd(x + o.x + 1, a.y * yy.x);
+            atomicAdd(x + o.x + 2, b.x * yy.x);
+        }
+        if (o.y >= 0) {
+            atomicAdd(x + o.y, b.y * yy.y);
+            atomicAdd(x + o.y + 1, c.x * yy.y);
+            atomicAdd(x + o.y + 2, c.y * yy.y);
+        }
+    }
+    if ((m & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        int64_t t = m - 1;
+        int32_t o = off[t];
+        if (o >= 0)
+            for (int j = 0; j < 3; j++) atomicAdd(x + o + j, w[3 * t + j] * y[t]);
+    }
+}
+
+__global__ void trmatvec_general_kernel(const int32_t *__restrict__ local, const double *__restrict__ w,
+                                        const double *__restrict__ y, double *__restrict__ x, int64_t m, int nnz,
+                                        int trash) {
+    for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t) gridDim.x * blockDim.x) {
+        if (trash && local[t * nnz] == 0) continue;
+        for (int j = 0; j < nnz; j++) atomicAdd(x + local[t * nnz + j] - nnz * trash, w[t * nnz + j] * y[t]);
+    }
+}
+
+int mdp_trmatvec_launch(mdp_context *ctx, const mdp_pointing *A, const double *d_y, double *d_x) {
+    MDP_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * A->n_map(), ctx->stream));
+    if (A->triplet && !aligned16(A->values, d_y)) {
+        trmatvec_triplet_scalar_kernel<<<grid_for(A->m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+                A->off.as<int32_t>(), A->values, d_y, d_x, A->m);
+    } else if (A->triplet) {
+        int64_t npair = A->m >> 1;
+        trmatvec_triplet_kernel<<<grid_for(npair > 0 ? npair : 1, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+                A->off.as<int32_t>(), A->values, d_y, d_x, A->m);
+    } else {
+        trmatvec_general_kernel<<<grid_for(A->m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+                A->local.as<int32_t>(), A->values, d_y, d_x, A->m, A->nnz, A->trash_pix);
+    }
+    MDP_CHECK_LAUNCH(ctx);
+    return MDP_OK;
+}
+
+extern "C" int mdp_trmatvec(mdp_context *ctx, const mdp_pointing *A, const double *d_y, double *d_x) {
+    if (!ctx || !A || !d_x || !d_y) return MDP_EINVAL;
+    return mdp_trmatvec_launch(ctx, A, d_y, d_x);
+}

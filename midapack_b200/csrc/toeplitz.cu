@@ -1,0 +1,621 @@
+// Inverse-noise operator N^-1 on the device: per stationary block, remove the
+// block mean and apply the symmetric banded Toeplitz block.
+//
+// Reference: algebra/src/toeplitz/toeplitz_wizard.c:80-111 (stbmmProd: mean
+// removal then mpi_stbmm), toeplitz_block.c:115-636 (per-block dispatch),
+// toeplitz.c:298-367 (tpltz_init), 441-470 (circ_init_fftw: circulant
+// embedding c[0]=T[0], c[i]=c[bs-i]=T[i]), 731-865 (stmm_core overlap-save:
+// tile stride bs - 2(lambda-1), zero padding outside the block),
+// 569-616 (scmm_direct: forward FFT, spectrum product, inverse FFT).
+//
+// B200 design.  All tiles of all blocks run in one launch: one CTA (or one
+// thread-block cluster of C CTAs sharing the FFT through distributed shared
+// memory) per overlap-save tile.  A tile of N real samples is packed as N/2
+// complex points z[j] = x[2j] + i x[2j+1]; the complex FFT is an in-place
+// radix-2 decimation-in-frequency transform executed as radix-16 register
+// passes over shared memory (natural order in, bit-reversed out).  The real
+// FFT untangling, the product with the block's real even spectrum H and the
+// re-tangling for the inverse are fused into one pass over bit-reversed
+// pairs (k, M-k); the inverse is the mirror decimation-in-time transform with
+// conjugate twiddles (bit-reversed in, natural out).  No bit-reversal pass and
+// no global-memory round trip exist between the forward and inverse
+// transforms.  Spectra (N/2+1 doubles per distinct block row) and twiddles
+// (exp(-2 pi i k/N), computed on the host in long double) are built once.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+
+#include "mdp_internal.cuh"
+
+namespace cg = cooperative_groups;
+
+// ------------------------------------------------------------------ complex helpers
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
+    return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+// DIF stages of a radix-R register set.  Element i of the set sits at group
+// position q + i*(L/R) inside a DIF group of size L.  Stage j (group L/2^j,
+// span L/2^(j+1)) pairs i and i + R/2^(j+1); the difference is multiplied by
+// W_{L_j}^{pos} = tw[pos * (N / L_j)], tw[k] = exp(-2 pi i k / N).
+template <int R>
+__device__ __forceinline__ void dif_set(double2 (&v)[R], int L, int q, int logN_over_L, const double2 *__restrict__ tw) {
+#pragma unroll
+    for (int j = 0, sub = R; sub > 1; j++, sub >>= 1) {
+        const int half = sub >> 1;
+        const int shift = logN_over_L + j;  // N / L_j = 2^shift
+#pragma unroll
+        for (int i = 0; i < R; i++) {
+            if ((i % sub) < half) {
+                const int     pos = q + (i % sub) * (L / R);
+                const double2 a = v[i], b = v[i + half];
+                v[i] = cadd(a, b);
+                const double2 d = csub(a, b);
+                v[i + half] = (pos == 0) ? d : cmul(d, __ldg(tw + ((int64_t) pos << shift)));
+            }
+        }
+    }
+}
+
+// exact mirror of dif_set with conjugate twiddles (decimation in time)
+template <int R>
+__device__ __forceinline__ void dit_set(double2 (&v)[R], int L, int q, int logN_over_L, const double2 *__restrict__ tw) {
+    int j = 0;
+    for (int sub = R; sub > 2; sub >>= 1) j++;
+#pragma unroll
+    for (int sub = 2; sub <= R; sub <<= 1, j--) {
+        const int half = sub >> 1;
+        const int shift = logN_over_L + j;
+#pragma unroll
+        for (int i = 0; i < R; i++) {
+            if ((i % sub) < half) {
+                const int     pos = q + (i % sub) * (L / R);
+                const double2 a = v[i];
+                const double2 t = (pos == 0) ? v[i + half] : cmulc(v[i + half], __ldg(tw + ((int64_t) pos << shift)));
+                v[i] = cadd(a, t);
+                v[i + half] = csub(a, t);
+            }
+        }
+    }
+}
+
+// one local pass of R = 2^k stages starting at group size L over smem s[0..ML)
+template <int R, bool INVERSE>
+__device__ __forceinline__ void local_pass(double2 *s, int ML, int L, int logN_over_L, const double2 *__restrict__ tw) {
+    const int nsets = ML / R;
+    const int stride = L / R;
+    for (int set = threadIdx.x; set < nsets; set += blockDim.x) {
+        const int g = set / stride, q = set - g * stride;
+        double2  *base = s + g * L + q;
+        double2   v[R];
+#pragma unroll
+        for (int i = 0; i < R; i++) v[i] = base[i * stride];
+        if (INVERSE) dit_set<R>(v, L, q, logN_over_L, tw);
+        else dif_set<R>(v, L, q, logN_over_L, tw);
+#pragma unroll
+        for (int i = 0; i < R; i++) base[i * stride] = v[i];
+    }
+    __syncthreads();
+}
+
+template <bool INVERSE>
+__device__ __forceinline__ void local_fft(double2 *s, int logML, int logN, const double2 *__restrict__ tw) {
+    // stages grouped 4 at a time, largest groups first (forward) / last (inverse)
+    int ks[8], Ls[8], np = 0;
+    for (int rem = logML, L = 1 << logML; rem > 0;) {
+        int k = rem >= 4 ? 4 : rem;
+        ks[np] = k;
+        Ls[np] = L;
+        np++;
+        L >>= k;
+        rem -= k;
+    }
+    const int ML = 1 << logML;
+    for (int pi = 0; pi < np; pi++) {
+        const int p = INVERSE ? (np - 1 - pi) : pi;
+        const int L = Ls[p];
+        int       logL = 0;
+        while ((1 << logL) < L) logL++;
+        const int lno = logN - logL;
+        switch (ks[p]) {
+            case 4: local_pass<16, INVERSE>(s, ML, L, lno, tw); break;
+            case 3: local_pass<8, INVERSE>(s, ML, L, lno, tw); break;
+            case 2: local_pass<4, INVERSE>(s, ML, L, lno, tw); break;
+            default: local_pass<2, INVERSE>(s, ML, L, lno, tw); break;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ the tile kernel
+struct TileArgs {
+    const double  *vin;
+    double        *vout;
+    const int64_t *tile_start;  // first output row of the tile (global)
+    const int32_t *tile_block;
+    const int64_t *blk_start;
+    const int32_t *blk_len;
+    const int32_t *blk_spec;
+    const double  *spectra;     // [n_spec][M+1]
+    const double2 *tw;          // [M]
+    const double  *means;       // [nb] or nullptr
+    int            lambda;
+};
+
+template <int LOG_ML, int C>
+__global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgs a) {
+    extern __shared__ __align__(16) double2 smem[];
+    constexpr int ML = 1 << LOG_ML;
+    constexpr int M = ML * C;       // complex points per tile
+    constexpr int N = 2 * M;        // real samples per tile
+    int           logM = LOG_ML;
+    for (int c = C; c > 1; c >>= 1) logM++;
+    const int logN = logM + 1;
+
+    const int     rank = (C > 1) ? (int) (blockIdx.x % C) : 0;
+    const int64_t tile = (C > 1) ? (int64_t) (blockIdx.x / C) : (int64_t) blockIdx.x;
+    const int     blk = a.tile_block[tile];
+    const int64_t bs = a.blk_start[blk];
+    const int64_t be = bs + a.blk_len[blk];
+    const int64_t t0 = a.tile_start[tile];
+    const int     halo = a.lambda - 1;
+    const int64_t ws = t0 - halo;               // window start (row of x[0])
+    const int     E = N - 2 * halo;            // outputs per tile
+    const double  mu = a.means ? a.means[blk] : 0.0;
+
+    // ---- load this CTA's 2*ML real samples of the window (zero outside the block)
+    double       *sd = reinterpret_cast<double *>(smem);
+    const int64_t r0 = ws + (int64_t) rank * 2 * ML;
+    for (int j = threadIdx.x; j < 2 * ML; j += blockDim.x) {
+        const int64_t row = r0 + j;
+        sd[j] = (row >= bs && row < be) ? (__ldg(a.vin + row) - mu) : 0.0;
+    }
+
+    if constexpr (C > 1) {
+        cg::cluster_group cluster = cg::this_cluster();
+        cluster.sync();
+        // cross-CTA DIF stages: set q holds element c of CTA c at local q
+        for (int q = rank * (ML / C) + threadIdx.x; q < (rank + 1) * (ML / C); q += blockDim.x) {
+            double2 v[C];
+#pragma unroll
+            for (int c = 0; c < C; c++) v[c] = cluster.map_shared_rank(smem, c)[q];
+            dif_set<C>(v, M, q, 1, a.tw);
+#pragma unroll
+            for (int c = 0; c < C; c++) cluster.map_shared_rank(smem, c)[q] = v[c];
+        }
+        cluster.sync();
+    } else {
+        __syncthreads();
+    }
+
+    local_fft<false>(smem, LOG_ML, logN, a.tw);
+
+    if constexpr (C > 1) cg::this_cluster().sync();
+
+    // ---- real-FFT untangle, spectrum product, re-tangle (bit-reversed storage)
+    const double *H = a.spectra + (int64_t) a.blk_spec[blk] * (M + 1);
+    for (int p = threadIdx.x; p < ML; p += blockDim.x) {
+        const int P1 = rank * ML + p;
+        const int k = (int) (__brev((unsigned) P1) >> (32 - logM));
+        if (k > M / 2) continue;
+        const int k2 = (M - k) & (M - 1);
+        const int P2 = (int) (__brev((unsigned) k2) >> (32 - logM));
+        double2  *s1 = smem + p;
+        double2  *s2;
+        if constexpr (C > 1) s2 = cg::this_cluster().map_shared_rank(smem, P2 / ML) + (P2 % ML);
+        else s2 = smem + P2;
+        const double2 Z1 = *s1, Z2 = *s2;
+        const double2 E0 = make_double2(0.5 * (Z1.x + Z2.x), 0.5 * (Z1.y - Z2.y));
+        const double2 O0 = make_double2(0.5 * (Z1.y + Z2.y), -0.5 * (Z1.x - Z2.x));
+        const double  Hk = __ldg(H + k), Hm = __ldg(H + (M - k));
+        const double  ca = 0.5 * (Hk + Hm), cb = 0.5 * (Hk - Hm);
+        const double2 w = __ldg(a.tw + k);
+        const double2 wO = cmul(w, O0);
+        const double2 Ep = make_double2(ca * E0.x + cb * wO.x, ca * E0.y + cb * wO.y);
+        const double2 cE = cmulc(E0, w);  // conj(w) * E
+        const double2 Op = make_double2(cb * cE.x + ca * O0.x, cb * cE.y + ca * O0.y);
+        *s1 = make_double2(Ep.x - Op.y, Ep.y + Op.x);
+        if (P2 != P1) *s2 = make_double2(Ep.x + Op.y, -Ep.y + Op.x);
+    }
+
+    if constexpr (C > 1) cg::this_cluster().sync();
+    else __syncthreads();
+
+    local_fft<true>(smem, LOG_ML, logN, a.tw);
+
+    if constexpr (C > 1) {
+        cg::cluster_group cluster = cg::this_cluster();
+        cluster.sync();
+        for (int q = rank * (ML / C) + threadIdx.x; q < (rank + 1) * (ML / C); q += blockDim.x) {
+            double2 v[C];
+#pragma unroll
+            for (int c = 0; c < C; c++) v[c] = cluster.map_shared_rank(smem, c)[q];
+            dit_set<C>(v, M, q, 1, a.tw);
+#pragma unroll
+            for (int c = 0; c < C; c++) cluster.map_shared_rank(smem, c)[q] = v[c];
+        }
+        cluster.sync();
+    }
+
+    // ---- store the tile's central outputs, scaled by 1/M
+    const double  scale = 1.0 / (double) M;
+    const int64_t out_end = min(t0 + (int64_t) E, be);
+    for (int j = threadIdx.x; j < 2 * ML; j += blockDim.x) {
+        const int64_t row = r0 + j;
+        if (row >= t0 && row < out_end) a.vout[row] = sd[j] * scale;
+    }
+}
+
+// ------------------------------------------------------------------ spectra
+// H[k] = T0 + 2 sum_{i<lambda} T[i] cos(2 pi i k / N), k = 0..N/2: the DFT of
+// the circulant embedding, which is real and even.
+__global__ void spectrum_kernel(const double *__restrict__ T, int lambda, int N, const double2 *__restrict__ tw,
+                                double *__restrict__ H) {
+    const int M = N / 2;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= M; k += gridDim.x * blockDim.x) {
+        double acc = 0.0, comp = 0.0;  // Kahan-compensated sum of the cosine terms
+        for (int i = 1; i < lambda; i++) {
+            const int64_t e = ((int64_t) i * k) % N;
+            // cos(2 pi e / N) from the half-period table (tw covers e < N/2)
+            const double  c = (e < M) ? tw[e].x : -tw[e - M].x;
+            const double  y = T[i] * c - comp;
+            const double  t = acc + y;
+            comp = (t - acc) - y;
+            acc = t;
+        }
+        H[k] = T[0] + 2.0 * acc;
+    }
+}
+
+// ------------------------------------------------------------------ block means and white noise
+__global__ void block_partial_sums(const double *__restrict__ v, const int64_t *__restrict__ chunk_start,
+                                   const int32_t *__restrict__ chunk_len, double *__restrict__ partial) {
+    const int64_t s = chunk_start[blockIdx.x];
+    const int     n = chunk_len[blockIdx.x];
+    double        acc = 0.0;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) acc += v[s + j];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    __shared__ double ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double x = (threadIdx.x < (blockDim.x >> 5)) ? ws[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (threadIdx.x == 0) partial[blockIdx.x] = x;
+    }
+}
+
+__global__ void block_means_final(const double *__restrict__ partial, const int32_t *__restrict__ blk_chunk0,
+                                  const int32_t *__restrict__ blk_nchunk, const int32_t *__restrict__ blk_len,
+                                  int nb, double *__restrict__ means) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int c = 0; c < blk_nchunk[b]; c++) s += partial[blk_chunk0[b] + c];
+        means[b] = s / (double) blk_len[b];
+    }
+}
+
+__global__ void white_kernel(const double *__restrict__ vin, double *__restrict__ vout, const int64_t *__restrict__ bstart,
+                             const int32_t *__restrict__ blen, const double *__restrict__ t0, int nb) {
+    const int b = blockIdx.y;
+    const int64_t s = bstart[b];
+    const int n = blen[b];
+    const double d = t0[b];
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) vout[s + j] = d * vin[s + j];
+}
+
+// ------------------------------------------------------------------ plan
+struct NoiseExtra {
+    DevBuf chunk_start, chunk_len, blk_chunk0, blk_nchunk, partial;
+    int    n_chunks = 0;
+    bool   covers_all = true;
+};
+static std::map<const mdp_noise *, NoiseExtra *> g_extra;
+
+static int choose_fft(int lambda, int64_t max_block, int *log_ml, int *cluster) {
+    const char *env = getenv("MDP_TOEPLITZ_FFT");  // force the real tile size N (power of two)
+    int         forced = env ? atoi(env) : 0;
+    double      best = 1e300;
+    int         bl = -1, bc = 1;
+    for (int C = 1; C <= 8; C <<= 1)
+        for (int lml = 6; lml <= 13; lml++) {
+            if (C > 1 && lml != 13) continue;
+            const int64_t N = 2LL * C * (1LL << lml);
+            const int64_t E = N - 2LL * (lambda - 1);
+            if (E < 1) continue;
+            if (forced && N != forced) continue;
+            int logN = lml + 1;
+            for (int c = C; c > 1; c >>= 1) logN++;
+            // FFT work per useful output, a penalty for cluster traffic, and a
+            // penalty when a tile is much larger than the blocks it covers
+            double eff = (double) std::min<int64_t>(E, max_block);
+            double cost = (double) N / eff * (logN + 3) + (C > 1 ? 3.0 * std::log2((double) C) : 0.0);
+            if (E < N / 4 && !forced) cost *= 1.5;
+            if (cost < best) {
+                best = cost;
+                bl = lml;
+                bc = C;
+            }
+        }
+    if (bl < 0) return MDP_EUNSUPPORTED;
+    *log_ml = bl;
+    *cluster = bc;
+    return MDP_OK;
+}
+
+typedef void (*tile_fn)(TileArgs);
+static tile_fn pick_kernel(int log_ml, int C) {
+    if (C == 1) switch (log_ml) {
+            case 6: return toeplitz_tile_kernel<6, 1>;
+            case 7: return toeplitz_tile_kernel<7, 1>;
+            case 8: return toeplitz_tile_kernel<8, 1>;
+            case 9: return toeplitz_tile_kernel<9, 1>;
+            case 10: return toeplitz_tile_kernel<10, 1>;
+            case 11: return toeplitz_tile_kernel<11, 1>;
+            case 12: return toeplitz_tile_kernel<12, 1>;
+            case 13: return toeplitz_tile_kernel<13, 1>;
+        }
+    if (log_ml == 13) switch (C) {
+            case 2: return toeplitz_tile_kernel<13, 2>;
+            case 4: return toeplitz_tile_kernel<13, 4>;
+            case 8: return toeplitz_tile_kernel<13, 8>;
+        }
+    return nullptr;
+}
+
+extern "C" int mdp_noise_create(mdp_context *ctx, int nb_blocks, const int64_t *h_idv, const int32_t *h_n, int lambda,
+                                const double *h_T, mdp_noise **out) {
+    if (!ctx || !out || nb_blocks <= 0 || !h_idv || !h_n || !h_T || lambda < 1) {
+        mdp_set_error("mdp_noise_create: invalid arguments");
+        return MDP_EINVAL;
+    }
+    *out = nullptr;
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    int64_t max_block = 0;
+    for (int b = 0; b < nb_blocks; b++) {
+        if (h_n[b] < 0 || h_idv[b] < 0) {
+            mdp_set_error("mdp_noise_create: negative block size or offset (block %d)", b);
+            return MDP_EINVAL;
+        }
+        if (b > 0 && h_idv[b] < h_idv[b - 1] + h_n[b - 1]) {
+            mdp_set_error("mdp_noise_create: blocks must be sorted and disjoint (block %d)", b);
+            return MDP_EINVAL;
+        }
+        if (lambda > 1 && h_n[b] > 0 && h_n[b] < lambda - 1) {
+            // the reference rejects this case in stmm_main (toeplitz.c:948-949, error 1)
+            mdp_set_error("mdp_noise_create: Toeplitz band width > block size (block %d: n=%d, lambda=%d)", b, h_n[b],
+                          lambda);
+            return MDP_EINVAL;
+        }
+        max_block = std::max<int64_t>(max_block, h_n[b]);
+    }
+    mdp_noise *N = new mdp_noise();
+    NoiseExtra *X = new NoiseExtra();
+    N->nb = nb_blocks;
+    N->lambda = lambda;
+    N->h_idv.assign(h_idv, h_idv + nb_blocks);
+    N->h_n.assign(h_n, h_n + nb_blocks);
+    N->h_T0.resize(nb_blocks);
+    int64_t expect = 0;
+    for (int b = 0; b < nb_blocks; b++) {
+        N->h_T0[b] = h_T[(size_t) b * lambda];
+        if (h_idv[b] != expect) X->covers_all = false;
+        expect = h_idv[b] + h_n[b];
+    }
+    N->nrow_end = expect;
+    auto fail = [&](int rc) {
+        delete X;
+        delete N;
+        return rc;
+    };
+    int rc;
+    std::vector<int32_t> h_len(N->h_n);
+    if ((rc = N->blk_start.alloc(8 * nb_blocks)) || (rc = N->blk_len.alloc(4 * nb_blocks)) ||
+        (rc = N->blk_t0.alloc(8 * nb_blocks)) || (rc = N->means.alloc(8 * nb_blocks)) ||
+        (rc = N->blk_spec.alloc(4 * nb_blocks)))
+        return fail(rc);
+    cudaMemcpy(N->blk_start.p, h_idv, 8 * nb_blocks, cudaMemcpyHostToDevice);
+    cudaMemcpy(N->blk_len.p, h_n, 4 * nb_blocks, cudaMemcpyHostToDevice);
+    cudaMemcpy(N->blk_t0.p, N->h_T0.data(), 8 * nb_blocks, cudaMemcpyHostToDevice);
+
+    // chunks for the deterministic block-mean reduction
+    const int            CH = 1 << 16;
+    std::vector<int64_t> cs;
+    std::vector<int32_t> cl, c0(nb_blocks), cn(nb_blocks);
+    for (int b = 0; b < nb_blocks; b++) {
+        c0[b] = (int32_t) cs.size();
+        for (int64_t o = 0; o < h_n[b]; o += CH) {
+            cs.push_back(h_idv[b] + o);
+            cl.push_back((int32_t) std::min<int64_t>(CH, h_n[b] - o));
+        }
+        cn[b] = (int32_t) cs.size() - c0[b];
+    }
+    X->n_chunks = (int) cs.size();
+    if ((rc = X->chunk_start.alloc(8 * std::max<size_t>(cs.size(), 1))) ||
+        (rc = X->chunk_len.alloc(4 * std::max<size_t>(cl.size(), 1))) || (rc = X->blk_chunk0.alloc(4 * nb_blocks)) ||
+        (rc = X->blk_nchunk.alloc(4 * nb_blocks)) || (rc = X->partial.alloc(8 * std::max<size_t>(cs.size(), 1))))
+        return fail(rc);
+    if (!cs.empty()) {
+        cudaMemcpy(X->chunk_start.p, cs.data(), 8 * cs.size(), cudaMemcpyHostToDevice);
+        cudaMemcpy(X->chunk_len.p, cl.data(), 4 * cl.size(), cudaMemcpyHostToDevice);
+    }
+    cudaMemcpy(X->blk_chunk0.p, c0.data(), 4 * nb_blocks, cudaMemcpyHostToDevice);
+    cudaMemcpy(X->blk_nchunk.p, cn.data(), 4 * nb_blocks, cudaMemcpyHostToDevice);
+
+    if (lambda > 1) {
+        if ((rc = choose_fft(lambda, max_block, &N->log2_ml, &N->cluster))) {
+            mdp_set_error("mdp_noise_create: no FFT tile fits lambda=%d", lambda);
+            return fail(rc);
+        }
+        const int M = N->cluster << N->log2_ml;
+        N->fft_n = 2 * M;
+        const int64_t E = (int64_t) N->fft_n - 2LL * (lambda - 1);
+        std::vector<int64_t> ts;
+        std::vector<int32_t> tb;
+        for (int b = 0; b < nb_blocks; b++)
+            for (int64_t o = 0; o < h_n[b]; o += E) {
+                ts.push_back(h_idv[b] + o);
+                tb.push_back(b);
+            }
+        N->n_tiles = (int64_t) ts.size();
+        if ((rc = N->tile_start.alloc(8 * std::max<size_t>(ts.size(), 1))) ||
+            (rc = N->tile_block.alloc(4 * std::max<size_t>(tb.size(), 1))))
+            return fail(rc);
+        if (!ts.empty()) {
+            cudaMemcpy(N->tile_start.p, ts.data(), 8 * ts.size(), cudaMemcpyHostToDevice);
+            cudaMemcpy(N->tile_block.p, tb.data(), 4 * tb.size(), cudaMemcpyHostToDevice);
+        }
+        // twiddles exp(-2 pi i k / N), k < N/2, in long double then rounded
+        std::vector<double2> tw(M);
+        for (int k = 0; k < M; k++) {
+            long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double) k / (long double) N->fft_n;
+            tw[k] = make_double2((double) cosl(ang), (double) sinl(ang));
+        }
+        if ((rc = N->twiddle.alloc(sizeof(double2) * M))) return fail(rc);
+        cudaMemcpy(N->twiddle.p, tw.data(), sizeof(double2) * M, cudaMemcpyHostToDevice);
+        // distinct block rows share one spectrum
+        std::vector<int32_t> spec_of(nb_blocks);
+        std::vector<int>     uniq;
+        for (int b = 0; b < nb_blocks; b++) {
+            int found = -1;
+            for (size_t u = 0; u < uniq.size(); u++)
+                if (!memcmp(h_T + (size_t) uniq[u] * lambda, h_T + (size_t) b * lambda, sizeof(double) * lambda)) {
+                    found = (int) u;
+                    break;
+                }
+            if (found < 0) {
+                found = (int) uniq.size();
+                uniq.push_back(b);
+            }
+            spec_of[b] = found;
+        }
+        N->n_spec = (int) uniq.size();
+        cudaMemcpy(N->blk_spec.p, spec_of.data(), 4 * nb_blocks, cudaMemcpyHostToDevice);
+        if ((rc = N->spectra.alloc(sizeof(double) * (size_t) N->n_spec * (M + 1)))) return fail(rc);
+        DevBuf dT;
+        if ((rc = dT.alloc(sizeof(double) * lambda))) return fail(rc);
+        for (int u = 0; u < N->n_spec; u++) {
+            cudaMemcpy(dT.p, h_T + (size_t) uniq[u] * lambda, sizeof(double) * lambda, cudaMemcpyHostToDevice);
+            spectrum_kernel<<<grid_for(M + 1, 128, 4096), 128, 0, ctx->stream>>>(
+                    dT.as<double>(), lambda, N->fft_n, N->twiddle.as<double2>(),
+                    N->spectra.as<double>() + (size_t) u * (M + 1));
+            ctx->launches++;
+            cudaStreamSynchronize(ctx->stream);
+        }
+        tile_fn fn = pick_kernel(N->log2_ml, N->cluster);
+        size_t  smem = sizeof(double2) << N->log2_ml;
+        cudaFuncSetAttribute((const void *) fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        if (N->cluster > 1) cudaFuncSetAttribute((const void *) fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    }
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        mdp_set_error("mdp_noise_create: %s", cudaGetErrorString(e));
+        return fail(MDP_ECUDA);
+    }
+    g_extra[N] = X;
+    *out = N;
+    return MDP_OK;
+}
+
+extern "C" void mdp_noise_destroy(mdp_noise *N) {
+    if (!N) return;
+    auto it = g_extra.find(N);
+    if (it != g_extra.end()) {
+        delete it->second;
+        g_extra.erase(it);
+    }
+    delete N;
+}
+
+extern "C" int mdp_noise_tile(const mdp_noise *N, int *fft_size, int *cluster_ctas, int64_t *n_tiles) {
+    if (!N) return MDP_EINVAL;
+    if (fft_size) *fft_size = N->fft_n;
+    if (cluster_ctas) *cluster_ctas = N->cluster;
+    if (n_tiles) *n_tiles = N->n_tiles;
+    return MDP_OK;
+}
+
+int mdp_block_means(mdp_context *ctx, const mdp_noise *N, const double *d_v, double *d_means) {
+    NoiseExtra *X = g_extra.at(N);
+    if (X->n_chunks == 0) {
+        MDP_CUDA(cudaMemsetAsync(d_means, 0, 8 * N->nb, ctx->stream));
+        return MDP_OK;
+    }
+    block_partial_sums<<<X->n_chunks, 512, 0, ctx->stream>>>(d_v, X->chunk_start.as<int64_t>(),
+                                                             X->chunk_len.as<int32_t>(), X->partial.as<double>());
+    MDP_CHECK_LAUNCH(ctx);
+    block_means_final<<<grid_for(N->nb, 128, 1024), 128, 0, ctx->stream>>>(
+            X->partial.as<double>(), X->blk_chunk0.as<int32_t>(), X->blk_nchunk.as<int32_t>(), N->blk_len.as<int32_t>(),
+            N->nb, d_means);
+    MDP_CHECK_LAUNCH(ctx);
+    return MDP_OK;
+}
+
+// out = N^-1 in (in != out required); d_means: precomputed block means or nullptr to compute here
+int mdp_stbmm_impl(mdp_context *ctx, const mdp_noise *N, const double *d_in, double *d_out, const double *d_means) {
+    NoiseExtra *X = g_extra.at(N);
+    if (!X->covers_all)
+        MDP_CUDA(cudaMemcpyAsync(d_out, d_in, sizeof(double) * N->nrow_end, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (N->lambda == 1) {
+        dim3 grid(std::max(1, std::min(64, (int) ((N->h_n.empty() ? 1 : N->h_n[0]) / 256 + 1))), N->nb);
+        white_kernel<<<grid, 256, 0, ctx->stream>>>(d_in, d_out, N->blk_start.as<int64_t>(), N->blk_len.as<int32_t>(),
+                                                    N->blk_t0.as<double>(), N->nb);
+        MDP_CHECK_LAUNCH(ctx);
+        return MDP_OK;
+    }
+    if (!d_means) {
+        MDP_TRY(mdp_block_means(ctx, N, d_in, N->means.as<double>()));
+        d_means = N->means.as<double>();
+    }
+    if (N->n_tiles == 0) return MDP_OK;
+    TileArgs a;
+    a.vin = d_in;
+    a.vout = d_out;
+    a.tile_start = N->tile_start.as<int64_t>();
+    a.tile_block = N->tile_block.as<int32_t>();
+    a.blk_start = N->blk_start.as<int64_t>();
+    a.blk_len = N->blk_len.as<int32_t>();
+    a.blk_spec = N->blk_spec.as<int32_t>();
+    a.spectra = N->spectra.as<double>();
+    a.tw = N->twiddle.as<double2>();
+    a.means = d_means;
+    a.lambda = N->lambda;
+    tile_fn  fn = pick_kernel(N->log2_ml, N->cluster);
+    size_t   smem = sizeof(double2) << N->log2_ml;
+    int      threads = std::min(512, std::max(64, (1 << N->log2_ml) / 16));
+    if (N->n_tiles * N->cluster > 0x7fffffffLL) return MDP_EUNSUPPORTED;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned) (N->n_tiles * N->cluster));
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = N->cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    MDP_CUDA(cudaLaunchKernelEx(&cfg, fn, a));
+    MDP_CHECK_LAUNCH(ctx);
+    return MDP_OK;
+}
+
+extern "C" int mdp_stbmm(mdp_context *ctx, const mdp_noise *N, const double *d_in, double *d_out) {
+    if (!ctx || !N || !d_in || !d_out) return MDP_EINVAL;
+    const double *src = d_in;
+    if (d_in == d_out) {
+        MDP_TRY(ctx->scratch.alloc(sizeof(double) * N->nrow_end));
+        MDP_CUDA(cudaMemcpyAsync(ctx->scratch.p, d_in, sizeof(double) * N->nrow_end, cudaMemcpyDeviceToDevice,
+                                 ctx->stream));
+        src = ctx->scratch.as<double>();
+    }
+    return mdp_stbmm_impl(ctx, N, src, d_out, nullptr);
+}

@@ -1,0 +1,109 @@
+"""N^-1 (block mean removal + banded Toeplitz, overlap-save FFT) on the GPU vs
+the oracle's exact long-double banded product.  Tolerance: 1e-12 norm-wise
+relative per application (FP64)."""
+import os
+
+import numpy as np
+import pytest
+
+from midapack_b200 import synth
+from oracle import restate as R
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def _run(gpu_ctx, block_sizes, lam, invtt, v, fft=None):
+    import torch
+    import midapack_b200 as mb
+    old = os.environ.get("MDP_TOEPLITZ_FFT")
+    if fft:
+        os.environ["MDP_TOEPLITZ_FFT"] = str(fft)
+    try:
+        N = mb.Noise(gpu_ctx, block_sizes, lam, invtt)
+    finally:
+        if fft:
+            if old is None:
+                del os.environ["MDP_TOEPLITZ_FFT"]
+            else:
+                os.environ["MDP_TOEPLITZ_FFT"] = old
+    vin = torch.from_numpy(v).cuda()
+    vout = torch.empty_like(vin)
+    N.apply(vin, vout)
+    torch.cuda.synchronize()
+    return vout.cpu().numpy(), N.tile()
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("lam,sizes,fft", [
+    (1, [100, 37], None),            # white noise: diagonal scaling, no mean removal
+    (2, [50, 9, 64], None),
+    (16, [1000, 333], None),
+    (64, [4096, 777, 130], None),     # ragged blocks, one shorter than a tile
+    (300, [5000, 600], None),         # lambda not a power of two
+    (100, [3000], 512),               # forced small tile: many tiles per block
+    (2048, [20000, 4100], None),
+    (4096, [40000], 16384),           # largest single-CTA tile
+    (4096, [40000, 9000], 32768),     # 2-CTA cluster tile (distributed shared memory)
+    (8192, [24000, 24000], None),     # the reference fixture's shape
+    (8192, [70000], 65536),           # 4-CTA cluster tile
+    (16384, [140000], 131072),        # 8-CTA cluster tile
+])
+def test_stbmm_vs_exact(gpu_ctx, lam, sizes, fft):
+    rng = np.random.default_rng(lam + len(sizes))
+    t = np.zeros(lam)
+    t[0] = 2.0
+    if lam > 1:
+        t[1:] = rng.standard_normal(lam - 1) * np.exp(-np.arange(1, lam) / (0.3 * lam))
+    invtt = np.tile(t, len(sizes))
+    v = rng.standard_normal(int(sum(sizes))) + 3.0
+    out, tile = _run(gpu_ctx, sizes, lam, invtt, v, fft)
+    ref = R.stbmm(v, np.array(sizes), lam, invtt, exact=True)
+    assert _rel(out, ref) < TOL, (tile, _rel(out, ref))
+
+
+def test_stbmm_distinct_blocks(gpu_ctx):
+    """Blocks with different first rows get their own spectra."""
+    rng = np.random.default_rng(4)
+    lam, sizes = 128, [3000, 2500, 4000]
+    invtt = np.concatenate([synth.invtt_row(4096, lam, fk) for fk in (0.1, 1.0, 5.0)])
+    v = rng.standard_normal(sum(sizes))
+    out, _ = _run(gpu_ctx, sizes, lam, invtt, v)
+    ref = R.stbmm(v, np.array(sizes), lam, invtt, exact=True)
+    assert _rel(out, ref) < TOL
+
+
+def test_stbmm_noise_model_full_block(gpu_ctx):
+    """The 1/f inverse-noise row of the 2^20-sample, lambda 2^12 workload, one block,
+    against the oracle's FFT product (exact within FP64 rounding)."""
+    n, lam = 1 << 20, 1 << 12
+    row = synth.invtt_row(n, lam, 1.0)
+    rng = np.random.default_rng(9)
+    v = synth.noise_tod(n, 1.0, rng)
+    out, tile = _run(gpu_ctx, [n], lam, row, v)
+    ref = R.stbmm(v, np.array([n]), lam, row)
+    assert _rel(out, ref) < TOL, tile
+
+
+def test_stbmm_in_place(gpu_ctx):
+    import torch
+    import midapack_b200 as mb
+    rng = np.random.default_rng(2)
+    lam, sizes = 64, [2000, 1500]
+    invtt = np.tile(synth.invtt_row(2048, lam, 1.0), 2)
+    v = rng.standard_normal(sum(sizes))
+    N = mb.Noise(gpu_ctx, sizes, lam, invtt)
+    d = torch.from_numpy(v.copy()).cuda()
+    N.apply(d, d)
+    torch.cuda.synchronize()
+    ref = R.stbmm(v, np.array(sizes), lam, invtt, exact=True)
+    assert _rel(d.cpu().numpy(), ref) < TOL
+
+
+def test_stbmm_rejects_band_wider_than_block(gpu_ctx):
+    import midapack_b200 as mb
+    with pytest.raises(mb.MidapackError):
+        mb.Noise(gpu_ctx, [10], 64, np.ones(64))
