@@ -1,0 +1,344 @@
+"""Time-to-map benchmark: the FP64 GLS map-making solve on one B200.
+
+Workload (synthetic, seeded; no public dataset is involved): 64 detectors x
+2^24 samples (1.07e9 samples) on a 2048x1536 flat grid (3.1M pixels, 9.4M
+I/Q/U unknowns), 2^20-sample stationary intervals (1024 Toeplitz blocks,
+lambda = 2^14), 1% flagged samples, int32 pointing, FP64 weights and TOD.
+One step = one complete map-making solve from device-resident inputs:
+pointing compression (MatInit), inverse-noise spectra, block-Jacobi build with
+the rcond cut, PCG to relative residual 1e-8 (the reference's criterion).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With --impl reference the reference's own C code (oracle/_ref, built from its
+sources) is timed on the host cores on a bounded sample of the same workload
+(one operator application P^T N^-1 P per rank, one detector per rank) and
+extrapolated to the full solve with the iteration count of the GPU solve.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIG = "c2_64det_2p24_2048x1536_lam16384"
+METRIC = "time-to-map at 1e-8 residual, FP64 GLS PCG (64 det x 2^24 samples, 2048x1536 px, lambda 2^14, 1% gaps)"
+TOL = 1e-8
+MAXITER = 500
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default=CONFIG)
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, device: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={device}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 8:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def algorithmic_bytes(ns: int, n_map: int, n_tiles: int, fft_m: int):
+    """Bytes one application of each operator must move (FP64, triplet pointing)."""
+    return {
+        "P": ns * (4 + 24 + 8) + n_map * 8,
+        "Ninv": ns * (8 + 8 + 8) + n_tiles * (fft_m + 1) * 8,   # mean pass read, tile read, write
+        "Pt": ns * (4 + 24 + 8) + n_map * 8,
+    }
+
+
+def cpu_reference(wl_host, iterations: int, sample_dets: int, full_samples: int, cores: int):
+    """Reference C operator (oracle/_ref) on host cores: one P^T N^-1 P application
+    over `sample_dets` detectors (one per forked rank, in a fresh process that
+    never initialised CUDA), extrapolated to the full solve."""
+    from oracle import ref
+    if not ref.available():
+        return None
+    pix, w, bs, lam, invtt, per_det = wl_host
+    nb_per_det = len(bs) // (len(pix) // 3 // per_det)
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "sample.npz")
+        np.savez(path, pix=pix, weights=w, block_sizes=bs, lam=lam, invtt=invtt, per_det=per_det,
+                 nb_per_det=nb_per_det)
+        r = subprocess.run([sys.executable, "-m", "oracle.cpu_baseline", path, str(sample_dets)], cwd=ROOT,
+                           capture_output=True, text=True, timeout=900)
+        lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+        if r.returncode != 0 or not lines:
+            raise RuntimeError(f"reference baseline failed: {r.stderr[-300:]}")
+        t = json.loads(lines[-1])["seconds_per_application"]
+    # sample_dets ranks ran concurrently: per-application time of the full job on `cores` ranks
+    per_iter_full = t * (full_samples / (per_det * sample_dets)) * (sample_dets / cores)
+    return {"op_seconds_sample": t, "per_iter_full_s": per_iter_full, "time_to_map_s": per_iter_full * (iterations + 1)}
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    import torch
+    if args.impl == "reference" and rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    import midapack_b200 as mb
+    from midapack_b200 import synth
+    cfg = dict(synth.CONFIGS[args.config])
+    cfg["seed"] = cfg["seed"] + rank
+    wl = synth.make_workload_torch(args.config, **cfg)
+    torch.cuda.synchronize()
+    ns = wl.n_samples
+    nb = len(wl.block_sizes)
+    idv = np.arange(nb, dtype=np.int64) * wl.block_len
+    ctx = mb.Context(local)
+
+    def one_solve(profile=False):
+        P = mb.Pointing(ctx, wl.pix, wl.weights, ns, 3)
+        N = mb.Noise(ctx, wl.block_sizes, wl.lam, wl.invtt, idv=idv)
+        out = mb.gls_solve(ctx, P, N, wl.signal, wl.noise, tol=TOL, maxiter=MAXITER)
+        return P, N, out
+
+    if args.impl == "reference":
+        return run_reference(args, wl, ctx, one_solve)
+
+    for _ in range(args.warmup):
+        one_solve()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    launches0 = ctx.launches
+    ctx.profile(True)
+    clocks = Clocks(local)
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    infos = []
+    for _ in range(args.steps):
+        P, N, out = one_solve()
+        infos.append(out[5])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    launches = ctx.launches - launches0
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t)
+        torch.distributed.barrier()
+    info = infos[-1]
+    tile = N.tile()
+    n_map = info.n_map
+    ab = algorithmic_bytes(ns, n_map, tile["n_tiles"], tile["fft_n"] // 2)
+    per = {k: (prof[k][0] / max(prof[k][1], 1)) for k in ("P", "Ninv", "Pt", "vec")}
+    dom = max(("P", "Ninv", "Pt"), key=lambda k: per[k])
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = ab[dom] / (per[dom] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": {"P": "matvec_triplet_kernel", "Ninv": "toeplitz_tile_kernel",
+                                           "Pt": "trmatvec_triplet_kernel"}[dom],
+                "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                "traffic": None, "peak_source": "measured" if peaks else "fallback",
+                "per_application_ms": {k: round(v, 4) for k, v in per.items()},
+                "algorithmic_bytes": ab}
+
+    # host copies: a bounded sample for the CPU baseline, pinned inputs for the end-to-end run
+    sample = None
+    if rank == 0 and not args.no_cpu and world == 1:
+        sample = cpu_sample(wl)
+    pinned = None
+    if not args.no_e2e:
+        pinned = {k: torch.empty(getattr(wl, k).numel(), dtype=getattr(wl, k).dtype, pin_memory=True)
+                  for k in ("pix", "weights", "signal", "noise")}
+        for k, v in pinned.items():
+            v.copy_(getattr(wl, k))
+    del P, N, infos
+    wl.pix = wl.weights = wl.signal = wl.noise = None
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+
+    # end to end through the reference-facing API with host buffers
+    e2e = run_e2e(args, wl, world, pinned) if pinned else None
+    cpu = run_cpu_baseline(wl, sample, info.iterations, ns) if sample else None
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(ms / 1e3 * 1.0, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 2), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": {"workload": args.config, "samples": ns, "detectors": wl.n_det, "pixels": wl.npix,
+                       "unknowns": int(n_map), "lambda": wl.lam, "blocks": nb, "tol": TOL,
+                       "iterations": info.iterations, "converged": bool(info.converged),
+                       "precond_s": round(info.precond_seconds, 4), "solve_s": round(info.solve_seconds, 4),
+                       "fft_tile": tile, "l2": "inputs (tens of GB) far larger than L2", "parallelism":
+                           "one solve per GPU" if world == 1 else f"{world} independent solves (replicas)"},
+            "roofline": roofline, "clocks": clk, "gpu_launches": int(launches),
+        }
+        if e2e:
+            line["e2e"] = e2e
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def run_e2e(args, wl, world, pinned):
+    """MLmap_b200 (the MLmap solve, host buffers in and maps out) with pinned host inputs."""
+    import torch
+    import midapack_b200 as mb
+    pix, w, s, n = pinned["pix"], pinned["weights"], pinned["signal"], pinned["noise"]
+    npix = 12 * wl.nside * wl.nside
+    maps = [np.zeros(npix) for _ in range(4)] + [np.zeros(npix, dtype=np.int32)]
+    bs = np.ascontiguousarray(wl.block_sizes, dtype=np.int32)
+    tt = np.ascontiguousarray(wl.invtt)
+    it = mb.ct.c_int()
+    rr = mb.ct.c_double()
+    L = mb.lib()
+    P = lambda t, ty: mb.ct.cast(mb.ct.c_void_p(t.data_ptr()), mb.ct.POINTER(ty))  # noqa: E731
+    times = []
+    for _ in range(args.e2e_steps):
+        t0 = time.perf_counter()
+        mb.check(L.MLmap_b200(0, 0, TOL, MAXITER, wl.nside, wl.n_samples, len(bs), bs.ctypes.data_as(mb.c_i32p), 3,
+                              P(pix, mb.ct.c_int32), P(w, mb.ct.c_double), P(s, mb.ct.c_double),
+                              P(n, mb.ct.c_double), wl.lam, tt.ctypes.data_as(mb.c_f64p),
+                              *[m.ctypes.data_as(mb.c_f64p) for m in maps[:4]], maps[4].ctypes.data_as(mb.c_i32p),
+                              mb.ct.byref(it), mb.ct.byref(rr)), "MLmap_b200")
+        times.append(time.perf_counter() - t0)
+    t = max(times) if times else 0.0
+    if world > 1:
+        tt_ = torch.tensor([t], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(tt_, op=torch.distributed.ReduceOp.MAX)
+        t = float(tt_)
+    h2d = pix.numel() * 4 + (w.numel() + s.numel() + n.numel()) * 8 + tt.nbytes + bs.nbytes
+    d2h = 4 * npix * 8 + npix * 4
+    del pix, w, s, n
+    return {"value": round(t, 4), "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "api": "MLmap_b200 (MLmap solve, host buffers)", "iterations": it.value}
+
+
+def cpu_sample(wl):
+    cores = os.cpu_count() or 1
+    sample_dets = max(1, min(cores, 8, wl.n_det))
+    per_det = wl.n_samp
+    return (sample_dets, wl.pix[:3 * per_det * sample_dets].cpu().numpy(),
+            wl.weights[:3 * per_det * sample_dets].cpu().numpy())
+
+
+def run_cpu_baseline(wl, sample, iterations, ns):
+    sample_dets, pix, w = sample
+    per_det = wl.n_samp
+    try:
+        r = cpu_reference((pix, w, wl.block_sizes, wl.lam, wl.invtt, per_det), iterations, sample_dets, ns,
+                          sample_dets)
+    except Exception as ex:  # the baseline is reported, never required
+        return {"value": None, "unit": "s", "cores": sample_dets, "kind": "reference", "sample": f"failed: {ex}"}
+    if r is None:
+        return None
+    return {"value": round(r["time_to_map_s"], 2), "unit": "s", "cores": sample_dets, "kind": "reference",
+            "sample": (f"reference C (oracle/_ref, shim FFT/MPI) P^T N^-1 P on {sample_dets} detector(s) x 2^24 samples "
+                       f"as {sample_dets} forked ranks: {r['op_seconds_sample']:.2f} s per application; "
+                       f"extrapolated x{ns // (per_det * sample_dets)} samples x {iterations + 1} applications on "
+                       f"{sample_dets} cores")}
+
+
+def run_reference(args, wl, ctx, one_solve):
+    import torch
+    # iteration count of the same solve (device run, untimed) to extrapolate the operator cost
+    _, _, out = one_solve()
+    iters = out[5].iterations
+    cores = os.cpu_count() or 1
+    sample_dets = max(1, min(cores, 8, wl.n_det))
+    per_det = wl.n_samp
+    pix = wl.pix[:3 * per_det * sample_dets].cpu().numpy()
+    w = wl.weights[:3 * per_det * sample_dets].cpu().numpy()
+    vals = []
+    for _ in range(max(args.steps, 1)):
+        r = cpu_reference((pix, w, wl.block_sizes, wl.lam, wl.invtt, per_det), iters, sample_dets, wl.n_samples,
+                          sample_dets)
+        vals.append(r["time_to_map_s"])
+    v = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 2), "unit": "s", "n_gpus": 0,
+            "steps": len(vals), "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": {"workload": args.config, "iterations": iters},
+            "cpu_baseline": {"value": round(v, 2), "unit": "s", "cores": sample_dets, "kind": "reference",
+                             "sample": f"{sample_dets} detector(s) x 2^24 samples, one P^T N^-1 P per rank, "
+                                       f"extrapolated to 64 detectors x {iters + 1} applications"},
+            "e2e": {"value": round(v, 2), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    del torch
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -47,6 +47,12 @@ void    *mdp_context_stream(mdp_context *ctx);
 int      mdp_synchronize(mdp_context *ctx);
 /* number of kernels this library launched on ctx since creation */
 uint64_t mdp_launch_count(const mdp_context *ctx);
+/* per-operator timing of PCG iterations (CUDA events on the context stream):
+ * enable = 1 starts (and zeroes) the counters; ms[4]/count[4] receive the
+ * accumulated milliseconds and launches of P, N^-1, P^T and the fused
+ * vector/dot kernels. */
+int      mdp_profile_enable(mdp_context *ctx, int enable);
+int      mdp_profile_read(const mdp_context *ctx, double *ms, int64_t *count);
 
 /* ---- pointing matrix P (reference: Mat, algebra/include/mapmat/mapmat.h:46-69) ----
  * m rows (time samples), nnz entries per row, global column indices d_gindices

@@ -48,6 +48,8 @@ _SIGS = {
     "mdp_context_stream": (ct.c_void_p, [ct.c_void_p]),
     "mdp_synchronize": (ct.c_int, [ct.c_void_p]),
     "mdp_launch_count": (ct.c_uint64, [ct.c_void_p]),
+    "mdp_profile_enable": (ct.c_int, [ct.c_void_p, ct.c_int]),
+    "mdp_profile_read": (ct.c_int, [ct.c_void_p, c_f64p, ct.POINTER(ct.c_int64)]),
     "mdp_pointing_create": (ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_int, ct.c_void_p, ct.c_void_p,
                                        ct.POINTER(ct.c_void_p)]),
     "mdp_pointing_destroy": (None, [ct.c_void_p]),
@@ -146,6 +148,15 @@ class Context:
 
     def synchronize(self):
         check(lib().mdp_synchronize(self.h), "mdp_synchronize")
+
+    def profile(self, enable: bool = True):
+        check(lib().mdp_profile_enable(self.h, 1 if enable else 0), "mdp_profile_enable")
+
+    def profile_read(self):
+        ms = (ct.c_double * 4)()
+        n = (ct.c_int64 * 4)()
+        check(lib().mdp_profile_read(self.h, ms, n), "mdp_profile_read")
+        return {k: (ms[i], n[i]) for i, k in enumerate(("P", "Ninv", "Pt", "vec"))}
 
     @property
     def launches(self) -> int:

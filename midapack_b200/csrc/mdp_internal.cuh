@@ -83,6 +83,11 @@ struct mdp_context {
     DevBuf       scratch;   // large temporary (stbmm in place, scans)
     DevBuf       scratch2;
     double      *h_pinned = nullptr;  // pinned host scalars
+    // optional per-operator timing inside the solver (CUDA events on the stream)
+    int          profile = 0;
+    double       prof_ms[4] = {0, 0, 0, 0};   // P, N^-1, P^T, vector/dot kernels
+    int64_t      prof_n[4] = {0, 0, 0, 0};
+    cudaEvent_t  ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 // ---------------------------------------------------------------- pointing

@@ -73,6 +73,8 @@ extern "C" void mdp_context_destroy(mdp_context *ctx) {
     cudaStreamSynchronize(ctx->stream);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    for (int i = 0; i < 5; i++)
+        if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
     delete ctx;
 }
 
@@ -99,6 +101,27 @@ extern "C" int mdp_synchronize(mdp_context *ctx) {
 }
 
 extern "C" uint64_t mdp_launch_count(const mdp_context *ctx) { return ctx ? ctx->launches : 0; }
+
+extern "C" int mdp_profile_enable(mdp_context *ctx, int enable) {
+    if (!ctx) return MDP_EINVAL;
+    if (enable && !ctx->ev[0])
+        for (int i = 0; i < 5; i++) MDP_CUDA(cudaEventCreate(&ctx->ev[i]));
+    ctx->profile = enable ? 1 : 0;
+    for (int i = 0; i < 4; i++) {
+        ctx->prof_ms[i] = 0.0;
+        ctx->prof_n[i] = 0;
+    }
+    return MDP_OK;
+}
+
+extern "C" int mdp_profile_read(const mdp_context *ctx, double *ms, int64_t *count) {
+    if (!ctx) return MDP_EINVAL;
+    for (int i = 0; i < 4; i++) {
+        if (ms) ms[i] = ctx->prof_ms[i];
+        if (count) count[i] = ctx->prof_n[i];
+    }
+    return MDP_OK;
+}
 
 // ============================================================== device-wide exclusive scan (uint32)
 // Three phases: per-tile totals, scan of the totals (recursively), rescan of
@@ -266,6 +289,19 @@ __global__ void triplet_kernel(const int32_t *__restrict__ g, int64_t m, int32_t
     if (local_bad) atomicOr(bad, 1);
 }
 
+// In trash mode the reference reads x[local - nnz] for every entry of a row
+// whose first local index is not 0 (mapmat.c:711-719): an entry with local
+// index < nnz there would read before the map.  Such pointings are rejected.
+__global__ void validate_general_kernel(const int32_t *__restrict__ local, int64_t m, int nnz, int *__restrict__ bad) {
+    int local_bad = 0;
+    for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t) gridDim.x * blockDim.x) {
+        if (local[t * nnz] == 0) continue;
+        for (int j = 0; j < nnz; j++)
+            if (local[t * nnz + j] < nnz) local_bad = 1;
+    }
+    if (local_bad) atomicOr(bad, 1);
+}
+
 int mdp_pointing_create_ex(mdp_context *ctx, int64_t m, int nnz, const int32_t *d_g, const double *d_values,
                            int32_t *d_local_out, mdp_pointing **out) {
     if (!ctx || !out || m < 0 || nnz <= 0 || (m > 0 && (!d_g || !d_values))) {
@@ -350,6 +386,25 @@ int mdp_pointing_create_ex(mdp_context *ctx, int64_t m, int nnz, const int32_t *
         localize_kernel<<<grid_for(n, 256, ctx->sm_count * 32), 256, 0, ctx->stream>>>(d_g, n, gmin, rank.as<uint32_t>(),
                                                                                       A->local.as<int32_t>());
         ctx->launches++;
+        if (A->trash_pix) {
+            DevBuf bad;
+            if ((rc = bad.alloc(sizeof(int)))) {
+                delete A;
+                return rc;
+            }
+            cudaMemsetAsync(bad.p, 0, sizeof(int), ctx->stream);
+            validate_general_kernel<<<grid_for(m, 256, ctx->sm_count * 32), 256, 0, ctx->stream>>>(
+                    A->local.as<int32_t>(), m, nnz, bad.as<int>());
+            ctx->launches++;
+            int hbad = 0;
+            cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+            cudaStreamSynchronize(ctx->stream);
+            if (hbad) {
+                delete A;
+                mdp_set_error("mdp_pointing_create: a row that is not a trash row holds a negative (flagged) index");
+                return MDP_EINVAL;
+            }
+        }
         if (d_local_out)
             cudaMemcpyAsync(d_local_out, A->local.p, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, ctx->stream);
     } else if (local) {

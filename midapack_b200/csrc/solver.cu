@@ -550,6 +550,8 @@ int mdp_bj_build(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, BJState 
     MDP_TRY(mdp_exclusive_scan_u32(ctx, keep.as<uint32_t>(), rankb.as<uint32_t>(), npix0, &kept_blocks));
     MDP_CUDA(cudaMemsetAsync(bj->inv.p, 0, 72 * npix0, st));
     MDP_CUDA(cudaMemsetAsync(bj->W.p, 0, 72 * npix0, st));
+    MDP_CUDA(cudaMemsetAsync(bj->rcond.p, 0, 8 * npix0, st));
+    MDP_CUDA(cudaMemsetAsync(bj->hits.p, 0, 4 * npix0, st));
     compact_blocks_kernel<<<gb, 256, 0, st>>>(keep.as<uint32_t>(), rankb.as<uint32_t>(), npix0, inv.as<double>(),
                                               rcond.as<double>(), hits.as<int>(), bj->inv.as<double>(),
                                               bj->rcond.as<double>(), bj->hits.as<int32_t>());
@@ -564,8 +566,10 @@ int mdp_bj_build(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, BJState 
     A->trash_pix = 1;
     A->lcount = 3 * (int64_t) kept_pix + 3;
     // the reference pairs kept blocks with kept pixels in order; both counts
-    // agree except when a cut target falls past the last pixel
-    bj->npix = std::min<int64_t>(kept_pix, kept_blocks);
+    // agree except when, with flagged samples, the last pixel is cut: its
+    // target falls past the end, no pixel leaves the map and the reference
+    // leaves the last preconditioner rows unset.  Here they are zero blocks.
+    bj->npix = kept_pix;
     return MDP_OK;
 }
 
@@ -614,17 +618,31 @@ int mdp_pcg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const dou
         k = params->maxiter;
         converged = 1;
     }
+    const bool prof = ctx->profile != 0;
     for (; k < params->maxiter; k++) {
         std::swap(g, gp);
+        if (prof) cudaEventRecord(ctx->ev[0], st);
         MDP_TRY(mdp_matvec_launch(ctx, A, h, ta));
+        if (prof) cudaEventRecord(ctx->ev[1], st);
         MDP_TRY(mdp_stbmm_impl(ctx, N, ta, tb, nullptr));
+        if (prof) cudaEventRecord(ctx->ev[2], st);
         MDP_TRY(mdp_trmatvec_launch(ctx, A, tb, q));
+        if (prof) cudaEventRecord(ctx->ev[3], st);
         pcg_coeff_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(h, q, n, S);
         MDP_CHECK_LAUNCH(ctx);
         pcg_update_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(inv, x, h, q, gp, g, Cg, npix, S);
         MDP_CHECK_LAUNCH(ctx);
+        if (prof) cudaEventRecord(ctx->ev[4], st);
         MDP_CUDA(cudaMemcpyAsync(hs, S, 8 * 8, cudaMemcpyDeviceToHost, st));
         MDP_CUDA(cudaStreamSynchronize(st));
+        if (prof) {
+            for (int e = 0; e < 4; e++) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ctx->ev[e], ctx->ev[e + 1]);
+                ctx->prof_ms[e] += ms;
+                ctx->prof_n[e] += 1;
+            }
+        }
         res = hs->res;
         if (!std::isfinite(res)) {
             mdp_set_error("mdp_gls_solve: residual became %f at iteration %d", res, k);

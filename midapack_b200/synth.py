@@ -23,6 +23,7 @@ white noise with sqrt(PSD) per detector.  d = P m_true + n, returned as
 """
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -171,3 +172,63 @@ def small(name: str = "small", width: int = 32, height: int = 24, n_det: int = 2
           block_len: int = 2048, lam: int = 64, fknee: float = 1.0, seed: int = 7, gap_frac: float = 0.0
           ) -> Workload:
     return make_workload(name, width, height, n_det, n_samp, block_len, lam, fknee, seed, gap_frac)
+
+
+def make_workload_torch(name: str, width: int, height: int, n_det: int, n_samp: int, block_len: int, lam: int,
+                        fknee: float = 1.0, seed: int = 20261203, gap_frac: float = 0.0, device: str = "cuda"):
+    """Same generator as make_workload, run on the GPU with torch for the
+    ~1e9-sample workloads (its own seeded streams, so values differ from the
+    numpy version).  Returns a Workload whose arrays are device tensors
+    (pix int32 [3Ns], weights/signal/noise float64) plus numpy block_sizes/invtt."""
+    import torch
+
+    wl = Workload(name, width, height, n_det, n_samp, block_len, lam, fknee, seed, gap_frac)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    ns = n_det * n_samp
+    npix = width * height
+    sky = torch.empty((npix, 3), dtype=torch.float64, device=device)
+    sky.normal_(generator=g)
+    sky[:, 0] *= 100.0
+    pix = torch.empty(3 * ns, dtype=torch.int32, device=device)
+    w = torch.empty(3 * ns, dtype=torch.float64, device=device)
+    signal = torch.empty(ns, dtype=torch.float64, device=device)
+    noise = torch.empty(ns, dtype=torch.float64, device=device)
+    t = torch.arange(n_samp, device=device, dtype=torch.int64)
+    run = t // width
+    u = t % width
+    tsec = t.to(torch.float64) / FS
+    f = torch.fft.rfftfreq(n_samp, 1.0 / FS, dtype=torch.float64, device=device)
+    amp = torch.sqrt(1.0 + fknee / (f + F_MIN))
+    offs = torch.randint(0, 1 << 30, (n_det, 2), generator=g, device=device)
+    k3 = torch.arange(3, device=device, dtype=torch.int32)
+    for d in range(n_det):
+        r0 = int(offs[d, 0]) % height
+        c0 = int(offs[d, 1]) % width
+        col = torch.where(run % 2 == 0, u, width - 1 - u)
+        col = (col + c0) % width
+        row = (run + r0) % height
+        p = (row * width + col)
+        psi = math.radians(45.0 * (d % 4)) + 2.0 * math.pi * F_HWP * tsec
+        sl = slice(3 * d * n_samp, 3 * (d + 1) * n_samp)
+        wd = w[sl].view(n_samp, 3)
+        wd[:, 0] = 1.0
+        wd[:, 1] = torch.cos(2.0 * psi)
+        wd[:, 2] = torch.sin(2.0 * psi)
+        signal[d * n_samp:(d + 1) * n_samp] = (wd * sky[p]).sum(dim=1)
+        white = torch.randn(n_samp, dtype=torch.float64, device=device, generator=g)
+        noise[d * n_samp:(d + 1) * n_samp] = torch.fft.irfft(torch.fft.rfft(white) * amp, n=n_samp)
+        if gap_frac > 0:
+            flagged = torch.rand(n_samp, device=device, generator=g, dtype=torch.float64) < gap_frac
+            p = torch.where(flagged, torch.full_like(p, -1), p)
+        pix[sl].view(n_samp, 3).copy_((3 * p.to(torch.int32))[:, None] + k3[None, :])
+        del p, psi, col, row
+    if n_samp % block_len != 0:
+        raise ValueError("block_len must divide n_samp")
+    nb = ns // block_len
+    row_t = invtt_row(block_len, lam, fknee)
+    wl.pix, wl.weights, wl.signal, wl.noise = pix, w, signal, noise
+    wl.invtt = np.tile(row_t, nb)
+    wl.block_sizes = np.full(nb, block_len, dtype=np.int32)
+    wl.sky = sky
+    return wl

@@ -240,7 +240,18 @@ def precond_blockjacobi(A: Pointing, signal: np.ndarray, block_sizes, lam, invtt
     if cut.any():
         A2.trash_pix = 1
     keep = ~cut
-    return BJResult(A2, sig, inv[keep], W[keep], rcond[keep], hits[keep], cut)
+    inv_k, W_k, rc_k, h_k = inv[keep], W[keep], rcond[keep], hits[keep]
+    npix2 = A2.n // nnz
+    if npix2 > inv_k.shape[0]:
+        # with flagged samples and the last pixel cut, the cut target lies past
+        # the end: no pixel leaves the map and the reference leaves the last
+        # preconditioner rows unset (uninitialised); they are zero blocks here
+        pad = npix2 - inv_k.shape[0]
+        inv_k = np.concatenate([inv_k, np.zeros((pad, nnz, nnz))])
+        W_k = np.concatenate([W_k, np.zeros((pad, nnz, nnz))])
+        rc_k = np.concatenate([rc_k, np.zeros(pad)])
+        h_k = np.concatenate([h_k, np.zeros(pad, dtype=h_k.dtype)])
+    return BJResult(A2, sig, inv_k, W_k, rc_k, h_k, cut)
 
 
 def apply_bj(inv: np.ndarray, g: np.ndarray) -> np.ndarray:

@@ -55,7 +55,10 @@ def test_general_layout(gpu_ctx, nnz):
     import midapack_b200 as mb
     rng = np.random.default_rng(10 + nnz)
     m = 5000
-    gidx = rng.integers(-2, 700, size=m * nnz).astype(np.int32)
+    gidx = rng.integers(0, 700, size=(m, nnz)).astype(np.int32)
+    flagged = rng.random(m) < 0.05  # whole rows flagged: every entry negative, the first the smallest
+    gidx[flagged] = -nnz + np.arange(nnz)
+    gidx = gidx.reshape(-1)
     vals = rng.standard_normal(m * nnz)
     A = R.local_shape(gidx, vals, m, nnz)
     P = mb.Pointing(gpu_ctx, _dev(gidx), _dev(vals), m, nnz)
@@ -95,3 +98,15 @@ def test_adjoint_full_size(gpu_ctx):
     a = float(torch.dot(Px, y))
     b = float(torch.dot(x, Pty))
     assert abs(a - b) <= 1e-12 * (float(Px.norm()) * float(y.norm()))
+
+
+def test_rejects_negative_index_in_valid_row(gpu_ctx):
+    """A non-trash row holding a flagged index would make the reference read
+    before the map (mapmat.c:711-719); it is rejected on creation."""
+    import midapack_b200 as mb
+    m, nnz = 100, 2
+    gidx = np.arange(m * nnz, dtype=np.int32) + 10
+    gidx[0:2] = [-2, -1]    # a trash row
+    gidx[11] = -1           # row 5, second entry: invalid
+    with pytest.raises(mb.MidapackError):
+        mb.Pointing(gpu_ctx, _dev(gidx), _dev(np.ones(m * nnz)), m, nnz)

@@ -27,27 +27,34 @@ def _rel(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
 
 
+def _budget(case):
+    # without flagged samples the operator is singular (a constant I map is the
+    # all-ones TOD, which stbmmProd's block-mean removal annihilates) and PCG
+    # stalls near 1e-6 in the reference too: compare a fixed number of iterates
+    return (1e-10, 12) if case == "plain" else (1e-10, 400)
+
+
 @pytest.mark.parametrize("case", list(solver_cases()))
 def test_solve_vs_reference(gpu_ctx, ref_lib, case):
     wl = solver_cases()[case]()
-    tol, maxiter = 1e-10, 400
+    tol, maxiter = _budget(case)
     x, lst, cond, hits, res, info = _gpu_solve(gpu_ctx, wl, tol, maxiter)
     xr, lstr, condr, hitsr, resr = ref_lib.pcg(wl.pix, wl.weights, wl.signal, wl.noise, wl.block_sizes, wl.lam,
                                                wl.invtt, tol=tol, maxiter=maxiter)
     assert np.array_equal(lst, lstr)
     assert np.array_equal(hits, hitsr)
     assert np.allclose(cond, condr, rtol=1e-12, atol=0)
+    if case.startswith("cut"):
+        assert info.n_cut > 0
     assert abs(info.iterations - (len(resr) - 1)) <= 1, (info.iterations, len(resr) - 1)
     for k in range(3):
         assert _rel(x[k::3], xr[k::3]) < MAP_TOL, (k, _rel(x[k::3], xr[k::3]))
-    if case.startswith("cut"):
-        assert info.n_cut > 0
 
 
-@pytest.mark.parametrize("case", ["plain", "cut_gaps"])
+@pytest.mark.parametrize("case", ["plain", "cut", "gaps"])
 def test_solve_vs_restatement(gpu_ctx, case):
     wl = solver_cases()[case]()
-    tol, maxiter = 1e-10, 400
+    tol, maxiter = _budget(case)
     x, lst, cond, hits, res, info = _gpu_solve(gpu_ctx, wl, tol, maxiter)
     o = R.pcg(wl.pix, wl.weights, wl.signal, wl.noise, wl.block_sizes, wl.lam, wl.invtt, tol=tol, maxiter=maxiter)
     assert np.array_equal(lst, o.bj.A.lindices[3 * o.bj.A.trash_pix:])
@@ -58,7 +65,7 @@ def test_solve_vs_restatement(gpu_ctx, case):
 
 def test_residual_history_monotone_prefix(gpu_ctx, ref_lib):
     """The per-iteration relative residuals follow the reference's to 1e-6 relative."""
-    wl = solver_cases()["plain"]()
+    wl = solver_cases()["gaps"]()
     x, lst, cond, hits, res, info = _gpu_solve(gpu_ctx, wl, 1e-8, 200)
     _, _, _, _, resr = ref_lib.pcg(wl.pix, wl.weights, wl.signal, wl.noise, wl.block_sizes, wl.lam, wl.invtt,
                                    tol=1e-8, maxiter=200)

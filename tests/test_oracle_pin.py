@@ -1,0 +1,98 @@
+"""Pins the numpy restatement to the reference's own compiled C
+(oracle/_ref): compression bit-exact, P and P^T bit-exact (same summation
+order), N^-1 within 1e-13, the full PCG within 1e-12, and the rcond cut
+(including the reference's behaviour with flagged samples).  Plus the
+project LAPACK shim against scipy's LAPACK.  CPU only."""
+import ctypes as ct
+import os
+
+import numpy as np
+import pytest
+
+from midapack_b200 import synth
+from oracle import restate as R
+from tests._cases import solver_cases
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.mark.parametrize("case", list(solver_cases()))
+def test_operators_bitexact(ref_lib, case):
+    wl = solver_cases()[case]()
+    m = wl.n_samples
+    A = R.local_shape(wl.pix, wl.weights, m, 3)
+    loc, lind, trash = ref_lib.local_shape(wl.pix, m, 3)
+    assert np.array_equal(A.lindices, lind) and np.array_equal(A.local, loc) and A.trash_pix == trash
+    x = np.random.default_rng(0).standard_normal(A.n)
+    assert np.array_equal(R.matvec(A, x), ref_lib.matvec(wl.pix, wl.weights, x, m))
+    y = np.random.default_rng(1).standard_normal(m)
+    assert np.array_equal(R.trmatvec(A, y), ref_lib.trmatvec(wl.pix, wl.weights, y, m, A.n))
+    v = np.random.default_rng(2).standard_normal(m)
+    assert _rel(R.stbmm(v, wl.block_sizes, wl.lam, wl.invtt, exact=True),
+                ref_lib.stbmm(v, wl.block_sizes, wl.lam, wl.invtt)) < 1e-13
+
+
+@pytest.mark.parametrize("case", list(solver_cases()))
+def test_pcg_and_cut(ref_lib, case):
+    wl = solver_cases()[case]()
+    maxiter = 12 if case == "plain" else 400  # gap-free: singular operator, compare fixed iterates
+    o = R.pcg(wl.pix, wl.weights, wl.signal, wl.noise, wl.block_sizes, wl.lam, wl.invtt, tol=1e-10, maxiter=maxiter)
+    xr, lst, cond, hits, res = ref_lib.pcg(wl.pix, wl.weights, wl.signal, wl.noise, wl.block_sizes, wl.lam, wl.invtt,
+                                           tol=1e-10, maxiter=maxiter)
+    assert np.array_equal(o.bj.A.lindices[3 * o.bj.A.trash_pix:], lst)
+    # entries past the kept blocks are stale memory in the reference (see restate.precond_blockjacobi)
+    kb = int((~o.bj.cut).sum())
+    assert np.array_equal(o.bj.hits[:kb], hits[:kb])
+    assert np.allclose(o.bj.cond[:kb], cond[:kb], rtol=1e-13, atol=0)
+    assert min(o.iters, maxiter - 1) == len(res) - 1
+    assert _rel(o.x, xr) < 1e-12
+
+
+def test_mlmap_multirank_matches_single(ref_lib):
+    """The fork/shared-memory MPI stand-in: 4-rank MLmap == 1-rank MLmap."""
+    wl = synth.small(n_det=4, n_samp=2048, block_len=1024, lam=32, seed=51, gap_frac=0.02)
+    args = (wl.block_sizes, wl.pix, wl.weights, wl.signal, wl.noise, wl.lam, wl.invtt, wl.nside)
+    one = ref_lib.mlmap(1, [wl.n_samples], [len(wl.block_sizes)], *args, tol=1e-10, maxiter=300)
+    per = wl.n_samples // 4
+    four = ref_lib.mlmap(4, [per] * 4, [len(wl.block_sizes) // 4] * 4, *args, tol=1e-10, maxiter=300)
+    for k in range(3):
+        assert _rel(four[k], one[k]) < 1e-10
+    assert np.array_equal(four[4], one[4])
+
+
+def test_shim_lapack_vs_scipy(ref_lib):
+    from scipy.linalg import lapack
+    L = ct.CDLL(os.path.join(os.path.dirname(ref_lib.LIB_PATH), "libmidapack_ref_shims.so"))
+    L.LAPACKE_dgetrf.argtypes = [ct.c_int, ct.c_int, ct.c_int, ct.POINTER(ct.c_double), ct.c_int,
+                                 ct.POINTER(ct.c_int)]
+    L.LAPACKE_dgecon.argtypes = [ct.c_int, ct.c_char, ct.c_int, ct.POINTER(ct.c_double), ct.c_int, ct.c_double,
+                                 ct.POINTER(ct.c_double)]
+    L.LAPACKE_dgetri.argtypes = [ct.c_int, ct.c_int, ct.POINTER(ct.c_double), ct.c_int, ct.POINTER(ct.c_int)]
+    rng = np.random.default_rng(3)
+    for trial in range(300):
+        w = rng.standard_normal((rng.integers(1, 40), 3))
+        w[:, 0] = 1.0
+        a = (w[:, :, None] * w[:, None, :]).sum(0) * rng.uniform(0.5, 2e7)
+        if trial % 7 == 0:
+            a = np.outer(w[0], w[0])  # rank one
+        anorm = np.abs(a).sum(axis=0).max()
+        m = np.ascontiguousarray(a.copy())
+        ipiv = np.zeros(3, dtype=np.int32)
+        L.LAPACKE_dgetrf(101, 3, 3, m.ctypes.data_as(ct.POINTER(ct.c_double)), 3,
+                         ipiv.ctypes.data_as(ct.POINTER(ct.c_int)))
+        rc = ct.c_double()
+        L.LAPACKE_dgecon(101, b"1", 3, m.ctypes.data_as(ct.POINTER(ct.c_double)), 3, anorm, ct.byref(rc))
+        lu, piv, _ = lapack.dgetrf(np.asfortranarray(a))
+        rs, _ = lapack.dgecon(lu, anorm, norm="1")
+        assert np.array_equal(ipiv - 1, piv)
+        assert np.allclose(m, lu, rtol=1e-13, atol=1e-13 * np.abs(a).max())
+        assert (rc.value > 0.1) == (rs > 0.1)
+        if rs > 1e-8:
+            assert abs(rc.value - rs) <= 1e-12 * rs
+        if rs > 0.1:
+            L.LAPACKE_dgetri(101, 3, m.ctypes.data_as(ct.POINTER(ct.c_double)), 3,
+                             ipiv.ctypes.data_as(ct.POINTER(ct.c_int)))
+            inv, _ = lapack.dgetri(lu, piv)
+            assert np.allclose(m, inv, rtol=1e-12, atol=1e-12 * np.abs(inv).max())
