@@ -210,10 +210,11 @@ def main():
                 "per_application_ms": {k: round(v, 4) for k, v in per.items()},
                 "algorithmic_bytes": ab}
 
-    # host copies: a bounded sample for the CPU baseline, pinned inputs for the end-to-end run
-    sample = None
+    # the reference's CPU path on a bounded sample (before any large host allocation)
+    cpu = None
     if rank == 0 and not args.no_cpu and world == 1:
-        sample = cpu_sample(wl)
+        cpu = run_cpu_baseline(wl, cpu_sample(wl), info.iterations, ns)
+    # pinned host inputs for the end-to-end run
     pinned = None
     if not args.no_e2e:
         pinned = {k: torch.empty(getattr(wl, k).numel(), dtype=getattr(wl, k).dtype, pin_memory=True)
@@ -227,7 +228,7 @@ def main():
 
     # end to end through the reference-facing API with host buffers
     e2e = run_e2e(args, wl, world, pinned) if pinned else None
-    cpu = run_cpu_baseline(wl, sample, info.iterations, ns) if sample else None
+    pinned = None
 
     if rank == 0:
         line = {
