@@ -87,6 +87,20 @@ void mdp_noise_destroy(mdp_noise *N);
  * in == out is allowed. */
 int  mdp_stbmm(mdp_context *ctx, const mdp_noise *N, const double *d_in, double *d_out);
 int  mdp_noise_tile(const mdp_noise *N, int *fft_size, int *cluster_ctas, int64_t *n_tiles);
+/* No counterpart in the reference.  out = N^-1 in like mdp_stbmm, but the call
+ * allocates no device memory: for callers that cannot call cudaMalloc while
+ * they apply the operator (a memory arena or pool that owns the device memory,
+ * a solve loop that must not synchronise the device through cudaMalloc/cudaFree,
+ * a plugin that may only touch buffers its host gives it).  The block-mean
+ * scratch lives in a fixed 1 MiB device array (131072 doubles) that the library
+ * keeps on every device it is loaded on until the process exits; a noise
+ * operator needing more (one double per block plus one per 65536-row chunk of
+ * every block) is rejected with MDP_EINVAL, as is d_in == d_out.  The first
+ * call on a device looks up that array's device address (once per device), so
+ * make the first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (other streams, other threads, other contexts
+ * on the same device) race on it and must be serialised by the caller. */
+int  mdp_stbmm_noalloc(mdp_context *ctx, const mdp_noise *N, const double *d_in, double *d_out);
 
 /* ---- GLS solve (reference PCG_GLS_true with block-Jacobi, pcg_true.c:20-241) ---- */
 typedef struct {

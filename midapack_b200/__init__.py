@@ -63,6 +63,7 @@ _SIGS = {
                                     ct.POINTER(ct.c_void_p)]),
     "mdp_noise_destroy": (None, [ct.c_void_p]),
     "mdp_stbmm": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mdp_stbmm_noalloc": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "mdp_noise_tile": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int), ct.POINTER(ct.c_int64)]),
     "mdp_gls_solve": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                  ct.POINTER(SolveParams), ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,

@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 
 #include "mdp_internal.cuh"
 
@@ -618,4 +619,77 @@ extern "C" int mdp_stbmm(mdp_context *ctx, const mdp_noise *N, const double *d_i
         src = ctx->scratch.as<double>();
     }
     return mdp_stbmm_impl(ctx, N, src, d_out, nullptr);
+}
+
+// ------------------------------------------------------------------ allocation-free N^-1
+// Some callers cannot allocate device memory at the moment they apply the
+// noise operator: code running inside a fixed memory arena or pool that owns
+// all device memory, callers that forbid cudaMalloc/cudaFree in their solve
+// loop because those calls synchronise the device, and plugins loaded into a
+// host that hands them only the buffers it owns.  mdp_stbmm_noalloc serves
+// them: the per-chunk partial sums and per-block means of the mean-removal
+// pass live in the file-scope array below instead of buffers of the noise
+// object, and the call allocates nothing.  The array holds
+// MDP_NOALLOC_SCRATCH_DOUBLES doubles (1 MiB) on every device that loads this
+// library, until the process exits.
+#define MDP_NOALLOC_SCRATCH_DOUBLES (1 << 17)
+static __device__ __align__(256) double g_stbmm_scratch[MDP_NOALLOC_SCRATCH_DOUBLES];
+
+static std::mutex g_noalloc_mu;
+static double    *g_noalloc_ptr[64] = {nullptr};
+
+// The host-side name g_stbmm_scratch is only a stand-in for the symbol, not a
+// device address: the address is looked up once per device, with that device
+// current, and cached.
+static int noalloc_scratch(int device, double **out) {
+    if (device < 0 || device >= 64) return MDP_EINVAL;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void       *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_stbmm_scratch);
+        if (e != cudaSuccess) {
+            mdp_set_error("mdp_stbmm_noalloc: cudaGetSymbolAddress failed on device %d: %s", device,
+                          cudaGetErrorString(e));
+            return MDP_ECUDA;
+        }
+        g_noalloc_ptr[device] = static_cast<double *>(p);
+    }
+    *out = g_noalloc_ptr[device];
+    return MDP_OK;
+}
+
+extern "C" int mdp_stbmm_noalloc(mdp_context *ctx, const mdp_noise *N, const double *d_in, double *d_out) {
+    if (!ctx || !N || !d_in || !d_out) {
+        mdp_set_error("mdp_stbmm_noalloc: invalid arguments");
+        return MDP_EINVAL;
+    }
+    if (d_in == d_out) {
+        mdp_set_error("mdp_stbmm_noalloc: in-place application needs a copy of the input; pass d_out != d_in");
+        return MDP_EINVAL;
+    }
+    NoiseExtra   *X = g_extra.at(N);
+    const int64_t need = (int64_t) X->n_chunks + N->nb;
+    if (N->lambda > 1 && need > MDP_NOALLOC_SCRATCH_DOUBLES) {
+        mdp_set_error("mdp_stbmm_noalloc: %lld scratch doubles needed (%d blocks, %d 65536-row chunks), limit %d",
+                      (long long) need, N->nb, X->n_chunks, MDP_NOALLOC_SCRATCH_DOUBLES);
+        return MDP_EINVAL;
+    }
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    double *scratch = nullptr;
+    MDP_TRY(noalloc_scratch(ctx->device, &scratch));
+    if (N->lambda == 1) return mdp_stbmm_impl(ctx, N, d_in, d_out, nullptr);  // no mean removal, no scratch
+    double *partial = scratch;                 // [n_chunks], each written before it is read
+    double *means = scratch + X->n_chunks;     // [nb], each written before it is read
+    if (X->n_chunks > 0) {
+        block_partial_sums<<<X->n_chunks, 512, 0, ctx->stream>>>(d_in, X->chunk_start.as<int64_t>(),
+                                                                 X->chunk_len.as<int32_t>(), partial);
+        MDP_CHECK_LAUNCH(ctx);
+        block_means_final<<<grid_for(N->nb, 128, 1024), 128, 0, ctx->stream>>>(
+                partial, X->blk_chunk0.as<int32_t>(), X->blk_nchunk.as<int32_t>(), N->blk_len.as<int32_t>(), N->nb,
+                means);
+        MDP_CHECK_LAUNCH(ctx);
+    } else {
+        MDP_CUDA(cudaMemsetAsync(means, 0, sizeof(double) * N->nb, ctx->stream));
+    }
+    return mdp_stbmm_impl(ctx, N, d_in, d_out, means);
 }
