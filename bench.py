@@ -122,7 +122,11 @@ def cpu_reference(wl_host, iterations: int, sample_dets: int, full_samples: int,
                            capture_output=True, text=True, timeout=900)
         lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
         if r.returncode != 0 or not lines:
-            raise RuntimeError(f"reference baseline failed: {r.stderr[-300:]}")
+            os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+            with open(os.path.join(ROOT, "gpurun_out", "cpu_baseline_failure.log"), "w") as fh:
+                fh.write(r.stdout[-20000:] + "\n----- stderr -----\n" + r.stderr[-20000:])
+            errs = [ln for ln in r.stderr.splitlines() if "shim_mpi" in ln or "Error" in ln]
+            raise RuntimeError(f"reference baseline failed: {' | '.join(errs[-3:])}")
         t = json.loads(lines[-1])["seconds_per_application"]
     # sample_dets ranks ran concurrently: per-application time of the full job on `cores` ranks
     per_iter_full = t * (full_samples / (per_det * sample_dets)) * (sample_dets / cores)

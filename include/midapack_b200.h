@@ -41,7 +41,8 @@ const char *mdp_last_error(void);
 /* ---- context: one device, one stream ---------------------------------- */
 int      mdp_context_create(int device, mdp_context **out);
 void     mdp_context_destroy(mdp_context *ctx);
-/* queue work on an existing cudaStream_t (e.g. the caller's); NULL = own stream */
+/* queue work on an existing cudaStream_t (e.g. the caller's; pass cudaStreamLegacy,
+ * i.e. (void *) 1, for the legacy default stream); NULL = a stream of its own */
 int      mdp_context_set_stream(mdp_context *ctx, void *cuda_stream);
 void    *mdp_context_stream(mdp_context *ctx);
 int      mdp_synchronize(mdp_context *ctx);

@@ -145,7 +145,9 @@ class Context:
         if use_torch_stream:
             import torch
             s = torch.cuda.current_stream(device).cuda_stream
-            check(lib().mdp_context_set_stream(self.h, ct.c_void_p(s)), "mdp_context_set_stream")
+            # torch's default stream is the legacy default stream, handle 0; the
+            # C API reads NULL as "own stream", so name it explicitly (cudaStreamLegacy)
+            check(lib().mdp_context_set_stream(self.h, ct.c_void_p(s if s else 1)), "mdp_context_set_stream")
 
     def synchronize(self):
         check(lib().mdp_synchronize(self.h), "mdp_synchronize")

@@ -101,6 +101,12 @@ struct mdp_pointing {
     DevBuf        lindices;           // int32 [lcount]
     DevBuf        local;              // int32 [m*nnz] (general layout only)
     DevBuf        off;                // int32 [m]: map offset 3q, -1 trash row, -2 cut row (triplet layout)
+    // P^T by map bins (triplet layout): samples grouped by bins of bin_pix pixels
+    int           bins_valid = 0;
+    int           bin_pix = 0;
+    int64_t       nbins = 0;
+    DevBuf        bin_start;          // int64 [nbins+1] offsets into bin_perm
+    DevBuf        bin_perm;           // uint32 [valid rows] sample index, grouped by bin
     int64_t n_map() const { return lcount - (int64_t) nnz * trash_pix; }
 };
 
@@ -155,6 +161,8 @@ int mdp_exclusive_scan_u32(mdp_context *ctx, const uint32_t *d_in, uint32_t *d_o
 int mdp_stbmm_impl(mdp_context *ctx, const mdp_noise *N, const double *d_in, double *d_out,
                    const double *d_means_or_null);
 int mdp_block_means(mdp_context *ctx, const mdp_noise *N, const double *d_v, double *d_means);
+int mdp_matvec_blockmeans(mdp_context *ctx, const mdp_pointing *A, const mdp_noise *N, const double *d_x,
+                          double *d_y);
 
 inline int grid_for(int64_t n, int threads, int max_blocks = 148 * 16) {
     int64_t b = (n + threads - 1) / threads;

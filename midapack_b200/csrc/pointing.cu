@@ -597,8 +597,130 @@ __global__ void trmatvec_general_kernel(const int32_t *__restrict__ local, const
     }
 }
 
+// ---- P^T by map bins.  The samples of a bin of BIN_PIX consecutive pixels are
+// listed once per pointing (roughly in time order: a warp's 32 consecutive
+// samples that fall in one bin get consecutive slots).  Each CTA then sums a
+// slice of one bin's samples into a shared-memory copy of the bin's map
+// (FP64 shared atomics) and adds it to the map with one global atomic per
+// entry, instead of three global atomics per sample.
+#define PT_BIN_PIX 2048
+#define PT_SPLIT 4
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+__global__ void bin_count_kernel(const int32_t *__restrict__ off, int64_t m, int bin3, uint32_t *__restrict__ count) {
+    for (int64_t t0 = (int64_t) blockIdx.x * blockDim.x; t0 < m; t0 += (int64_t) gridDim.x * blockDim.x) {
+        const int64_t t = t0 + threadIdx.x;
+        const int32_t o = (t < m) ? off[t] : -1;
+        const int     b = (o >= 0) ? o / bin3 : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, b);
+        if (b >= 0 && lane_id() == __ffs(peers) - 1) atomicAdd(count + b, (uint32_t) __popc(peers));
+    }
+}
+
+__global__ void bin_scatter_kernel(const int32_t *__restrict__ off, int64_t m, int bin3,
+                                   const uint32_t *__restrict__ start, uint32_t *__restrict__ cursor,
+                                   uint32_t *__restrict__ perm) {
+    for (int64_t t0 = (int64_t) blockIdx.x * blockDim.x; t0 < m; t0 += (int64_t) gridDim.x * blockDim.x) {
+        const int64_t t = t0 + threadIdx.x;
+        const int32_t o = (t < m) ? off[t] : -1;
+        const int     b = (o >= 0) ? o / bin3 : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, b);
+        const int      leader = __ffs(peers) - 1;
+        uint32_t       base = 0;
+        if (b >= 0 && lane_id() == leader) base = atomicAdd(cursor + b, (uint32_t) __popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        if (b >= 0) {
+            const unsigned below = peers & ((1u << lane_id()) - 1u);
+            perm[start[b] + base + __popc(below)] = (uint32_t) t;
+        }
+    }
+}
+
+static int build_bins(mdp_context *ctx, mdp_pointing *A) {
+    const int64_t npix = A->n_map() / 3;
+    const int     bin3 = 3 * PT_BIN_PIX;
+    const int64_t nb = (npix + PT_BIN_PIX - 1) / PT_BIN_PIX;
+    DevBuf        count, start, cursor;
+    MDP_TRY(count.alloc(4 * (nb + 1)));
+    MDP_TRY(start.alloc(4 * (nb + 1)));
+    MDP_TRY(cursor.alloc(4 * (nb + 1)));
+    MDP_CUDA(cudaMemsetAsync(count.p, 0, 4 * (nb + 1), ctx->stream));
+    MDP_CUDA(cudaMemsetAsync(cursor.p, 0, 4 * (nb + 1), ctx->stream));
+    const int g = grid_for(A->m, 256, ctx->sm_count * 16);
+    bin_count_kernel<<<g, 256, 0, ctx->stream>>>(A->off.as<int32_t>(), A->m, bin3, count.as<uint32_t>());
+    MDP_CHECK_LAUNCH(ctx);
+    uint32_t total = 0;
+    MDP_TRY(mdp_exclusive_scan_u32(ctx, count.as<uint32_t>(), start.as<uint32_t>(), nb + 1, &total));
+    MDP_TRY(A->bin_perm.alloc(4 * std::max<int64_t>(total, 1)));
+    bin_scatter_kernel<<<g, 256, 0, ctx->stream>>>(A->off.as<int32_t>(), A->m, bin3, start.as<uint32_t>(),
+                                                   cursor.as<uint32_t>(), A->bin_perm.as<uint32_t>());
+    MDP_CHECK_LAUNCH(ctx);
+    std::vector<uint32_t> hs(nb + 1);
+    MDP_CUDA(cudaMemcpyAsync(hs.data(), start.p, 4 * (nb + 1), cudaMemcpyDeviceToHost, ctx->stream));
+    MDP_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::vector<int64_t> hs64(nb + 1);
+    for (int64_t i = 0; i <= nb; i++) hs64[i] = hs[i];
+    MDP_TRY(A->bin_start.alloc(8 * (nb + 1)));
+    MDP_CUDA(cudaMemcpy(A->bin_start.p, hs64.data(), 8 * (nb + 1), cudaMemcpyHostToDevice));
+    A->nbins = nb;
+    A->bin_pix = PT_BIN_PIX;
+    A->bins_valid = 1;
+    return MDP_OK;
+}
+
+__global__ void __launch_bounds__(512) trmatvec_binned_kernel(const int32_t *__restrict__ off,
+                                                              const double *__restrict__ w,
+                                                              const double *__restrict__ y, double *__restrict__ x,
+                                                              const int64_t *__restrict__ bin_start,
+                                                              const uint32_t *__restrict__ perm, int64_t n_map) {
+    __shared__ double acc[3 * PT_BIN_PIX];
+    const int64_t bin = blockIdx.x / PT_SPLIT;
+    const int     part = blockIdx.x % PT_SPLIT;
+    for (int i = threadIdx.x; i < 3 * PT_BIN_PIX; i += blockDim.x) acc[i] = 0.0;
+    __syncthreads();
+    const int64_t s0 = bin_start[bin], s1 = bin_start[bin + 1];
+    const int64_t len = s1 - s0;
+    const int64_t a = s0 + len * part / PT_SPLIT, b = s0 + len * (part + 1) / PT_SPLIT;
+    const int64_t base = bin * 3 * PT_BIN_PIX;
+    for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+        const int64_t t = perm[i];
+        const int     o = (int) (off[t] - base);
+        const double  v = y[t];
+        atomicAdd(acc + o, w[3 * t] * v);
+        atomicAdd(acc + o + 1, w[3 * t + 1] * v);
+        atomicAdd(acc + o + 2, w[3 * t + 2] * v);
+    }
+    __syncthreads();
+    const int64_t lim = min((int64_t) 3 * PT_BIN_PIX, n_map - base);
+    for (int i = threadIdx.x; i < lim; i += blockDim.x) {
+        const double v = acc[i];
+        if (v != 0.0) atomicAdd(x + base + i, v);
+    }
+}
+
+static bool use_bins(const mdp_pointing *A) {
+    static int env = -1;
+    if (env < 0) {
+        const char *e = getenv("MDP_PT_BINNED");
+        env = e ? atoi(e) : 1;
+    }
+    return env != 0 && A->triplet && A->m >= (1 << 20);
+}
+
 int mdp_trmatvec_launch(mdp_context *ctx, const mdp_pointing *A, const double *d_y, double *d_x) {
     MDP_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * A->n_map(), ctx->stream));
+    if (use_bins(A)) {
+        mdp_pointing *Am = const_cast<mdp_pointing *>(A);  // the bin list is a cache of the pointing
+        if (!Am->bins_valid) MDP_TRY(build_bins(ctx, Am));
+        if (A->nbins > 0) {
+            trmatvec_binned_kernel<<<(unsigned) (A->nbins * PT_SPLIT), 512, 0, ctx->stream>>>(
+                    A->off.as<int32_t>(), A->values, d_y, d_x, A->bin_start.as<int64_t>(), A->bin_perm.as<uint32_t>(),
+                    A->n_map());
+            MDP_CHECK_LAUNCH(ctx);
+        }
+        return MDP_OK;
+    }
     if (A->triplet && !aligned16(A->values, d_y)) {
         trmatvec_triplet_scalar_kernel<<<grid_for(A->m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
                 A->off.as<int32_t>(), A->values, d_y, d_x, A->m);

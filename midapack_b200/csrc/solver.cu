@@ -563,6 +563,7 @@ int mdp_bj_build(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, BJState 
     MDP_CUDA(cudaStreamSynchronize(st));
     std::swap(A->lindices.p, lind2.p);
     std::swap(A->lindices.bytes, lind2.bytes);
+    A->bins_valid = 0;  // pixels were renumbered
     A->trash_pix = 1;
     A->lcount = 3 * (int64_t) kept_pix + 3;
     // the reference pairs kept blocks with kept pixels in order; both counts
@@ -622,9 +623,12 @@ int mdp_pcg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const dou
     for (; k < params->maxiter; k++) {
         std::swap(g, gp);
         if (prof) cudaEventRecord(ctx->ev[0], st);
-        MDP_TRY(mdp_matvec_launch(ctx, A, h, ta));
+        // P h with the block means of P h fused in when the blocks tile the rows
+        const int fused = mdp_matvec_blockmeans(ctx, A, N, h, ta);
+        if (fused != MDP_OK && fused != MDP_EUNSUPPORTED) return fused;
+        if (fused == MDP_EUNSUPPORTED) MDP_TRY(mdp_matvec_launch(ctx, A, h, ta));
         if (prof) cudaEventRecord(ctx->ev[1], st);
-        MDP_TRY(mdp_stbmm_impl(ctx, N, ta, tb, nullptr));
+        MDP_TRY(mdp_stbmm_impl(ctx, N, ta, tb, fused == MDP_OK ? N->means.as<double>() : nullptr));
         if (prof) cudaEventRecord(ctx->ev[2], st);
         MDP_TRY(mdp_trmatvec_launch(ctx, A, tb, q));
         if (prof) cudaEventRecord(ctx->ev[3], st);

@@ -43,44 +43,71 @@ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
     return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 
+// 16th roots of unity exp(-2 pi i k / 16), k < 8, correctly rounded
+__constant__ double2 c_w16[8] = {
+    {0x1.0000000000000p+0, 0.0},
+    {0x1.d906bcf328d46p-1, -0x1.87de2a6aea963p-2},
+    {0x1.6a09e667f3bcdp-1, -0x1.6a09e667f3bcdp-1},
+    {0x1.87de2a6aea963p-2, -0x1.d906bcf328d46p-1},
+    {0.0, -0x1.0000000000000p+0},
+    {-0x1.87de2a6aea963p-2, -0x1.d906bcf328d46p-1},
+    {-0x1.6a09e667f3bcdp-1, -0x1.6a09e667f3bcdp-1},
+    {-0x1.d906bcf328d46p-1, -0x1.87de2a6aea963p-2},
+};
+
+// Shared-memory index swizzle: XOR the low 3 bits of a complex index with
+// bits 5-7.  Every pass below reads sets of elements at a stride of L/R; the
+// swizzle spreads those over all 8 16-byte bank groups of a 128-byte row, so
+// no pass (including the small-group ones) has bank conflicts.
+__device__ __forceinline__ int swz(int i) { return i ^ ((i >> 5) & 7); }
+
+__device__ __forceinline__ double2 csq(double2 a) {  // a^2
+    return make_double2(a.x * a.x - a.y * a.y, 2.0 * a.x * a.y);
+}
+
 // DIF stages of a radix-R register set.  Element i of the set sits at group
-// position q + i*(L/R) inside a DIF group of size L.  Stage j (group L/2^j,
-// span L/2^(j+1)) pairs i and i + R/2^(j+1); the difference is multiplied by
-// W_{L_j}^{pos} = tw[pos * (N / L_j)], tw[k] = exp(-2 pi i k / N).
+// position q + i*(L/R) inside a DIF group of size L; w = W_L^q is loaded by
+// the caller.  Stage j (group L/2^j, span L/2^(j+1)) pairs i and i + R/2^(j+1)
+// (i mod R/2^j < R/2^(j+1)); the difference is multiplied by
+// W_{L/2^j}^{q + r L/R} = w^(2^j) * W_16^(r 2^j 16/R), r = i mod R/2^j.
 template <int R>
-__device__ __forceinline__ void dif_set(double2 (&v)[R], int L, int q, int logN_over_L, const double2 *__restrict__ tw) {
+__device__ __forceinline__ void dif_set(double2 (&v)[R], double2 w) {
+    double2 wj = w;
 #pragma unroll
     for (int j = 0, sub = R; sub > 1; j++, sub >>= 1) {
         const int half = sub >> 1;
-        const int shift = logN_over_L + j;  // N / L_j = 2^shift
 #pragma unroll
         for (int i = 0; i < R; i++) {
-            if ((i % sub) < half) {
-                const int     pos = q + (i % sub) * (L / R);
+            const int r = i % sub;
+            if (r < half) {
                 const double2 a = v[i], b = v[i + half];
                 v[i] = cadd(a, b);
-                const double2 d = csub(a, b);
-                v[i + half] = (pos == 0) ? d : cmul(d, __ldg(tw + ((int64_t) pos << shift)));
+                const double2 tw = (r == 0) ? wj : cmul(wj, c_w16[(r << j) * (16 / R)]);
+                v[i + half] = cmul(csub(a, b), tw);
             }
         }
+        wj = csq(wj);
     }
 }
 
 // exact mirror of dif_set with conjugate twiddles (decimation in time)
 template <int R>
-__device__ __forceinline__ void dit_set(double2 (&v)[R], int L, int q, int logN_over_L, const double2 *__restrict__ tw) {
-    int j = 0;
-    for (int sub = R; sub > 2; sub >>= 1) j++;
+__device__ __forceinline__ void dit_set(double2 (&v)[R], double2 w) {
+    constexpr int NS = (R >= 16) ? 4 : (R >= 8) ? 3 : (R >= 4) ? 2 : 1;
+    double2       wpow[NS];
+    wpow[0] = w;
 #pragma unroll
-    for (int sub = 2; sub <= R; sub <<= 1, j--) {
-        const int half = sub >> 1;
-        const int shift = logN_over_L + j;
+    for (int j = 1; j < NS; j++) wpow[j] = csq(wpow[j - 1]);
+#pragma unroll
+    for (int j = NS - 1; j >= 0; j--) {
+        const int sub = R >> j, half = sub >> 1;
 #pragma unroll
         for (int i = 0; i < R; i++) {
-            if ((i % sub) < half) {
-                const int     pos = q + (i % sub) * (L / R);
+            const int r = i % sub;
+            if (r < half) {
+                const double2 tw = (r == 0) ? wpow[j] : cmul(wpow[j], c_w16[(r << j) * (16 / R)]);
                 const double2 a = v[i];
-                const double2 t = (pos == 0) ? v[i + half] : cmulc(v[i + half], __ldg(tw + ((int64_t) pos << shift)));
+                const double2 t = cmulc(v[i + half], tw);
                 v[i] = cadd(a, t);
                 v[i + half] = csub(a, t);
             }
@@ -88,50 +115,45 @@ __device__ __forceinline__ void dit_set(double2 (&v)[R], int L, int q, int logN_
     }
 }
 
-// one local pass of R = 2^k stages starting at group size L over smem s[0..ML)
+// one local pass of R = 2^k stages starting at group size L over smem s[0..ML);
+// tw[k] = exp(-2 pi i k / N) with N = 2^logN
 template <int R, bool INVERSE>
 __device__ __forceinline__ void local_pass(double2 *s, int ML, int L, int logN_over_L, const double2 *__restrict__ tw) {
     const int nsets = ML / R;
     const int stride = L / R;
     for (int set = threadIdx.x; set < nsets; set += blockDim.x) {
-        const int g = set / stride, q = set - g * stride;
-        double2  *base = s + g * L + q;
-        double2   v[R];
+        const int     g = set / stride, q = set - g * stride;
+        const int     base = g * L + q;
+        const double2 w = __ldg(tw + ((int64_t) q << logN_over_L));  // W_L^q
+        double2       v[R];
 #pragma unroll
-        for (int i = 0; i < R; i++) v[i] = base[i * stride];
-        if (INVERSE) dit_set<R>(v, L, q, logN_over_L, tw);
-        else dif_set<R>(v, L, q, logN_over_L, tw);
+        for (int i = 0; i < R; i++) v[i] = s[swz(base + i * stride)];
+        if (INVERSE) dit_set<R>(v, w);
+        else dif_set<R>(v, w);
 #pragma unroll
-        for (int i = 0; i < R; i++) base[i * stride] = v[i];
+        for (int i = 0; i < R; i++) s[swz(base + i * stride)] = v[i];
     }
     __syncthreads();
 }
 
-template <bool INVERSE>
-__device__ __forceinline__ void local_fft(double2 *s, int logML, int logN, const double2 *__restrict__ tw) {
-    // stages grouped 4 at a time, largest groups first (forward) / last (inverse)
-    int ks[8], Ls[8], np = 0;
-    for (int rem = logML, L = 1 << logML; rem > 0;) {
-        int k = rem >= 4 ? 4 : rem;
-        ks[np] = k;
-        Ls[np] = L;
-        np++;
-        L >>= k;
-        rem -= k;
-    }
-    const int ML = 1 << logML;
-    for (int pi = 0; pi < np; pi++) {
-        const int p = INVERSE ? (np - 1 - pi) : pi;
-        const int L = Ls[p];
-        int       logL = 0;
-        while ((1 << logL) < L) logL++;
+// all local stages of the per-CTA transform, 4 per pass; the schedule is
+// resolved at compile time (no local-memory tables)
+template <int LOG_ML, bool INVERSE>
+__device__ __forceinline__ void local_fft(double2 *s, int logN, const double2 *__restrict__ tw) {
+    constexpr int NP = (LOG_ML + 3) / 4;
+    constexpr int ML = 1 << LOG_ML;
+#pragma unroll
+    for (int pi = 0; pi < NP; pi++) {
+        const int p = INVERSE ? (NP - 1 - pi) : pi;
+        const int rem = LOG_ML - 4 * p;
+        const int k = rem >= 4 ? 4 : rem;
+        const int logL = LOG_ML - 4 * p;
+        const int L = 1 << logL;
         const int lno = logN - logL;
-        switch (ks[p]) {
-            case 4: local_pass<16, INVERSE>(s, ML, L, lno, tw); break;
-            case 3: local_pass<8, INVERSE>(s, ML, L, lno, tw); break;
-            case 2: local_pass<4, INVERSE>(s, ML, L, lno, tw); break;
-            default: local_pass<2, INVERSE>(s, ML, L, lno, tw); break;
-        }
+        if (k == 4) local_pass<16, INVERSE>(s, ML, L, lno, tw);
+        else if (k == 3) local_pass<8, INVERSE>(s, ML, L, lno, tw);
+        else if (k == 2) local_pass<4, INVERSE>(s, ML, L, lno, tw);
+        else local_pass<2, INVERSE>(s, ML, L, lno, tw);
     }
 }
 
@@ -176,7 +198,7 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgs a) {
     const int64_t r0 = ws + (int64_t) rank * 2 * ML;
     for (int j = threadIdx.x; j < 2 * ML; j += blockDim.x) {
         const int64_t row = r0 + j;
-        sd[j] = (row >= bs && row < be) ? (__ldg(a.vin + row) - mu) : 0.0;
+        sd[2 * swz(j >> 1) + (j & 1)] = (row >= bs && row < be) ? (__ldg(a.vin + row) - mu) : 0.0;
     }
 
     if constexpr (C > 1) {
@@ -184,19 +206,20 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgs a) {
         cluster.sync();
         // cross-CTA DIF stages: set q holds element c of CTA c at local q
         for (int q = rank * (ML / C) + threadIdx.x; q < (rank + 1) * (ML / C); q += blockDim.x) {
-            double2 v[C];
+            double2   v[C];
+            const int sq = swz(q);
 #pragma unroll
-            for (int c = 0; c < C; c++) v[c] = cluster.map_shared_rank(smem, c)[q];
-            dif_set<C>(v, M, q, 1, a.tw);
+            for (int c = 0; c < C; c++) v[c] = cluster.map_shared_rank(smem, c)[sq];
+            dif_set<C>(v, __ldg(a.tw + 2 * q));  // W_M^q = W_N^(2q)
 #pragma unroll
-            for (int c = 0; c < C; c++) cluster.map_shared_rank(smem, c)[q] = v[c];
+            for (int c = 0; c < C; c++) cluster.map_shared_rank(smem, c)[sq] = v[c];
         }
         cluster.sync();
     } else {
         __syncthreads();
     }
 
-    local_fft<false>(smem, LOG_ML, logN, a.tw);
+    local_fft<LOG_ML, false>(smem, logN, a.tw);
 
     if constexpr (C > 1) cg::this_cluster().sync();
 
@@ -208,10 +231,10 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgs a) {
         if (k > M / 2) continue;
         const int k2 = (M - k) & (M - 1);
         const int P2 = (int) (__brev((unsigned) k2) >> (32 - logM));
-        double2  *s1 = smem + p;
+        double2  *s1 = smem + swz(p);
         double2  *s2;
-        if constexpr (C > 1) s2 = cg::this_cluster().map_shared_rank(smem, P2 / ML) + (P2 % ML);
-        else s2 = smem + P2;
+        if constexpr (C > 1) s2 = cg::this_cluster().map_shared_rank(smem, P2 / ML) + swz(P2 % ML);
+        else s2 = smem + swz(P2);
         const double2 Z1 = *s1, Z2 = *s2;
         const double2 E0 = make_double2(0.5 * (Z1.x + Z2.x), 0.5 * (Z1.y - Z2.y));
         const double2 O0 = make_double2(0.5 * (Z1.y + Z2.y), -0.5 * (Z1.x - Z2.x));
@@ -229,18 +252,19 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgs a) {
     if constexpr (C > 1) cg::this_cluster().sync();
     else __syncthreads();
 
-    local_fft<true>(smem, LOG_ML, logN, a.tw);
+    local_fft<LOG_ML, true>(smem, logN, a.tw);
 
     if constexpr (C > 1) {
         cg::cluster_group cluster = cg::this_cluster();
         cluster.sync();
         for (int q = rank * (ML / C) + threadIdx.x; q < (rank + 1) * (ML / C); q += blockDim.x) {
-            double2 v[C];
+            double2   v[C];
+            const int sq = swz(q);
 #pragma unroll
-            for (int c = 0; c < C; c++) v[c] = cluster.map_shared_rank(smem, c)[q];
-            dit_set<C>(v, M, q, 1, a.tw);
+            for (int c = 0; c < C; c++) v[c] = cluster.map_shared_rank(smem, c)[sq];
+            dit_set<C>(v, __ldg(a.tw + 2 * q));  // W_M^q = W_N^(2q)
 #pragma unroll
-            for (int c = 0; c < C; c++) cluster.map_shared_rank(smem, c)[q] = v[c];
+            for (int c = 0; c < C; c++) cluster.map_shared_rank(smem, c)[sq] = v[c];
         }
         cluster.sync();
     }
@@ -250,7 +274,7 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgs a) {
     const int64_t out_end = min(t0 + (int64_t) E, be);
     for (int j = threadIdx.x; j < 2 * ML; j += blockDim.x) {
         const int64_t row = r0 + j;
-        if (row >= t0 && row < out_end) a.vout[row] = sd[j] * scale;
+        if (row >= t0 && row < out_end) a.vout[row] = sd[2 * swz(j >> 1) + (j & 1)] * scale;
     }
 }
 
@@ -605,6 +629,55 @@ int mdp_stbmm_impl(mdp_context *ctx, const mdp_noise *N, const double *d_in, dou
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     MDP_CUDA(cudaLaunchKernelEx(&cfg, fn, a));
+    MDP_CHECK_LAUNCH(ctx);
+    return MDP_OK;
+}
+
+// y = P x fused with the block-mean partial sums of y: one CTA per 65536-row
+// chunk of a block, so the mean-removal pass of N^-1 needs no second read of y.
+__global__ void __launch_bounds__(512) matvec_chunk_sums_kernel(const int32_t *__restrict__ off,
+                                                                const double *__restrict__ w,
+                                                                const double *__restrict__ x, double *__restrict__ y,
+                                                                const int64_t *__restrict__ chunk_start,
+                                                                const int32_t *__restrict__ chunk_len,
+                                                                double *__restrict__ partial) {
+    const int64_t s = chunk_start[blockIdx.x];
+    const int     n = chunk_len[blockIdx.x];
+    double        acc = 0.0;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const int64_t t = s + j;
+        const int32_t o = off[t];
+        double        v = 0.0;
+        if (o >= 0) v = w[3 * t] * __ldg(x + o) + w[3 * t + 1] * __ldg(x + o + 1) + w[3 * t + 2] * __ldg(x + o + 2);
+        y[t] = v;
+        acc += v;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    __shared__ double ws[16];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = (threadIdx.x < (blockDim.x >> 5)) ? ws[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) partial[blockIdx.x] = v;
+    }
+}
+
+// y = P x and the block means of y into N->means.  Returns MDP_EUNSUPPORTED
+// (and does nothing) when the blocks do not cover every row or the pointing is
+// not in the triplet layout; the caller then runs P and N^-1 separately.
+int mdp_matvec_blockmeans(mdp_context *ctx, const mdp_pointing *A, const mdp_noise *N, const double *d_x,
+                          double *d_y) {
+    NoiseExtra *X = g_extra.at(N);
+    if (!A->triplet || !X->covers_all || N->lambda == 1 || N->nrow_end != A->m || X->n_chunks == 0)
+        return MDP_EUNSUPPORTED;
+    matvec_chunk_sums_kernel<<<X->n_chunks, 512, 0, ctx->stream>>>(A->off.as<int32_t>(), A->values, d_x, d_y,
+                                                                   X->chunk_start.as<int64_t>(),
+                                                                   X->chunk_len.as<int32_t>(), X->partial.as<double>());
+    MDP_CHECK_LAUNCH(ctx);
+    block_means_final<<<grid_for(N->nb, 128, 1024), 128, 0, ctx->stream>>>(
+            X->partial.as<double>(), X->blk_chunk0.as<int32_t>(), X->blk_nchunk.as<int32_t>(), N->blk_len.as<int32_t>(),
+            N->nb, N->means.as<double>());
     MDP_CHECK_LAUNCH(ctx);
     return MDP_OK;
 }

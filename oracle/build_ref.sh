@@ -15,7 +15,7 @@ if [ ! -d "$REF/algebra" ]; then
 fi
 mkdir -p "$OUT/obj"
 
-CFLAGS=(-O2 -fPIC -std=gnu11 -DW_MPI -w
+CFLAGS=(-O2 -g -fPIC -std=gnu11 -DW_MPI -w -rdynamic
   -I"$HERE/shim"
   -I"$REF/algebra/include" -I"$REF/algebra/include/mapmat" -I"$REF/algebra/include/toeplitz"
   -I"$REF/algebra/include/templates"

@@ -15,6 +15,7 @@
 #define _GNU_SOURCE
 #include "mpi.h"
 
+#include <execinfo.h>
 #include <pthread.h>
 #include <sched.h>
 #include <signal.h>
@@ -317,6 +318,17 @@ int MPI_Sendrecv_replace(void *buf, int count, MPI_Datatype dt, int dest, int se
     return MPI_SUCCESS;
 }
 
+/* a crashing rank prints where it crashed before it dies */
+static void crash_handler(int sig) {
+    void *frames[64];
+    int   n = backtrace(frames, 64);
+    char  msg[96];
+    int   len = snprintf(msg, sizeof(msg), "[shim_mpi rank %d] fatal signal %d, backtrace:\n", g_rank, sig);
+    if (write(2, msg, (size_t) len) < 0) _exit(128 + sig);
+    backtrace_symbols_fd(frames, n, 2);
+    _exit(128 + sig);
+}
+
 int shim_mpi_run(int nranks, void (*fn)(int rank, void *arg), void *arg) {
     if (nranks <= 1) {
         g_rank = 0;
@@ -352,6 +364,9 @@ int shim_mpi_run(int nranks, void (*fn)(int rank, void *arg), void *arg) {
     for (int r = 0; r < nranks; r++) {
         pid_t p = fork();
         if (p == 0) {
+            signal(SIGSEGV, crash_handler);
+            signal(SIGBUS, crash_handler);
+            signal(SIGFPE, crash_handler);
             g_rank  = r;
             g_size  = nranks;
             g_hdr   = h;
@@ -374,7 +389,15 @@ int shim_mpi_run(int nranks, void (*fn)(int rank, void *arg), void *arg) {
             if (pids[r] == p) {
                 pids[r] = 0;
                 alive--;
-                if (!WIFEXITED(st) || WEXITSTATUS(st) != 0) failed = 1;
+                if (!WIFEXITED(st) || WEXITSTATUS(st) != 0) {
+                    if (!failed) {
+                        if (WIFSIGNALED(st))
+                            fprintf(stderr, "[shim_mpi] rank %d killed by signal %d\n", r, WTERMSIG(st));
+                        else
+                            fprintf(stderr, "[shim_mpi] rank %d exited with status %d\n", r, WEXITSTATUS(st));
+                    }
+                    failed = 1;
+                }
             }
         if (failed)
             for (int r = 0; r < nranks; r++)
