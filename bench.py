@@ -31,7 +31,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 CONFIG = "c2_64det_2p24_2048x1536_lam16384"
-METRIC = "time-to-map at 1e-8 residual, FP64 GLS PCG (64 det x 2^24 samples, 2048x1536 px, lambda 2^14, 1% gaps)"
+METRIC = ("time-to-map at 1e-8 residual, GLS PCG on 1 B200 (64 det x 2^24 samples, 2048x1536 px, lambda 2^14, "
+          "1% gaps); value = mixed precision, config.fp64 = plain FP64")
 TOL = 1e-8
 MAXITER = 500
 
@@ -46,6 +47,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--inner-tol", type=float, default=1e-4)
+    ap.add_argument("--no-compare", action="store_true", help="skip timing the other precision")
     return ap.parse_args()
 
 
@@ -105,6 +109,16 @@ def algorithmic_bytes(ns: int, n_map: int, n_tiles: int, fft_m: int):
     }
 
 
+def algorithmic_bytes32(ns: int, n_map: int, t32):
+    """FP32 operator of the mixed solver: FP32 weights and TOD, FP64 map."""
+    n_tiles, fft_m = t32
+    return {
+        "P": ns * (4 + 12 + 4) + n_map * 8,
+        "Ninv": ns * (4 + 4) + n_tiles * (fft_m + 1) * 4,   # means fused into P
+        "Pt": ns * (4 + 4 + 12 + 4) + n_map * 8,            # bin list, offset, weights, TOD
+    }
+
+
 def cpu_reference(wl_host, iterations: int, sample_dets: int, full_samples: int, cores: int):
     """Reference C operator (oracle/_ref) on host cores: one P^T N^-1 P application
     over `sample_dets` detectors (one per forked rank, in a fresh process that
@@ -113,7 +127,11 @@ def cpu_reference(wl_host, iterations: int, sample_dets: int, full_samples: int,
     if not ref.available():
         return None
     pix, w, bs, lam, invtt, per_det = wl_host
-    nb_per_det = len(bs) // (len(pix) // 3 // per_det)
+    # Toeplitz blocks per detector: blocks whose cumulative end falls within one detector's samples
+    ends = np.cumsum(np.asarray(bs, dtype=np.int64))
+    nb_per_det = int(np.searchsorted(ends, per_det, side="right"))
+    if nb_per_det < 1 or ends[nb_per_det - 1] != per_det:
+        raise RuntimeError("Toeplitz blocks do not tile the detectors")
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "sample.npz")
         np.savez(path, pix=pix, weights=w, block_sizes=bs, lam=lam, invtt=invtt, per_det=per_det,
@@ -156,10 +174,14 @@ def main():
     idv = np.arange(nb, dtype=np.int64) * wl.block_len
     ctx = mb.Context(local)
 
-    def one_solve(profile=False):
+    def one_solve(precision=args.precision):
         P = mb.Pointing(ctx, wl.pix, wl.weights, ns, 3)
         N = mb.Noise(ctx, wl.block_sizes, wl.lam, wl.invtt, idv=idv)
-        out = mb.gls_solve(ctx, P, N, wl.signal, wl.noise, tol=TOL, maxiter=MAXITER)
+        if precision == "mixed":
+            out = mb.gls_solve_mixed(ctx, P, N, wl.signal, wl.noise, tol=TOL, maxiter=MAXITER,
+                                     inner_tol=args.inner_tol)
+        else:
+            out = mb.gls_solve(ctx, P, N, wl.signal, wl.noise, tol=TOL, maxiter=MAXITER)
         return P, N, out
 
     if args.impl == "reference":
@@ -196,6 +218,29 @@ def main():
         torch.distributed.barrier()
     info = infos[-1]
     tile = N.tile()
+    # the other precision, same steps, for the mixed-vs-FP64 comparison
+    other = None
+    if not args.no_compare:
+        oprec = "fp64" if args.precision == "mixed" else "mixed"
+        for _ in range(1):
+            one_solve(oprec)
+        torch.cuda.synchronize()
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        oinfo = None
+        for _ in range(args.steps):
+            _, _, oout = one_solve(oprec)
+            oinfo = oout[5]
+        e3.record(stream)
+        torch.cuda.synchronize()
+        oms = e2.elapsed_time(e3) / args.steps
+        if world > 1:
+            t = torch.tensor([oms], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            oms = float(t)
+        other = {"precision": oprec, "time_to_map_s": round(oms / 1e3, 4), "iterations": oinfo.iterations,
+                 "outer_iterations": oinfo.outer_iterations, "fp64_applications": oinfo.fp64_applications,
+                 "converged": bool(oinfo.converged)}
     n_map = info.n_map
     ab = algorithmic_bytes(ns, n_map, tile["n_tiles"], tile["fft_n"] // 2)
     per = {k: (prof[k][0] / max(prof[k][1], 1)) for k in ("P", "Ninv", "Pt", "vec")}
@@ -207,8 +252,17 @@ def main():
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     achieved = ab[dom] / (per[dom] * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": {"P": "matvec_triplet_kernel", "Ninv": "toeplitz_tile_kernel",
-                                           "Pt": "trmatvec_triplet_kernel"}[dom],
+    kname = {"P": "matvec_chunk_sums_kernel", "Ninv": "toeplitz_tile_kernel<double,13,8>",
+             "Pt": "trmatvec_binned_kernel"}
+    if args.precision == "mixed":
+        t32 = N.tile_fp32()
+        ab = algorithmic_bytes32(ns, n_map, (t32["n_tiles"], t32["fft_n"] // 2))
+        tile = {"fp64": tile, "fp32": t32}
+        kname = {"P": "matvec32_chunk_sums_kernel", "Ninv": "toeplitz_tile_kernel<float,...> (FP32)",
+                 "Pt": "trmatvec32_binned_kernel"}
+        dom = max(("P", "Ninv", "Pt"), key=lambda k: per[k])
+        achieved = ab[dom] / (per[dom] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": kname[dom],
                 "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                 "traffic": None, "peak_source": "measured" if peaks else "fallback",
                 "per_application_ms": {k: round(v, 4) for k, v in per.items()},
@@ -241,12 +295,18 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
             "config": {"workload": args.config, "samples": ns, "detectors": wl.n_det, "pixels": wl.npix,
                        "unknowns": int(n_map), "lambda": wl.lam, "blocks": nb, "tol": TOL,
-                       "iterations": info.iterations, "converged": bool(info.converged),
+                       "precision": args.precision, "iterations": info.iterations,
+                       "outer_iterations": info.outer_iterations, "fp64_applications": info.fp64_applications,
+                       "converged": bool(info.converged),
                        "precond_s": round(info.precond_seconds, 4), "solve_s": round(info.solve_seconds, 4),
                        "fft_tile": tile, "l2": "inputs (tens of GB) far larger than L2", "parallelism":
                            "one solve per GPU" if world == 1 else f"{world} independent solves (replicas)"},
             "roofline": roofline, "clocks": clk, "gpu_launches": int(launches),
         }
+        if other:
+            line["config"]["fp64" if other["precision"] == "fp64" else "mixed"] = other
+        if args.precision == "mixed":
+            line["dtype"] = "f32 operator + f64 refinement"
         if e2e:
             line["e2e"] = e2e
         if cpu:

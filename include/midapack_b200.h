@@ -88,6 +88,12 @@ void mdp_noise_destroy(mdp_noise *N);
  * in == out is allowed. */
 int  mdp_stbmm(mdp_context *ctx, const mdp_noise *N, const double *d_in, double *d_out);
 int  mdp_noise_tile(const mdp_noise *N, int *fft_size, int *cluster_ctas, int64_t *n_tiles);
+/* FP32 variant of mdp_stbmm (the operator of the mixed-precision solver):
+ * FP32 input/output, FP32 spectra and FFTs, block means accumulated in FP64.
+ * d_in != d_out required. */
+int  mdp_stbmm_fp32(mdp_context *ctx, mdp_noise *N, const float *d_in, float *d_out);
+/* FP32 tile plan (builds it on first use) */
+int  mdp_noise_tile_fp32(mdp_context *ctx, mdp_noise *N, int *fft_size, int *cluster_ctas, int64_t *n_tiles);
 /* No counterpart in the reference.  out = N^-1 in like mdp_stbmm, but the call
  * allocates no device memory: for callers that cannot call cudaMalloc while
  * they apply the operator (a memory arena or pool that owns the device memory,
@@ -117,6 +123,8 @@ typedef struct {
     int64_t n_map;         /* unknowns after the rcond cut */
     int64_t n_cut;         /* pixels removed by the rcond cut */
     double  precond_seconds, solve_seconds;
+    int     outer_iterations;   /* mixed precision: refinement steps (FP64 residuals) */
+    int     fp64_applications;  /* operator applications in FP64 */
 } mdp_solve_info;
 
 /* Builds the block-Jacobi preconditioner (rcond > 0.1 cut, exactly as
@@ -131,6 +139,20 @@ typedef struct {
 int mdp_gls_solve(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *d_signal,
                   const double *d_noise, const mdp_solve_params *params, double *d_x, int32_t *d_lstid,
                   double *d_cond, int32_t *d_hits, double *h_res_rel, mdp_solve_info *info);
+
+/* Mixed precision: the same solve as mdp_gls_solve (same preconditioner, cut
+ * and stop test on the FP64 residual sum(g^2) <= tol^2 sum(g0^2)), computed as
+ * FP64 iterative refinement.  Each step recomputes g = P^T N^-1 (d - P x) in
+ * FP64, then solves A delta = g approximately with block-Jacobi PCG whose
+ * operator P^T N^-1 P runs with FP32 weights, FP32 TOD and FP32 Toeplitz FFTs
+ * (dot products, PCG scalars, the 3x3 blocks and the map stay FP64), until the
+ * inner residual drops by inner_tol or inner_maxiter iterations, and adds delta
+ * to x.  info->iterations counts inner iterations; h_res_rel (optional,
+ * maxiter+1 entries) receives sqrt(res/res0) after each refinement step. */
+int mdp_gls_solve_mixed(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *d_signal,
+                        const double *d_noise, const mdp_solve_params *params, double inner_tol, int inner_maxiter,
+                        double *d_x, int32_t *d_lstid, double *d_cond, int32_t *d_hits, double *h_res_rel,
+                        mdp_solve_info *info);
 
 #ifdef __cplusplus
 }

@@ -34,7 +34,7 @@ class SolveParams(ct.Structure):
 class SolveInfo(ct.Structure):
     _fields_ = [("iterations", ct.c_int), ("converged", ct.c_int), ("res0", ct.c_double), ("res", ct.c_double),
                 ("n_map", ct.c_int64), ("n_cut", ct.c_int64), ("precond_seconds", ct.c_double),
-                ("solve_seconds", ct.c_double)]
+                ("solve_seconds", ct.c_double), ("outer_iterations", ct.c_int), ("fp64_applications", ct.c_int)]
 
 
 # exported symbols of include/*.h, with their ctypes signatures
@@ -64,10 +64,16 @@ _SIGS = {
     "mdp_noise_destroy": (None, [ct.c_void_p]),
     "mdp_stbmm": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "mdp_stbmm_noalloc": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mdp_stbmm_fp32": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mdp_noise_tile_fp32": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int),
+                                       ct.POINTER(ct.c_int64)]),
     "mdp_noise_tile": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int), ct.POINTER(ct.c_int64)]),
     "mdp_gls_solve": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                  ct.POINTER(SolveParams), ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                  c_f64p, ct.POINTER(SolveInfo)]),
+    "mdp_gls_solve_mixed": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                       ct.POINTER(SolveParams), ct.c_double, ct.c_int, ct.c_void_p, ct.c_void_p,
+                                       ct.c_void_p, ct.c_void_p, c_f64p, ct.POINTER(SolveInfo)]),
     # reference-compatible host API (include/mapmat.h, toeplitz.h, mappraiser.h)
     "MatInit": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, c_i32p, c_f64p, ct.c_int, ct.c_int]),
     "MatSetIndices": (None, [ct.c_void_p, ct.c_int, ct.c_int, c_i32p]),
@@ -243,8 +249,17 @@ class Noise:
         check(lib().mdp_noise_tile(self.h, ct.byref(n), ct.byref(c), ct.byref(t)))
         return dict(fft_n=n.value, cluster=c.value, n_tiles=t.value)
 
+    def tile_fp32(self):
+        n, c, t = ct.c_int(), ct.c_int(), ct.c_int64()
+        check(lib().mdp_noise_tile_fp32(self.ctx.h, self.h, ct.byref(n), ct.byref(c), ct.byref(t)))
+        return dict(fft_n=n.value, cluster=c.value, n_tiles=t.value)
+
     def apply(self, vin, vout):
         check(lib().mdp_stbmm(self.ctx.h, self.h, ct.c_void_p(_ptr(vin)), ct.c_void_p(_ptr(vout))), "mdp_stbmm")
+
+    def apply_fp32(self, vin, vout):
+        check(lib().mdp_stbmm_fp32(self.ctx.h, self.h, ct.c_void_p(_ptr(vin)), ct.c_void_p(_ptr(vout))),
+              "mdp_stbmm_fp32")
 
     def close(self):
         if self.h:
@@ -275,6 +290,27 @@ def gls_solve(ctx: Context, A: Pointing, N: Noise, signal, noise, tol=1e-8, maxi
           "mdp_gls_solve")
     n = info.n_map
     return x[:n], lst[:n], cond[:n // 3], hits[:n // 3], res[:info.iterations + 1], info
+
+
+def gls_solve_mixed(ctx: Context, A: Pointing, N: Noise, signal, noise, tol=1e-8, maxiter=500, inner_tol=1e-4,
+                    inner_maxiter=100, verbose=False):
+    """Mixed-precision solve (FP32 operator inside FP64 iterative refinement); same outputs as gls_solve."""
+    import torch
+    n0 = A.shape()["n_map"]
+    x = torch.empty(max(n0, 1), dtype=torch.float64, device="cuda")
+    lst = torch.empty(max(n0, 1), dtype=torch.int32, device="cuda")
+    cond = torch.empty(max(n0 // 3, 1), dtype=torch.float64, device="cuda")
+    hits = torch.empty(max(n0 // 3, 1), dtype=torch.int32, device="cuda")
+    res = np.zeros(maxiter + 1)
+    prm = SolveParams(tol, maxiter, 1 if verbose else 0)
+    info = SolveInfo()
+    check(lib().mdp_gls_solve_mixed(ctx.h, A.h, N.h, ct.c_void_p(_ptr(signal)), ct.c_void_p(_ptr(noise)),
+                                    ct.byref(prm), inner_tol, inner_maxiter, ct.c_void_p(x.data_ptr()),
+                                    ct.c_void_p(lst.data_ptr()), ct.c_void_p(cond.data_ptr()),
+                                    ct.c_void_p(hits.data_ptr()), res.ctypes.data_as(c_f64p), ct.byref(info)),
+          "mdp_gls_solve_mixed")
+    n = info.n_map
+    return x[:n], lst[:n], cond[:n // 3], hits[:n // 3], res[:info.outer_iterations + 1], info
 
 
 def mlmap_host(wl_pix, wl_weights, signal, noise, block_sizes, lam, invtt, nside, tol=1e-8, maxiter=500):

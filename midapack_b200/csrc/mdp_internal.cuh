@@ -107,6 +107,7 @@ struct mdp_pointing {
     int64_t       nbins = 0;
     DevBuf        bin_start;          // int64 [nbins+1] offsets into bin_perm
     DevBuf        bin_perm;           // uint32 [valid rows] sample index, grouped by bin
+    DevBuf        w32;                // float [m*3] weights for the FP32 operator (built on first use)
     int64_t n_map() const { return lcount - (int64_t) nnz * trash_pix; }
 };
 
@@ -133,6 +134,14 @@ struct mdp_noise {
     DevBuf  twiddle;       // double2 [N/2]: exp(-2 pi i k / N)
     DevBuf  means;         // double [nb]
     int     n_spec = 0;
+    std::vector<double> h_Tuniq;  // [n_spec][lambda] distinct first rows
+    // FP32 plan (mixed-precision operator), built on first use
+    struct {
+        int     ready = 0;
+        int     log2_ml = 0, cluster = 1, fft_n = 0;
+        int64_t n_tiles = 0;
+        DevBuf  tile_start, tile_block, spectra, twiddle;
+    } f32;
 };
 
 // ---------------------------------------------------------------- block Jacobi state (solver.cu)
@@ -163,6 +172,14 @@ int mdp_stbmm_impl(mdp_context *ctx, const mdp_noise *N, const double *d_in, dou
 int mdp_block_means(mdp_context *ctx, const mdp_noise *N, const double *d_v, double *d_means);
 int mdp_matvec_blockmeans(mdp_context *ctx, const mdp_pointing *A, const mdp_noise *N, const double *d_x,
                           double *d_y);
+// FP32 operator pieces (mixed precision)
+int mdp_noise_prepare_fp32(mdp_context *ctx, mdp_noise *N);
+int mdp_stbmm_impl32(mdp_context *ctx, mdp_noise *N, const float *d_in, float *d_out, const double *d_means);
+int mdp_pointing_prepare_fp32(mdp_context *ctx, mdp_pointing *A);
+int mdp_matvec32_blockmeans(mdp_context *ctx, const mdp_pointing *A, const mdp_noise *N, const double *d_x,
+                            float *d_y);
+int mdp_trmatvec32_launch(mdp_context *ctx, mdp_pointing *A, const float *d_y, double *d_x);
+int mdp_matvec32_launch(mdp_context *ctx, mdp_pointing *A, const double *d_x, float *d_y);
 
 inline int grid_for(int64_t n, int threads, int max_blocks = 148 * 16) {
     int64_t b = (n + threads - 1) / threads;

@@ -699,6 +699,68 @@ __global__ void __launch_bounds__(512) trmatvec_binned_kernel(const int32_t *__r
     }
 }
 
+// FP32 P^T by map bins for the mixed-precision operator: FP32 TOD and weights
+// in, products and sums in FP64 (shared memory), FP64 map out.
+__global__ void __launch_bounds__(512) trmatvec32_binned_kernel(const int32_t *__restrict__ off,
+                                                                const float *__restrict__ w,
+                                                                const float *__restrict__ y, double *__restrict__ x,
+                                                                const int64_t *__restrict__ bin_start,
+                                                                const uint32_t *__restrict__ perm, int64_t n_map) {
+    __shared__ double acc[3 * PT_BIN_PIX];
+    const int64_t bin = blockIdx.x / PT_SPLIT;
+    const int     part = blockIdx.x % PT_SPLIT;
+    for (int i = threadIdx.x; i < 3 * PT_BIN_PIX; i += blockDim.x) acc[i] = 0.0;
+    __syncthreads();
+    const int64_t s0 = bin_start[bin], s1 = bin_start[bin + 1];
+    const int64_t len = s1 - s0;
+    const int64_t a = s0 + len * part / PT_SPLIT, b = s0 + len * (part + 1) / PT_SPLIT;
+    const int64_t base = bin * 3 * PT_BIN_PIX;
+    for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+        const int64_t t = perm[i];
+        const int     o = (int) (off[t] - base);
+        const double  v = (double) y[t];
+        atomicAdd(acc + o, (double) w[3 * t] * v);
+        atomicAdd(acc + o + 1, (double) w[3 * t + 1] * v);
+        atomicAdd(acc + o + 2, (double) w[3 * t + 2] * v);
+    }
+    __syncthreads();
+    const int64_t lim = min((int64_t) 3 * PT_BIN_PIX, n_map - base);
+    for (int i = threadIdx.x; i < lim; i += blockDim.x) {
+        const double v = acc[i];
+        if (v != 0.0) atomicAdd(x + base + i, v);
+    }
+}
+
+__global__ void trmatvec32_kernel(const int32_t *__restrict__ off, const float *__restrict__ w,
+                                  const float *__restrict__ y, double *__restrict__ x, int64_t m) {
+    for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t) gridDim.x * blockDim.x) {
+        const int32_t o = off[t];
+        if (o < 0) continue;
+        const double v = (double) y[t];
+        atomicAdd(x + o, (double) w[3 * t] * v);
+        atomicAdd(x + o + 1, (double) w[3 * t + 1] * v);
+        atomicAdd(x + o + 2, (double) w[3 * t + 2] * v);
+    }
+}
+
+__global__ void weights_to_float_kernel(const double *__restrict__ in, float *__restrict__ out, int64_t n) {
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        out[i] = (float) in[i];
+}
+
+int mdp_pointing_prepare_fp32(mdp_context *ctx, mdp_pointing *A) {
+    if (!A->triplet) {
+        mdp_set_error("the FP32 operator needs the (I,Q,U) triplet pointing layout");
+        return MDP_EUNSUPPORTED;
+    }
+    if (A->w32.p) return MDP_OK;
+    MDP_TRY(A->w32.alloc(sizeof(float) * 3 * A->m));
+    weights_to_float_kernel<<<grid_for(3 * A->m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+            A->values, A->w32.as<float>(), 3 * A->m);
+    MDP_CHECK_LAUNCH(ctx);
+    return MDP_OK;
+}
+
 static bool use_bins(const mdp_pointing *A) {
     static int env = -1;
     if (env < 0) {
@@ -739,4 +801,42 @@ int mdp_trmatvec_launch(mdp_context *ctx, const mdp_pointing *A, const double *d
 extern "C" int mdp_trmatvec(mdp_context *ctx, const mdp_pointing *A, const double *d_y, double *d_x) {
     if (!ctx || !A || !d_x || !d_y) return MDP_EINVAL;
     return mdp_trmatvec_launch(ctx, A, d_y, d_x);
+}
+
+// x (FP64, n_map) = P^T y (FP32 TOD) with the FP32 weights
+int mdp_trmatvec32_launch(mdp_context *ctx, mdp_pointing *A, const float *d_y, double *d_x) {
+    MDP_TRY(mdp_pointing_prepare_fp32(ctx, A));
+    MDP_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * A->n_map(), ctx->stream));
+    if (use_bins(A)) {
+        if (!A->bins_valid) MDP_TRY(build_bins(ctx, A));
+        if (A->nbins > 0) {
+            trmatvec32_binned_kernel<<<(unsigned) (A->nbins * PT_SPLIT), 512, 0, ctx->stream>>>(
+                    A->off.as<int32_t>(), A->w32.as<float>(), d_y, d_x, A->bin_start.as<int64_t>(),
+                    A->bin_perm.as<uint32_t>(), A->n_map());
+            MDP_CHECK_LAUNCH(ctx);
+        }
+        return MDP_OK;
+    }
+    trmatvec32_kernel<<<grid_for(A->m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
+            A->off.as<int32_t>(), A->w32.as<float>(), d_y, d_x, A->m);
+    MDP_CHECK_LAUNCH(ctx);
+    return MDP_OK;
+}
+
+// y32 = P x with FP32 weights (x FP64), when the fused block-sum kernel does not apply
+__global__ void matvec32_kernel(const int32_t *__restrict__ off, const float *__restrict__ w,
+                                const double *__restrict__ x, float *__restrict__ y, int64_t m) {
+    for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t) gridDim.x * blockDim.x) {
+        const int32_t o = off[t];
+        y[t] = (o >= 0) ? w[3 * t] * (float) x[o] + w[3 * t + 1] * (float) x[o + 1] + w[3 * t + 2] * (float) x[o + 2]
+                        : 0.0f;
+    }
+}
+
+int mdp_matvec32_launch(mdp_context *ctx, mdp_pointing *A, const double *d_x, float *d_y) {
+    MDP_TRY(mdp_pointing_prepare_fp32(ctx, A));
+    matvec32_kernel<<<grid_for(A->m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(A->off.as<int32_t>(),
+                                                                                     A->w32.as<float>(), d_x, d_y, A->m);
+    MDP_CHECK_LAUNCH(ctx);
+    return MDP_OK;
 }

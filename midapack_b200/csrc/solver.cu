@@ -479,6 +479,31 @@ __global__ void __launch_bounds__(RED_THREADS) pcg_update_kernel(const double *_
     }
 }
 
+// out = d' - out where d' = b (0 on cut rows) + noise: the TOD residual d' - P x
+__global__ void tod_residual_kernel(const int32_t *__restrict__ off, const double *__restrict__ b,
+                                    const double *__restrict__ noise, double *__restrict__ out, int64_t m) {
+    for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t) gridDim.x * blockDim.x)
+        out[t] = ((off[t] == -2) ? 0.0 : b[t]) + noise[t] - out[t];
+}
+
+// x += d
+__global__ void axpy1_kernel(double *__restrict__ x, const double *__restrict__ d, int64_t n) {
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        x[i] += d[i];
+}
+
+// res = (g, g)
+__global__ void __launch_bounds__(RED_THREADS) dot_self_kernel(const double *__restrict__ g, int64_t n, Scal *S) {
+    double v[1] = {0.0};
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        v[0] += g[i] * g[i];
+    block_reduce_store<1>(v, S, 0);
+    if (last_block(S, 3) && threadIdx.x == 0) {
+        S->res = sum_partials(S, 0);
+        S->count[3] = 0;
+    }
+}
+
 // h = gamma h + Cg
 __global__ void pcg_direction_kernel(double *__restrict__ h, const double *__restrict__ Cg, int64_t n, const Scal *S) {
     const double gamma = S->gamma;
@@ -703,6 +728,160 @@ extern "C" int mdp_gls_solve(mdp_context *ctx, mdp_pointing *A, const mdp_noise 
         info->n_map = A->n_map();
         info->precond_seconds = std::chrono::duration<double>(tp1 - tp0).count();
         info->solve_seconds = std::chrono::duration<double>(tp2 - tp1).count();
+        info->outer_iterations = 0;
+        info->fp64_applications = info->iterations;
+    }
+    return MDP_OK;
+}
+
+// ================================================================= mixed precision
+extern "C" int mdp_gls_solve_mixed(mdp_context *ctx, mdp_pointing *A, const mdp_noise *Nc, const double *d_signal,
+                                   const double *d_noise, const mdp_solve_params *params, double inner_tol,
+                                   int inner_maxiter, double *d_x, int32_t *d_lstid, double *d_cond, int32_t *d_hits,
+                                   double *h_res_rel, mdp_solve_info *info) {
+    if (!ctx || !A || !Nc || !d_signal || !d_noise || !params || !d_x || inner_tol <= 0.0 || inner_maxiter < 1) {
+        mdp_set_error("mdp_gls_solve_mixed: invalid arguments");
+        return MDP_EINVAL;
+    }
+    mdp_noise *N = const_cast<mdp_noise *>(Nc);  // the FP32 plan is a cache of the operator
+    if (N->nrow_end > A->m) {
+        mdp_set_error("mdp_gls_solve_mixed: noise blocks extend past the pointing rows");
+        return MDP_EINVAL;
+    }
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    auto    tp0 = std::chrono::steady_clock::now();
+    BJState bj;
+    MDP_TRY(mdp_bj_build(ctx, A, N, &bj));
+    cudaStream_t st = ctx->stream;
+    if (d_lstid)
+        MDP_CUDA(cudaMemcpyAsync(d_lstid, A->lindices.as<int32_t>() + 3 * A->trash_pix, 4 * A->n_map(),
+                                 cudaMemcpyDeviceToDevice, st));
+    if (d_cond) MDP_CUDA(cudaMemcpyAsync(d_cond, bj.rcond.p, 8 * bj.npix, cudaMemcpyDeviceToDevice, st));
+    if (d_hits) MDP_CUDA(cudaMemcpyAsync(d_hits, bj.hits.p, 4 * bj.npix, cudaMemcpyDeviceToDevice, st));
+    MDP_TRY(mdp_pointing_prepare_fp32(ctx, A));
+    MDP_TRY(mdp_noise_prepare_fp32(ctx, N));
+    MDP_CUDA(cudaStreamSynchronize(st));
+    auto tp1 = std::chrono::steady_clock::now();
+
+    const int64_t m = A->m, npix = bj.npix, n = 3 * npix, nmap = A->n_map();
+    const double *inv = bj.inv.as<double>();
+    DevBuf        tod_a, tod_b, f_a, f_b, rb, gb1, gb2, hb, qb, cgb, db, scal;
+    int           rc;
+    if ((rc = tod_a.alloc(8 * m)) || (rc = tod_b.alloc(8 * m)) || (rc = f_a.alloc(4 * m)) || (rc = f_b.alloc(4 * m)) ||
+        (rc = rb.alloc(8 * nmap)) || (rc = gb1.alloc(8 * nmap)) || (rc = gb2.alloc(8 * nmap)) ||
+        (rc = hb.alloc(8 * nmap)) || (rc = qb.alloc(8 * nmap)) || (rc = cgb.alloc(8 * nmap)) ||
+        (rc = db.alloc(8 * nmap)) || (rc = scal.alloc(sizeof(Scal))))
+        return rc;
+    Scal     *S = scal.as<Scal>();
+    double   *x = d_x, *r = rb.as<double>(), *g = gb1.as<double>(), *gp = gb2.as<double>();
+    double   *h = hb.as<double>(), *q = qb.as<double>(), *Cg = cgb.as<double>(), *dl = db.as<double>();
+    double   *ta = tod_a.as<double>(), *tb = tod_b.as<double>();
+    float    *fa = f_a.as<float>(), *fb = f_b.as<float>();
+    const int gm = grid_for(m, 256, ctx->sm_count * 16);
+    const int gn = grid_for(nmap, 256, ctx->sm_count * 8);
+    Scal     *hs = reinterpret_cast<Scal *>(ctx->h_pinned);
+    MDP_CUDA(cudaMemsetAsync(S, 0, sizeof(Scal), st));
+    MDP_CUDA(cudaMemsetAsync(x, 0, 8 * nmap, st));
+    for (double *v : {r, g, gp, h, q, Cg, dl}) MDP_CUDA(cudaMemsetAsync(v, 0, 8 * nmap, st));
+
+    auto fetch = [&]() -> int {
+        MDP_CUDA(cudaMemcpyAsync(hs, S, 8 * 8, cudaMemcpyDeviceToHost, st));
+        MDP_CUDA(cudaStreamSynchronize(st));
+        return MDP_OK;
+    };
+    // FP64 residual r = P^T N^-1 (d' - P x)
+    int  fp64_apps = 0;
+    auto residual = [&](bool x_is_zero) -> int {
+        if (x_is_zero) MDP_CUDA(cudaMemsetAsync(ta, 0, 8 * m, st));
+        else MDP_TRY(mdp_matvec_launch(ctx, A, x, ta));
+        tod_residual_kernel<<<gm, 256, 0, st>>>(A->off.as<int32_t>(), d_signal, d_noise, ta, m);
+        MDP_CHECK_LAUNCH(ctx);
+        MDP_TRY(mdp_stbmm_impl(ctx, N, ta, tb, nullptr));
+        MDP_TRY(mdp_trmatvec_launch(ctx, A, tb, r));
+        dot_self_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(r, n, S);
+        MDP_CHECK_LAUNCH(ctx);
+        fp64_apps++;
+        return fetch();
+    };
+    MDP_TRY(residual(true));
+    const double res0 = hs->res;
+    if (!std::isfinite(res0)) {
+        mdp_set_error("mdp_gls_solve_mixed: initial residual is %f", res0);
+        return MDP_ENAN;
+    }
+    const double tol2rel = params->tol * params->tol * res0;
+    if (h_res_rel) h_res_rel[0] = 1.0;
+    double res = res0;
+    int    outer = 0, inner_total = 0, converged = (res0 <= params->tol);
+    const bool prof = ctx->profile != 0;
+    while (!converged && inner_total < params->maxiter) {
+        // inner PCG on A32 delta = r, delta0 = 0: g = r, Cg = M^-1 g, h = Cg
+        MDP_CUDA(cudaMemcpyAsync(g, r, 8 * n, cudaMemcpyDeviceToDevice, st));
+        MDP_CUDA(cudaMemsetAsync(dl, 0, 8 * nmap, st));
+        pcg_init_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(inv, g, Cg, h, npix, S);
+        MDP_CHECK_LAUNCH(ctx);
+        MDP_TRY(fetch());
+        const double rin0 = hs->res;
+        for (int j = 1; j <= inner_maxiter && inner_total < params->maxiter; j++) {
+            std::swap(g, gp);
+            if (prof) cudaEventRecord(ctx->ev[0], st);
+            const int fused = mdp_matvec32_blockmeans(ctx, A, N, h, fa);
+            if (fused != MDP_OK && fused != MDP_EUNSUPPORTED) return fused;
+            if (fused == MDP_EUNSUPPORTED) MDP_TRY(mdp_matvec32_launch(ctx, A, h, fa));
+            if (prof) cudaEventRecord(ctx->ev[1], st);
+            MDP_TRY(mdp_stbmm_impl32(ctx, N, fa, fb, fused == MDP_OK ? N->means.as<double>() : nullptr));
+            if (prof) cudaEventRecord(ctx->ev[2], st);
+            MDP_TRY(mdp_trmatvec32_launch(ctx, A, fb, q));
+            if (prof) cudaEventRecord(ctx->ev[3], st);
+            pcg_coeff_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(h, q, n, S);
+            MDP_CHECK_LAUNCH(ctx);
+            pcg_update_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(inv, dl, h, q, gp, g, Cg, npix, S);
+            MDP_CHECK_LAUNCH(ctx);
+            if (prof) cudaEventRecord(ctx->ev[4], st);
+            MDP_TRY(fetch());
+            inner_total++;
+            if (prof)
+                for (int e = 0; e < 4; e++) {
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, ctx->ev[e], ctx->ev[e + 1]);
+                    ctx->prof_ms[e] += ms;
+                    ctx->prof_n[e] += 1;
+                }
+            if (!std::isfinite(hs->res)) {
+                mdp_set_error("mdp_gls_solve_mixed: inner residual became %f", hs->res);
+                return MDP_ENAN;
+            }
+            if (hs->res <= inner_tol * inner_tol * rin0) break;
+            pcg_direction_kernel<<<gn, 256, 0, st>>>(h, Cg, n, S);
+            MDP_CHECK_LAUNCH(ctx);
+        }
+        axpy1_kernel<<<gn, 256, 0, st>>>(x, dl, n);
+        MDP_CHECK_LAUNCH(ctx);
+        outer++;
+        MDP_TRY(residual(false));
+        res = hs->res;
+        if (h_res_rel && outer <= params->maxiter) h_res_rel[outer] = std::sqrt(res / res0);
+        if (params->verbose)
+            printf("refinement %d: %d inner iterations so far, res_rel = %e\n", outer, inner_total, std::sqrt(res / res0));
+        if (!std::isfinite(res)) {
+            mdp_set_error("mdp_gls_solve_mixed: residual became %f after refinement %d", res, outer);
+            return MDP_ENAN;
+        }
+        converged = res <= tol2rel;
+    }
+    MDP_CUDA(cudaStreamSynchronize(st));
+    auto tp2 = std::chrono::steady_clock::now();
+    if (info) {
+        info->iterations = inner_total;
+        info->converged = converged;
+        info->res0 = res0;
+        info->res = res;
+        info->n_map = A->n_map();
+        info->n_cut = bj.ncut;
+        info->precond_seconds = std::chrono::duration<double>(tp1 - tp0).count();
+        info->solve_seconds = std::chrono::duration<double>(tp2 - tp1).count();
+        info->outer_iterations = outer;
+        info->fp64_applications = fp64_apps;
     }
     return MDP_OK;
 }

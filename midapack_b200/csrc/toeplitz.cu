@@ -34,13 +34,25 @@
 namespace cg = cooperative_groups;
 
 // ------------------------------------------------------------------ complex helpers
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+// The FFT runs on double2 (FP64 path) or float2 (FP32 operator of the mixed
+// precision solver); the helpers are overloaded on both.
+template <typename T> struct CT;
+template <> struct CT<double> { using V = double2; };
+template <> struct CT<float> { using V = float2; };
+
+__device__ __forceinline__ double2 mkv(double2, double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ float2 mkv(float2, float x, float y) { return make_float2(x, y); }
+
+template <typename V> __device__ __forceinline__ V cadd(V a, V b) { return mkv(a, a.x + b.x, a.y + b.y); }
+template <typename V> __device__ __forceinline__ V csub(V a, V b) { return mkv(a, a.x - b.x, a.y - b.y); }
+template <typename V> __device__ __forceinline__ V cmul(V a, V b) {
+    return mkv(a, a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
-    return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+template <typename V> __device__ __forceinline__ V cmulc(V a, V b) {  // a * conj(b)
+    return mkv(a, a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+template <typename V> __device__ __forceinline__ V csq(V a) {  // a^2
+    return mkv(a, a.x * a.x - a.y * a.y, 2 * a.x * a.y);
 }
 
 // 16th roots of unity exp(-2 pi i k / 16), k < 8, correctly rounded
@@ -54,25 +66,37 @@ __constant__ double2 c_w16[8] = {
     {-0x1.6a09e667f3bcdp-1, -0x1.6a09e667f3bcdp-1},
     {-0x1.d906bcf328d46p-1, -0x1.87de2a6aea963p-2},
 };
+__constant__ float2 c_w16f[8] = {
+    {0x1.000000p+0f, 0.0f},
+    {0x1.d906bcp-1f, -0x1.87de2ap-2f},
+    {0x1.6a09e6p-1f, -0x1.6a09e6p-1f},
+    {0x1.87de2ap-2f, -0x1.d906bcp-1f},
+    {0.0f, -0x1.000000p+0f},
+    {-0x1.87de2ap-2f, -0x1.d906bcp-1f},
+    {-0x1.6a09e6p-1f, -0x1.6a09e6p-1f},
+    {-0x1.d906bcp-1f, -0x1.87de2ap-2f},
+};
+__device__ __forceinline__ double2 w16(double2, int i) { return c_w16[i]; }
+__device__ __forceinline__ float2 w16(float2, int i) { return c_w16f[i]; }
 
 // Shared-memory index swizzle: XOR the low 3 bits of a complex index with
 // bits 5-7.  Every pass below reads sets of elements at a stride of L/R; the
-// swizzle spreads those over all 8 16-byte bank groups of a 128-byte row, so
-// no pass (including the small-group ones) has bank conflicts.
+// swizzle spreads those over all 8 bank groups of a 128-byte row (16-byte
+// elements; for 8-byte elements it halves the conflicts of the small-group
+// passes), so no FP64 pass has bank conflicts.
 __device__ __forceinline__ int swz(int i) { return i ^ ((i >> 5) & 7); }
-
-__device__ __forceinline__ double2 csq(double2 a) {  // a^2
-    return make_double2(a.x * a.x - a.y * a.y, 2.0 * a.x * a.y);
-}
+// 8-byte elements (float2): 16 per 128-byte row, XOR 4 bits
+__device__ __forceinline__ int swzv(double2, int i) { return swz(i); }
+__device__ __forceinline__ int swzv(float2, int i) { return i ^ ((i >> 5) & 15); }
 
 // DIF stages of a radix-R register set.  Element i of the set sits at group
 // position q + i*(L/R) inside a DIF group of size L; w = W_L^q is loaded by
 // the caller.  Stage j (group L/2^j, span L/2^(j+1)) pairs i and i + R/2^(j+1)
 // (i mod R/2^j < R/2^(j+1)); the difference is multiplied by
 // W_{L/2^j}^{q + r L/R} = w^(2^j) * W_16^(r 2^j 16/R), r = i mod R/2^j.
-template <int R>
-__device__ __forceinline__ void dif_set(double2 (&v)[R], double2 w) {
-    double2 wj = w;
+template <typename V, int R>
+__device__ __forceinline__ void dif_set(V (&v)[R], V w) {
+    V wj = w;
 #pragma unroll
     for (int j = 0, sub = R; sub > 1; j++, sub >>= 1) {
         const int half = sub >> 1;
@@ -80,9 +104,9 @@ __device__ __forceinline__ void dif_set(double2 (&v)[R], double2 w) {
         for (int i = 0; i < R; i++) {
             const int r = i % sub;
             if (r < half) {
-                const double2 a = v[i], b = v[i + half];
+                const V a = v[i], b = v[i + half];
                 v[i] = cadd(a, b);
-                const double2 tw = (r == 0) ? wj : cmul(wj, c_w16[(r << j) * (16 / R)]);
+                const V tw = (r == 0) ? wj : cmul(wj, w16(wj, (r << j) * (16 / R)));
                 v[i + half] = cmul(csub(a, b), tw);
             }
         }
@@ -91,10 +115,10 @@ __device__ __forceinline__ void dif_set(double2 (&v)[R], double2 w) {
 }
 
 // exact mirror of dif_set with conjugate twiddles (decimation in time)
-template <int R>
-__device__ __forceinline__ void dit_set(double2 (&v)[R], double2 w) {
+template <typename V, int R>
+__device__ __forceinline__ void dit_set(V (&v)[R], V w) {
     constexpr int NS = (R >= 16) ? 4 : (R >= 8) ? 3 : (R >= 4) ? 2 : 1;
-    double2       wpow[NS];
+    V             wpow[NS];
     wpow[0] = w;
 #pragma unroll
     for (int j = 1; j < NS; j++) wpow[j] = csq(wpow[j - 1]);
@@ -105,9 +129,9 @@ __device__ __forceinline__ void dit_set(double2 (&v)[R], double2 w) {
         for (int i = 0; i < R; i++) {
             const int r = i % sub;
             if (r < half) {
-                const double2 tw = (r == 0) ? wpow[j] : cmul(wpow[j], c_w16[(r << j) * (16 / R)]);
-                const double2 a = v[i];
-                const double2 t = cmulc(v[i + half], tw);
+                const V tw = (r == 0) ? wpow[j] : cmul(wpow[j], w16(w, (r << j) * (16 / R)));
+                const V a = v[i];
+                const V t = cmulc(v[i + half], tw);
                 v[i] = cadd(a, t);
                 v[i + half] = csub(a, t);
             }
@@ -117,29 +141,29 @@ __device__ __forceinline__ void dit_set(double2 (&v)[R], double2 w) {
 
 // one local pass of R = 2^k stages starting at group size L over smem s[0..ML);
 // tw[k] = exp(-2 pi i k / N) with N = 2^logN
-template <int R, bool INVERSE>
-__device__ __forceinline__ void local_pass(double2 *s, int ML, int L, int logN_over_L, const double2 *__restrict__ tw) {
+template <typename V, int R, bool INVERSE>
+__device__ __forceinline__ void local_pass(V *s, int ML, int L, int logN_over_L, const V *__restrict__ tw) {
     const int nsets = ML / R;
     const int stride = L / R;
     for (int set = threadIdx.x; set < nsets; set += blockDim.x) {
-        const int     g = set / stride, q = set - g * stride;
-        const int     base = g * L + q;
-        const double2 w = __ldg(tw + ((int64_t) q << logN_over_L));  // W_L^q
-        double2       v[R];
+        const int g = set / stride, q = set - g * stride;
+        const int base = g * L + q;
+        const V   w = __ldg(tw + ((int64_t) q << logN_over_L));  // W_L^q
+        V         v[R];
 #pragma unroll
-        for (int i = 0; i < R; i++) v[i] = s[swz(base + i * stride)];
-        if (INVERSE) dit_set<R>(v, w);
-        else dif_set<R>(v, w);
+        for (int i = 0; i < R; i++) v[i] = s[swzv(V{}, base + i * stride)];
+        if (INVERSE) dit_set<V, R>(v, w);
+        else dif_set<V, R>(v, w);
 #pragma unroll
-        for (int i = 0; i < R; i++) s[swz(base + i * stride)] = v[i];
+        for (int i = 0; i < R; i++) s[swzv(V{}, base + i * stride)] = v[i];
     }
     __syncthreads();
 }
 
 // all local stages of the per-CTA transform, 4 per pass; the schedule is
 // resolved at compile time (no local-memory tables)
-template <int LOG_ML, bool INVERSE>
-__device__ __forceinline__ void local_fft(double2 *s, int logN, const double2 *__restrict__ tw) {
+template <typename V, int LOG_ML, bool INVERSE>
+__device__ __forceinline__ void local_fft(V *s, int logN, const V *__restrict__ tw) {
     constexpr int NP = (LOG_ML + 3) / 4;
     constexpr int ML = 1 << LOG_ML;
 #pragma unroll
@@ -150,31 +174,35 @@ __device__ __forceinline__ void local_fft(double2 *s, int logN, const double2 *_
         const int logL = LOG_ML - 4 * p;
         const int L = 1 << logL;
         const int lno = logN - logL;
-        if (k == 4) local_pass<16, INVERSE>(s, ML, L, lno, tw);
-        else if (k == 3) local_pass<8, INVERSE>(s, ML, L, lno, tw);
-        else if (k == 2) local_pass<4, INVERSE>(s, ML, L, lno, tw);
-        else local_pass<2, INVERSE>(s, ML, L, lno, tw);
+        if (k == 4) local_pass<V, 16, INVERSE>(s, ML, L, lno, tw);
+        else if (k == 3) local_pass<V, 8, INVERSE>(s, ML, L, lno, tw);
+        else if (k == 2) local_pass<V, 4, INVERSE>(s, ML, L, lno, tw);
+        else local_pass<V, 2, INVERSE>(s, ML, L, lno, tw);
     }
 }
 
 // ------------------------------------------------------------------ the tile kernel
-struct TileArgs {
-    const double  *vin;
-    double        *vout;
-    const int64_t *tile_start;  // first output row of the tile (global)
-    const int32_t *tile_block;
-    const int64_t *blk_start;
-    const int32_t *blk_len;
-    const int32_t *blk_spec;
-    const double  *spectra;     // [n_spec][M+1]
-    const double2 *tw;          // [M]
-    const double  *means;       // [nb] or nullptr
-    int            lambda;
+template <typename T>
+struct TileArgsT {
+    const T                  *vin;
+    T                        *vout;
+    const int64_t            *tile_start;  // first output row of the tile (global)
+    const int32_t            *tile_block;
+    const int64_t            *blk_start;
+    const int32_t            *blk_len;
+    const int32_t            *blk_spec;
+    const T                  *spectra;     // [n_spec][M+1]
+    const typename CT<T>::V  *tw;          // [M]
+    const double             *means;       // [nb] or nullptr
+    int                       lambda;
 };
+typedef TileArgsT<double> TileArgs;
 
-template <int LOG_ML, int C>
-__global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgs a) {
-    extern __shared__ __align__(16) double2 smem[];
+template <typename T, int LOG_ML, int C>
+__global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgsT<T> a) {
+    using V = typename CT<T>::V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V            *smem = reinterpret_cast<V *>(smem_raw);
     constexpr int ML = 1 << LOG_ML;
     constexpr int M = ML * C;       // complex points per tile
     constexpr int N = 2 * M;        // real samples per tile
@@ -191,14 +219,25 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgs a) {
     const int     halo = a.lambda - 1;
     const int64_t ws = t0 - halo;               // window start (row of x[0])
     const int     E = N - 2 * halo;            // outputs per tile
-    const double  mu = a.means ? a.means[blk] : 0.0;
+    const T       mu = a.means ? (T) a.means[blk] : (T) 0;
 
     // ---- load this CTA's 2*ML real samples of the window (zero outside the block)
-    double       *sd = reinterpret_cast<double *>(smem);
+    T            *sd = reinterpret_cast<T *>(smem);
     const int64_t r0 = ws + (int64_t) rank * 2 * ML;
-    for (int j = threadIdx.x; j < 2 * ML; j += blockDim.x) {
-        const int64_t row = r0 + j;
-        sd[2 * swz(j >> 1) + (j & 1)] = (row >= bs && row < be) ? (__ldg(a.vin + row) - mu) : 0.0;
+    // batches of 8 independent loads per thread keep many HBM requests in flight
+    for (int j0 = threadIdx.x; j0 < 2 * ML; j0 += 8 * blockDim.x) {
+        T v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int     j = j0 + u * blockDim.x;
+            const int64_t row = r0 + j;
+            v[u] = (j < 2 * ML && row >= bs && row < be) ? __ldg(a.vin + row) : mu;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int j = j0 + u * blockDim.x;
+            if (j < 2 * ML) sd[2 * swzv(V{}, j >> 1) + (j & 1)] = v[u] - mu;
+        }
     }
 
     if constexpr (C > 1) {
@@ -206,11 +245,11 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgs a) {
         cluster.sync();
         // cross-CTA DIF stages: set q holds element c of CTA c at local q
         for (int q = rank * (ML / C) + threadIdx.x; q < (rank + 1) * (ML / C); q += blockDim.x) {
-            double2   v[C];
-            const int sq = swz(q);
+            V         v[C];
+            const int sq = swzv(V{}, q);
 #pragma unroll
             for (int c = 0; c < C; c++) v[c] = cluster.map_shared_rank(smem, c)[sq];
-            dif_set<C>(v, __ldg(a.tw + 2 * q));  // W_M^q = W_N^(2q)
+            dif_set<V, C>(v, __ldg(a.tw + 2 * q));  // W_M^q = W_N^(2q)
 #pragma unroll
             for (int c = 0; c < C; c++) cluster.map_shared_rank(smem, c)[sq] = v[c];
         }
@@ -219,50 +258,76 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgs a) {
         __syncthreads();
     }
 
-    local_fft<LOG_ML, false>(smem, logN, a.tw);
+    local_fft<V, LOG_ML, false>(smem, logN, a.tw);
 
     if constexpr (C > 1) cg::this_cluster().sync();
 
     // ---- real-FFT untangle, spectrum product, re-tangle (bit-reversed storage)
-    const double *H = a.spectra + (int64_t) a.blk_spec[blk] * (M + 1);
-    for (int p = threadIdx.x; p < ML; p += blockDim.x) {
-        const int P1 = rank * ML + p;
-        const int k = (int) (__brev((unsigned) P1) >> (32 - logM));
-        if (k > M / 2) continue;
-        const int k2 = (M - k) & (M - 1);
-        const int P2 = (int) (__brev((unsigned) k2) >> (32 - logM));
-        double2  *s1 = smem + swz(p);
-        double2  *s2;
-        if constexpr (C > 1) s2 = cg::this_cluster().map_shared_rank(smem, P2 / ML) + swz(P2 % ML);
-        else s2 = smem + swz(P2);
-        const double2 Z1 = *s1, Z2 = *s2;
-        const double2 E0 = make_double2(0.5 * (Z1.x + Z2.x), 0.5 * (Z1.y - Z2.y));
-        const double2 O0 = make_double2(0.5 * (Z1.y + Z2.y), -0.5 * (Z1.x - Z2.x));
-        const double  Hk = __ldg(H + k), Hm = __ldg(H + (M - k));
-        const double  ca = 0.5 * (Hk + Hm), cb = 0.5 * (Hk - Hm);
-        const double2 w = __ldg(a.tw + k);
-        const double2 wO = cmul(w, O0);
-        const double2 Ep = make_double2(ca * E0.x + cb * wO.x, ca * E0.y + cb * wO.y);
-        const double2 cE = cmulc(E0, w);  // conj(w) * E
-        const double2 Op = make_double2(cb * cE.x + ca * O0.x, cb * cE.y + ca * O0.y);
-        *s1 = make_double2(Ep.x - Op.y, Ep.y + Op.x);
-        if (P2 != P1) *s2 = make_double2(Ep.x + Op.y, -Ep.y + Op.x);
+    const T *H = a.spectra + (int64_t) a.blk_spec[blk] * (M + 1);
+    // Position P holds Z[rev(P)]; pairs (k, M-k) with k <= M/2 are handled by the
+    // owner of rev(k).  k <= M/2 exactly for even local positions plus the single
+    // position of k = M/2 (local index 1 of rank 0), so each thread walks even
+    // positions in batches of 4 with the spectrum and twiddle loads issued first.
+    constexpr int NPAIR = ML / 2;
+    const T       half = (T) 0.5;
+    for (int i0 = threadIdx.x; i0 < NPAIR + 1; i0 += 4 * blockDim.x) {
+        int  p1[4], p2[4];
+        T    hk[4], hm[4];
+        V    wk[4];
+        bool act[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int i = i0 + u * blockDim.x;
+            int       p = 2 * i;
+            act[u] = i < NPAIR;
+            if (i == NPAIR) {  // the k = M/2 pair: local position 1 of rank 0
+                p = 1;
+                act[u] = (rank == 0);
+            }
+            const int P1 = rank * ML + p;
+            const int k = act[u] ? (int) (__brev((unsigned) P1) >> (32 - logM)) : 0;
+            const int k2 = (M - k) & (M - 1);
+            p1[u] = p;
+            p2[u] = (int) (__brev((unsigned) k2) >> (32 - logM));
+            hk[u] = act[u] ? __ldg(H + k) : (T) 0;
+            hm[u] = act[u] ? __ldg(H + (M - k)) : (T) 0;
+            wk[u] = act[u] ? __ldg(a.tw + k) : mkv(wk[u], (T) 1, (T) 0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (!act[u]) continue;
+            const int P2 = p2[u];
+            V        *s1 = smem + swzv(V{}, p1[u]);
+            V        *s2;
+            if constexpr (C > 1) s2 = cg::this_cluster().map_shared_rank(smem, P2 / ML) + swzv(V{}, P2 % ML);
+            else s2 = smem + swzv(V{}, P2);
+            const V Z1 = *s1, Z2 = *s2;
+            const V E0 = mkv(Z1, half * (Z1.x + Z2.x), half * (Z1.y - Z2.y));
+            const V O0 = mkv(Z1, half * (Z1.y + Z2.y), -half * (Z1.x - Z2.x));
+            const T ca = half * (hk[u] + hm[u]), cb = half * (hk[u] - hm[u]);
+            const V wO = cmul(wk[u], O0);
+            const V Ep = mkv(Z1, ca * E0.x + cb * wO.x, ca * E0.y + cb * wO.y);
+            const V cE = cmulc(E0, wk[u]);  // conj(w) * E
+            const V Op = mkv(Z1, cb * cE.x + ca * O0.x, cb * cE.y + ca * O0.y);
+            *s1 = mkv(Z1, Ep.x - Op.y, Ep.y + Op.x);
+            if (P2 != rank * ML + p1[u]) *s2 = mkv(Z1, Ep.x + Op.y, -Ep.y + Op.x);
+        }
     }
 
     if constexpr (C > 1) cg::this_cluster().sync();
     else __syncthreads();
 
-    local_fft<LOG_ML, true>(smem, logN, a.tw);
+    local_fft<V, LOG_ML, true>(smem, logN, a.tw);
 
     if constexpr (C > 1) {
         cg::cluster_group cluster = cg::this_cluster();
         cluster.sync();
         for (int q = rank * (ML / C) + threadIdx.x; q < (rank + 1) * (ML / C); q += blockDim.x) {
-            double2   v[C];
-            const int sq = swz(q);
+            V         v[C];
+            const int sq = swzv(V{}, q);
 #pragma unroll
             for (int c = 0; c < C; c++) v[c] = cluster.map_shared_rank(smem, c)[sq];
-            dit_set<C>(v, __ldg(a.tw + 2 * q));  // W_M^q = W_N^(2q)
+            dit_set<V, C>(v, __ldg(a.tw + 2 * q));  // W_M^q = W_N^(2q)
 #pragma unroll
             for (int c = 0; c < C; c++) cluster.map_shared_rank(smem, c)[sq] = v[c];
         }
@@ -270,11 +335,11 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgs a) {
     }
 
     // ---- store the tile's central outputs, scaled by 1/M
-    const double  scale = 1.0 / (double) M;
+    const T       scale = (T) 1 / (T) M;
     const int64_t out_end = min(t0 + (int64_t) E, be);
     for (int j = threadIdx.x; j < 2 * ML; j += blockDim.x) {
         const int64_t row = r0 + j;
-        if (row >= t0 && row < out_end) a.vout[row] = sd[2 * swz(j >> 1) + (j & 1)] * scale;
+        if (row >= t0 && row < out_end) a.vout[row] = sd[2 * swzv(V{}, j >> 1) + (j & 1)] * scale;
     }
 }
 
@@ -300,12 +365,13 @@ __global__ void spectrum_kernel(const double *__restrict__ T, int lambda, int N,
 }
 
 // ------------------------------------------------------------------ block means and white noise
-__global__ void block_partial_sums(const double *__restrict__ v, const int64_t *__restrict__ chunk_start,
+template <typename T>
+__global__ void block_partial_sums(const T *__restrict__ v, const int64_t *__restrict__ chunk_start,
                                    const int32_t *__restrict__ chunk_len, double *__restrict__ partial) {
     const int64_t s = chunk_start[blockIdx.x];
     const int     n = chunk_len[blockIdx.x];
     double        acc = 0.0;
-    for (int j = threadIdx.x; j < n; j += blockDim.x) acc += v[s + j];
+    for (int j = threadIdx.x; j < n; j += blockDim.x) acc += (double) v[s + j];
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     __shared__ double ws[32];
     if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
@@ -378,19 +444,19 @@ static int choose_fft(int lambda, int64_t max_block, int *log_ml, int *cluster) 
 typedef void (*tile_fn)(TileArgs);
 static tile_fn pick_kernel(int log_ml, int C) {
     if (C == 1) switch (log_ml) {
-            case 6: return toeplitz_tile_kernel<6, 1>;
-            case 7: return toeplitz_tile_kernel<7, 1>;
-            case 8: return toeplitz_tile_kernel<8, 1>;
-            case 9: return toeplitz_tile_kernel<9, 1>;
-            case 10: return toeplitz_tile_kernel<10, 1>;
-            case 11: return toeplitz_tile_kernel<11, 1>;
-            case 12: return toeplitz_tile_kernel<12, 1>;
-            case 13: return toeplitz_tile_kernel<13, 1>;
+            case 6: return toeplitz_tile_kernel<double, 6, 1>;
+            case 7: return toeplitz_tile_kernel<double, 7, 1>;
+            case 8: return toeplitz_tile_kernel<double, 8, 1>;
+            case 9: return toeplitz_tile_kernel<double, 9, 1>;
+            case 10: return toeplitz_tile_kernel<double, 10, 1>;
+            case 11: return toeplitz_tile_kernel<double, 11, 1>;
+            case 12: return toeplitz_tile_kernel<double, 12, 1>;
+            case 13: return toeplitz_tile_kernel<double, 13, 1>;
         }
     if (log_ml == 13) switch (C) {
-            case 2: return toeplitz_tile_kernel<13, 2>;
-            case 4: return toeplitz_tile_kernel<13, 4>;
-            case 8: return toeplitz_tile_kernel<13, 8>;
+            case 2: return toeplitz_tile_kernel<double, 13, 2>;
+            case 4: return toeplitz_tile_kernel<double, 13, 4>;
+            case 8: return toeplitz_tile_kernel<double, 13, 8>;
         }
     return nullptr;
 }
@@ -522,6 +588,9 @@ extern "C" int mdp_noise_create(mdp_context *ctx, int nb_blocks, const int64_t *
             spec_of[b] = found;
         }
         N->n_spec = (int) uniq.size();
+        N->h_Tuniq.resize((size_t) N->n_spec * lambda);
+        for (int u = 0; u < N->n_spec; u++)
+            memcpy(N->h_Tuniq.data() + (size_t) u * lambda, h_T + (size_t) uniq[u] * lambda, sizeof(double) * lambda);
         cudaMemcpy(N->blk_spec.p, spec_of.data(), 4 * nb_blocks, cudaMemcpyHostToDevice);
         if ((rc = N->spectra.alloc(sizeof(double) * (size_t) N->n_spec * (M + 1)))) return fail(rc);
         DevBuf dT;
@@ -573,7 +642,7 @@ int mdp_block_means(mdp_context *ctx, const mdp_noise *N, const double *d_v, dou
         MDP_CUDA(cudaMemsetAsync(d_means, 0, 8 * N->nb, ctx->stream));
         return MDP_OK;
     }
-    block_partial_sums<<<X->n_chunks, 512, 0, ctx->stream>>>(d_v, X->chunk_start.as<int64_t>(),
+    block_partial_sums<double><<<X->n_chunks, 512, 0, ctx->stream>>>(d_v, X->chunk_start.as<int64_t>(),
                                                              X->chunk_len.as<int32_t>(), X->partial.as<double>());
     MDP_CHECK_LAUNCH(ctx);
     block_means_final<<<grid_for(N->nb, 128, 1024), 128, 0, ctx->stream>>>(
@@ -682,6 +751,261 @@ int mdp_matvec_blockmeans(mdp_context *ctx, const mdp_pointing *A, const mdp_noi
     return MDP_OK;
 }
 
+// ------------------------------------------------------------------ FP32 operator
+typedef void (*tile_fn32)(TileArgsT<float>);
+static tile_fn32 pick_kernel32(int log_ml, int C) {
+    if (C == 1) switch (log_ml) {
+            case 6: return toeplitz_tile_kernel<float, 6, 1>;
+            case 7: return toeplitz_tile_kernel<float, 7, 1>;
+            case 8: return toeplitz_tile_kernel<float, 8, 1>;
+            case 9: return toeplitz_tile_kernel<float, 9, 1>;
+            case 10: return toeplitz_tile_kernel<float, 10, 1>;
+            case 11: return toeplitz_tile_kernel<float, 11, 1>;
+            case 12: return toeplitz_tile_kernel<float, 12, 1>;
+            case 13: return toeplitz_tile_kernel<float, 13, 1>;
+            case 14: return toeplitz_tile_kernel<float, 14, 1>;
+        }
+    if (log_ml == 14) switch (C) {
+            case 2: return toeplitz_tile_kernel<float, 14, 2>;
+            case 4: return toeplitz_tile_kernel<float, 14, 4>;
+            case 8: return toeplitz_tile_kernel<float, 14, 8>;
+        }
+    return nullptr;
+}
+
+// FP32 tiles hold 2^14 complex points per CTA (128 KiB); same cost model as FP64
+static int choose_fft32(int lambda, int64_t max_block, int *log_ml, int *cluster) {
+    const char *env = getenv("MDP_TOEPLITZ_FFT32");
+    int         forced = env ? atoi(env) : 0;
+    double      best = 1e300;
+    int         bl = -1, bc = 1;
+    for (int C = 1; C <= 8; C <<= 1)
+        for (int lml = 6; lml <= 14; lml++) {
+            if (C > 1 && lml != 14) continue;
+            const int64_t N = 2LL * C * (1LL << lml);
+            const int64_t E = N - 2LL * (lambda - 1);
+            if (E < 1) continue;
+            if (forced && N != forced) continue;
+            int logN = lml + 1;
+            for (int c = C; c > 1; c >>= 1) logN++;
+            double eff = (double) std::min<int64_t>(E, max_block);
+            double cost = (double) N / eff * (logN + 3) + (C > 1 ? 3.0 * std::log2((double) C) : 0.0);
+            if (E < N / 4 && !forced) cost *= 1.5;
+            if (cost < best) {
+                best = cost;
+                bl = lml;
+                bc = C;
+            }
+        }
+    if (bl < 0) return MDP_EUNSUPPORTED;
+    *log_ml = bl;
+    *cluster = bc;
+    return MDP_OK;
+}
+
+__global__ void to_float_kernel(const double *__restrict__ in, float *__restrict__ out, int64_t n) {
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        out[i] = (float) in[i];
+}
+
+int mdp_noise_prepare_fp32(mdp_context *ctx, mdp_noise *N) {
+    if (N->f32.ready) return MDP_OK;
+    if (N->lambda == 1) {
+        N->f32.ready = 1;
+        return MDP_OK;
+    }
+    int64_t max_block = 0;
+    for (int b = 0; b < N->nb; b++) max_block = std::max<int64_t>(max_block, N->h_n[b]);
+    MDP_TRY(choose_fft32(N->lambda, max_block, &N->f32.log2_ml, &N->f32.cluster));
+    const int     M = N->f32.cluster << N->f32.log2_ml;
+    const int     Nn = 2 * M;
+    const int64_t E = (int64_t) Nn - 2LL * (N->lambda - 1);
+    N->f32.fft_n = Nn;
+    std::vector<int64_t> ts;
+    std::vector<int32_t> tb;
+    for (int b = 0; b < N->nb; b++)
+        for (int64_t o = 0; o < N->h_n[b]; o += E) {
+            ts.push_back(N->h_idv[b] + o);
+            tb.push_back(b);
+        }
+    N->f32.n_tiles = (int64_t) ts.size();
+    MDP_TRY(N->f32.tile_start.alloc(8 * std::max<size_t>(ts.size(), 1)));
+    MDP_TRY(N->f32.tile_block.alloc(4 * std::max<size_t>(tb.size(), 1)));
+    if (!ts.empty()) {
+        MDP_CUDA(cudaMemcpy(N->f32.tile_start.p, ts.data(), 8 * ts.size(), cudaMemcpyHostToDevice));
+        MDP_CUDA(cudaMemcpy(N->f32.tile_block.p, tb.data(), 4 * tb.size(), cudaMemcpyHostToDevice));
+    }
+    // twiddles: long double on the host, FP64 copy for the spectra, FP32 copy for the tiles
+    std::vector<double2> tw(M);
+    std::vector<float2>  twf(M);
+    for (int k = 0; k < M; k++) {
+        long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double) k / (long double) Nn;
+        tw[k] = make_double2((double) cosl(ang), (double) sinl(ang));
+        twf[k] = make_float2((float) cosl(ang), (float) sinl(ang));
+    }
+    DevBuf tw64, spec64, dT;
+    MDP_TRY(tw64.alloc(sizeof(double2) * M));
+    MDP_TRY(N->f32.twiddle.alloc(sizeof(float2) * M));
+    MDP_CUDA(cudaMemcpy(tw64.p, tw.data(), sizeof(double2) * M, cudaMemcpyHostToDevice));
+    MDP_CUDA(cudaMemcpy(N->f32.twiddle.p, twf.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
+    MDP_TRY(spec64.alloc(sizeof(double) * (size_t) N->n_spec * (M + 1)));
+    MDP_TRY(N->f32.spectra.alloc(sizeof(float) * (size_t) N->n_spec * (M + 1)));
+    MDP_TRY(dT.alloc(sizeof(double) * N->lambda));
+    for (int u = 0; u < N->n_spec; u++) {
+        MDP_CUDA(cudaMemcpy(dT.p, N->h_Tuniq.data() + (size_t) u * N->lambda, sizeof(double) * N->lambda,
+                            cudaMemcpyHostToDevice));
+        spectrum_kernel<<<grid_for(M + 1, 128, 4096), 128, 0, ctx->stream>>>(
+                dT.as<double>(), N->lambda, Nn, tw64.as<double2>(), spec64.as<double>() + (size_t) u * (M + 1));
+        MDP_CHECK_LAUNCH(ctx);
+    }
+    const int64_t ns = (int64_t) N->n_spec * (M + 1);
+    to_float_kernel<<<grid_for(ns, 256, 1024), 256, 0, ctx->stream>>>(spec64.as<double>(), N->f32.spectra.as<float>(), ns);
+    MDP_CHECK_LAUNCH(ctx);
+    MDP_CUDA(cudaStreamSynchronize(ctx->stream));
+    tile_fn32 fn = pick_kernel32(N->f32.log2_ml, N->f32.cluster);
+    const int smem = (int) (sizeof(float2) << N->f32.log2_ml);
+    MDP_CUDA(cudaFuncSetAttribute((const void *) fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    if (N->f32.cluster > 1)
+        MDP_CUDA(cudaFuncSetAttribute((const void *) fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    N->f32.ready = 1;
+    return MDP_OK;
+}
+
+__global__ void white32_kernel(const float *__restrict__ vin, float *__restrict__ vout,
+                               const int64_t *__restrict__ bstart, const int32_t *__restrict__ blen,
+                               const double *__restrict__ t0) {
+    const int     b = blockIdx.y;
+    const int64_t s = bstart[b];
+    const int     n = blen[b];
+    const float   d = (float) t0[b];
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) vout[s + j] = d * vin[s + j];
+}
+
+// out = N^-1 in with the FP32 tile kernels; d_means (FP64 block means of in)
+// may be given (fused into the producer of in) or nullptr
+int mdp_stbmm_impl32(mdp_context *ctx, mdp_noise *N, const float *d_in, float *d_out, const double *d_means) {
+    NoiseExtra *X = g_extra.at(N);
+    MDP_TRY(mdp_noise_prepare_fp32(ctx, N));
+    if (!X->covers_all)
+        MDP_CUDA(cudaMemcpyAsync(d_out, d_in, sizeof(float) * N->nrow_end, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (N->lambda == 1) {
+        dim3 grid(64, N->nb);
+        white32_kernel<<<grid, 256, 0, ctx->stream>>>(d_in, d_out, N->blk_start.as<int64_t>(), N->blk_len.as<int32_t>(),
+                                                      N->blk_t0.as<double>());
+        MDP_CHECK_LAUNCH(ctx);
+        return MDP_OK;
+    }
+    if (!d_means) {
+        if (X->n_chunks > 0) {
+            block_partial_sums<float><<<X->n_chunks, 512, 0, ctx->stream>>>(
+                    d_in, X->chunk_start.as<int64_t>(), X->chunk_len.as<int32_t>(), X->partial.as<double>());
+            MDP_CHECK_LAUNCH(ctx);
+            block_means_final<<<grid_for(N->nb, 128, 1024), 128, 0, ctx->stream>>>(
+                    X->partial.as<double>(), X->blk_chunk0.as<int32_t>(), X->blk_nchunk.as<int32_t>(),
+                    N->blk_len.as<int32_t>(), N->nb, N->means.as<double>());
+            MDP_CHECK_LAUNCH(ctx);
+        }
+        d_means = N->means.as<double>();
+    }
+    if (N->f32.n_tiles == 0) return MDP_OK;
+    TileArgsT<float> a;
+    a.vin = d_in;
+    a.vout = d_out;
+    a.tile_start = N->f32.tile_start.as<int64_t>();
+    a.tile_block = N->f32.tile_block.as<int32_t>();
+    a.blk_start = N->blk_start.as<int64_t>();
+    a.blk_len = N->blk_len.as<int32_t>();
+    a.blk_spec = N->blk_spec.as<int32_t>();
+    a.spectra = N->f32.spectra.as<float>();
+    a.tw = N->f32.twiddle.as<float2>();
+    a.means = d_means;
+    a.lambda = N->lambda;
+    tile_fn32 fn = pick_kernel32(N->f32.log2_ml, N->f32.cluster);
+    if (N->f32.n_tiles * N->f32.cluster > 0x7fffffffLL) return MDP_EUNSUPPORTED;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned) (N->f32.n_tiles * N->f32.cluster));
+    cfg.blockDim = dim3(std::min(512, std::max(64, (1 << N->f32.log2_ml) / 16)));
+    cfg.dynamicSmemBytes = sizeof(float2) << N->f32.log2_ml;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = N->f32.cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    MDP_CUDA(cudaLaunchKernelEx(&cfg, fn, a));
+    MDP_CHECK_LAUNCH(ctx);
+    return MDP_OK;
+}
+
+// y32 = P x (x FP64, weights FP32) fused with FP64 block-mean partial sums
+__global__ void __launch_bounds__(512) matvec32_chunk_sums_kernel(const int32_t *__restrict__ off,
+                                                                  const float *__restrict__ w,
+                                                                  const double *__restrict__ x, float *__restrict__ y,
+                                                                  const int64_t *__restrict__ chunk_start,
+                                                                  const int32_t *__restrict__ chunk_len,
+                                                                  double *__restrict__ partial) {
+    const int64_t s = chunk_start[blockIdx.x];
+    const int     n = chunk_len[blockIdx.x];
+    double        acc = 0.0;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const int64_t t = s + j;
+        const int32_t o = off[t];
+        float         v = 0.0f;
+        if (o >= 0)
+            v = w[3 * t] * (float) __ldg(x + o) + w[3 * t + 1] * (float) __ldg(x + o + 1) +
+                w[3 * t + 2] * (float) __ldg(x + o + 2);
+        y[t] = v;
+        acc += (double) v;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    __shared__ double ws[16];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = (threadIdx.x < (blockDim.x >> 5)) ? ws[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) partial[blockIdx.x] = v;
+    }
+}
+
+int mdp_matvec32_blockmeans(mdp_context *ctx, const mdp_pointing *A, const mdp_noise *N, const double *d_x,
+                            float *d_y) {
+    NoiseExtra *X = g_extra.at(N);
+    if (!A->triplet || !A->w32.p || !X->covers_all || N->lambda == 1 || N->nrow_end != A->m || X->n_chunks == 0)
+        return MDP_EUNSUPPORTED;
+    matvec32_chunk_sums_kernel<<<X->n_chunks, 512, 0, ctx->stream>>>(A->off.as<int32_t>(), A->w32.as<float>(), d_x, d_y,
+                                                                     X->chunk_start.as<int64_t>(),
+                                                                     X->chunk_len.as<int32_t>(), X->partial.as<double>());
+    MDP_CHECK_LAUNCH(ctx);
+    block_means_final<<<grid_for(N->nb, 128, 1024), 128, 0, ctx->stream>>>(
+            X->partial.as<double>(), X->blk_chunk0.as<int32_t>(), X->blk_nchunk.as<int32_t>(), N->blk_len.as<int32_t>(),
+            N->nb, N->means.as<double>());
+    MDP_CHECK_LAUNCH(ctx);
+    return MDP_OK;
+}
+
+extern "C" int mdp_noise_tile_fp32(mdp_context *ctx, mdp_noise *N, int *fft_size, int *cluster_ctas,
+                                   int64_t *n_tiles) {
+    if (!ctx || !N) return MDP_EINVAL;
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    MDP_TRY(mdp_noise_prepare_fp32(ctx, N));
+    if (fft_size) *fft_size = N->f32.fft_n;
+    if (cluster_ctas) *cluster_ctas = N->f32.cluster;
+    if (n_tiles) *n_tiles = N->f32.n_tiles;
+    return MDP_OK;
+}
+
+extern "C" int mdp_stbmm_fp32(mdp_context *ctx, mdp_noise *N, const float *d_in, float *d_out) {
+    if (!ctx || !N || !d_in || !d_out || d_in == d_out) {
+        mdp_set_error("mdp_stbmm_fp32: invalid arguments (in-place is not supported)");
+        return MDP_EINVAL;
+    }
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    return mdp_stbmm_impl32(ctx, N, d_in, d_out, nullptr);
+}
+
 extern "C" int mdp_stbmm(mdp_context *ctx, const mdp_noise *N, const double *d_in, double *d_out) {
     if (!ctx || !N || !d_in || !d_out) return MDP_EINVAL;
     const double *src = d_in;
@@ -754,7 +1078,7 @@ extern "C" int mdp_stbmm_noalloc(mdp_context *ctx, const mdp_noise *N, const dou
     double *partial = scratch;                 // [n_chunks], each written before it is read
     double *means = scratch + X->n_chunks;     // [nb], each written before it is read
     if (X->n_chunks > 0) {
-        block_partial_sums<<<X->n_chunks, 512, 0, ctx->stream>>>(d_in, X->chunk_start.as<int64_t>(),
+        block_partial_sums<double><<<X->n_chunks, 512, 0, ctx->stream>>>(d_in, X->chunk_start.as<int64_t>(),
                                                                  X->chunk_len.as<int32_t>(), partial);
         MDP_CHECK_LAUNCH(ctx);
         block_means_final<<<grid_for(N->nb, 128, 1024), 128, 0, ctx->stream>>>(

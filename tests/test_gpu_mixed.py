@@ -1,0 +1,80 @@
+"""Mixed precision: the FP32 inverse-noise operator against the exact product
+(FP32 tolerance 1e-5 norm-wise), and the mixed-precision solve (FP32 operator
+inside FP64 iterative refinement) against the FP64 GPU solve and the oracle:
+maps within 1e-8 relative, max over I/Q/U."""
+import os
+
+import numpy as np
+import pytest
+
+from midapack_b200 import synth
+from oracle import restate as R
+from tests._cases import solver_cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("lam,sizes,fft", [
+    (64, [5000, 777], None),
+    (300, [9000], None),
+    (2048, [40000, 5000], None),
+    (4096, [70000], 32768),     # single FP32 CTA
+    (8192, [70000], 65536),     # 2-CTA cluster
+    (16384, [140000], 131072),  # 4-CTA cluster
+    (16384, [300000], 262144),  # 8-CTA cluster
+])
+def test_stbmm_fp32_vs_exact(gpu_ctx, lam, sizes, fft):
+    import torch
+    import midapack_b200 as mb
+    rng = np.random.default_rng(lam)
+    invtt = np.tile(synth.invtt_row(max(4 * lam, 4096), lam, 1.0), len(sizes))
+    v = rng.standard_normal(sum(sizes)) + 1.0
+    old = os.environ.get("MDP_TOEPLITZ_FFT32")
+    if fft:
+        os.environ["MDP_TOEPLITZ_FFT32"] = str(fft)
+    try:
+        N = mb.Noise(gpu_ctx, sizes, lam, invtt)
+        vin = torch.from_numpy(v).float().cuda()
+        out = torch.empty_like(vin)
+        N.apply_fp32(vin, out)
+        torch.cuda.synchronize()
+    finally:
+        if fft:
+            if old is None:
+                del os.environ["MDP_TOEPLITZ_FFT32"]
+            else:
+                os.environ["MDP_TOEPLITZ_FFT32"] = old
+    ref = R.stbmm(v.astype(np.float32).astype(np.float64), np.array(sizes), lam, invtt,
+                  exact=sum(sizes) * lam < 3e8)
+    assert _rel(out.double().cpu().numpy(), ref) < 1e-5
+
+
+@pytest.mark.parametrize("case", ["gaps", "cut", "cut_gaps"])
+def test_mixed_solve_matches_fp64(gpu_ctx, case):
+    import torch
+    import midapack_b200 as mb
+    wl = solver_cases()[case]()
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    m = wl.n_samples
+    outs = []
+    for mixed in (False, True):
+        w = d(wl.weights)
+        P = mb.Pointing(gpu_ctx, d(wl.pix), w, m, 3)
+        N = mb.Noise(gpu_ctx, wl.block_sizes, wl.lam, wl.invtt)
+        fn = mb.gls_solve_mixed if mixed else mb.gls_solve
+        # the map error is bounded by cond(A) x the residual: solve to 1e-12 to compare maps at 1e-8
+        x, lst, cond, hits, res, info = fn(gpu_ctx, P, N, d(wl.signal), d(wl.noise), tol=1e-12, maxiter=900)
+        assert info.converged
+        outs.append((x.cpu().numpy(), lst.cpu().numpy(), hits.cpu().numpy(), info))
+    (x64, l64, h64, i64), (x32, l32, h32, i32) = outs
+    assert np.array_equal(l64, l32) and np.array_equal(h64, h32)
+    assert i32.outer_iterations >= 1 and i32.fp64_applications == i32.outer_iterations + 1
+    for k in range(3):
+        assert _rel(x32[k::3], x64[k::3]) < 1e-8, (k, _rel(x32[k::3], x64[k::3]))
+    o = R.pcg(wl.pix, wl.weights, wl.signal, wl.noise, wl.block_sizes, wl.lam, wl.invtt, tol=1e-12, maxiter=900)
+    for k in range(3):
+        assert _rel(x32[k::3], o.x[k::3]) < 1e-8
