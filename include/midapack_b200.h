@@ -94,6 +94,14 @@ int  mdp_noise_tile(const mdp_noise *N, int *fft_size, int *cluster_ctas, int64_
 int  mdp_stbmm_fp32(mdp_context *ctx, mdp_noise *N, const float *d_in, float *d_out);
 /* FP32 tile plan (builds it on first use) */
 int  mdp_noise_tile_fp32(mdp_context *ctx, mdp_noise *N, int *fft_size, int *cluster_ctas, int64_t *n_tiles);
+/* Launch shape of a tile plan (fp32 = 0: FP64 tiles, 1: FP32 tiles, built on
+ * first use): 2^log2_cta_points complex points per CTA, CTAs per cluster,
+ * threads per CTA, and whether the autotuner picked it (1) by timing the
+ * candidate plans on this device, or the cost model did (0).  The autotuner
+ * runs once per precision, band (ceil log2 lambda) and block length class;
+ * MDP_TOEPLITZ_TUNE=0 switches it off. */
+int  mdp_noise_plan(mdp_context *ctx, mdp_noise *N, int fp32, int *log2_cta_points, int *cluster_ctas,
+                    int *threads, int *tuned);
 /* No counterpart in the reference.  out = N^-1 in like mdp_stbmm, but the call
  * allocates no device memory: for callers that cannot call cudaMalloc while
  * they apply the operator (a memory arena or pool that owns the device memory,
@@ -153,6 +161,56 @@ int mdp_gls_solve_mixed(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, c
                         const double *d_noise, const mdp_solve_params *params, double inner_tol, int inner_maxiter,
                         double *d_x, int32_t *d_lstid, double *d_cond, int32_t *d_hits, double *h_res_rel,
                         mdp_solve_info *info);
+
+/* No counterpart in the reference (MLmap solves one right-hand side per call).
+ * Multi-RHS mixed-precision solve: nrhs right-hand sides that share A and N,
+ * column r's TOD being d_r = noise_r (+ signal on column signal_col, zeroed on
+ * cut samples as in MLmap).  Each column is the mdp_gls_solve_mixed solve
+ * (same block-Jacobi preconditioner and cut, built once, FP64 refinement, stop
+ * on sum(g^2) <= tol^2 sum(g0^2)); the inner FP32 PCGs of up to `slots`
+ * columns advance together in batched iterations (one pass over the pointing
+ * for all of them, their Toeplitz tiles in one launch), a column that
+ * converges leaves its slot to the next column, and the batched iteration is
+ * replayed as a CUDA graph (use_graph = 1).  slots = 0 times one batched
+ * operator application for 1, 2, 4 and 8 slots and keeps the cheapest per
+ * column.  Needs the (I,Q,U) triplet layout, lambda > 1 and noise blocks
+ * covering every row.
+ *   d_noise   column r at d_noise + r*noise_stride elements (float when
+ *             noise_fp32 = 1, else double); FP32 values are used exactly
+ *   d_signal  FP64 signal of column signal_col (signal_col < 0: none)
+ *   d_x       [nrhs][n_map] solutions (n_map after the cut, as mdp_gls_solve)
+ *   col_info  [nrhs] per-column iterations, refinements, convergence, res0/res */
+typedef struct {
+    double tol;            /* relative residual of the FP64 stop test */
+    int    maxiter;        /* inner iterations per column, all refinements together */
+    double inner_tol;      /* relative residual of each inner FP32 solve */
+    int    inner_maxiter;  /* iterations of each inner solve */
+    int    slots;          /* columns iterated together: 1, 2, 4, 8, or 0 = timed choice */
+    int    use_graph;      /* 1: replay the batched iteration as a CUDA graph */
+    int    verbose;
+} mdp_multi_params;
+
+typedef struct {
+    int    iterations;        /* inner iterations of this column */
+    int    outer_iterations;  /* FP64 refinement steps */
+    int    converged;
+    double res0, res;         /* sum(g^2) at x = 0 and at the end */
+} mdp_multi_col_info;
+
+typedef struct {
+    int     slots;                /* columns per batched iteration */
+    int     graph;                /* 1 when the iteration ran as a CUDA graph */
+    int     total_iterations;     /* sum of the columns' inner iterations */
+    int     batched_iterations;   /* batched iterations launched */
+    int     fp64_applications;    /* FP64 operator applications (refinement residuals) */
+    int64_t n_map, n_cut;
+    double  precond_seconds, solve_seconds;
+} mdp_multi_info;
+
+int mdp_gls_solve_multi(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, int nrhs, const void *d_noise,
+                        int noise_fp32, int64_t noise_stride, const double *d_signal, int signal_col,
+                        const mdp_multi_params *params, double *d_x, int32_t *d_lstid, double *d_cond,
+                        int32_t *d_hits, mdp_multi_col_info *col_info, mdp_multi_info *info);
 
 #ifdef __cplusplus
 }

@@ -37,6 +37,22 @@ class SolveInfo(ct.Structure):
                 ("solve_seconds", ct.c_double), ("outer_iterations", ct.c_int), ("fp64_applications", ct.c_int)]
 
 
+class MultiParams(ct.Structure):
+    _fields_ = [("tol", ct.c_double), ("maxiter", ct.c_int), ("inner_tol", ct.c_double), ("inner_maxiter", ct.c_int),
+                ("slots", ct.c_int), ("use_graph", ct.c_int), ("verbose", ct.c_int)]
+
+
+class MultiColInfo(ct.Structure):
+    _fields_ = [("iterations", ct.c_int), ("outer_iterations", ct.c_int), ("converged", ct.c_int),
+                ("res0", ct.c_double), ("res", ct.c_double)]
+
+
+class MultiInfo(ct.Structure):
+    _fields_ = [("slots", ct.c_int), ("graph", ct.c_int), ("total_iterations", ct.c_int),
+                ("batched_iterations", ct.c_int), ("fp64_applications", ct.c_int), ("n_map", ct.c_int64),
+                ("n_cut", ct.c_int64), ("precond_seconds", ct.c_double), ("solve_seconds", ct.c_double)]
+
+
 # exported symbols of include/*.h, with their ctypes signatures
 _SIGS = {
     # device API (include/midapack_b200.h)
@@ -68,6 +84,11 @@ _SIGS = {
     "mdp_noise_tile_fp32": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int),
                                        ct.POINTER(ct.c_int64)]),
     "mdp_noise_tile": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int), ct.POINTER(ct.c_int64)]),
+    "mdp_gls_solve_multi": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int,
+                                       ct.c_int64, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                       ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mdp_noise_plan": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_int, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int),
+                                  ct.POINTER(ct.c_int), ct.POINTER(ct.c_int)]),
     "mdp_gls_solve": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                  ct.POINTER(SolveParams), ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                  c_f64p, ct.POINTER(SolveInfo)]),
@@ -244,15 +265,26 @@ class Noise:
                                      bs.ctypes.data_as(c_i32p), lam, tt.ctypes.data_as(c_f64p), ct.byref(self.h)),
               "mdp_noise_create")
 
+    def _plan(self, fp32: int):
+        lm, c, th, tu = ct.c_int(), ct.c_int(), ct.c_int(), ct.c_int()
+        check(lib().mdp_noise_plan(self.ctx.h, self.h, fp32, ct.byref(lm), ct.byref(c), ct.byref(th), ct.byref(tu)))
+        return dict(cta_points=1 << lm.value, threads=th.value, tuned=bool(tu.value))
+
     def tile(self):
         n, c, t = ct.c_int(), ct.c_int(), ct.c_int64()
         check(lib().mdp_noise_tile(self.h, ct.byref(n), ct.byref(c), ct.byref(t)))
-        return dict(fft_n=n.value, cluster=c.value, n_tiles=t.value)
+        out = dict(fft_n=n.value, cluster=c.value, n_tiles=t.value)
+        if n.value:
+            out.update(self._plan(0))
+        return out
 
     def tile_fp32(self):
         n, c, t = ct.c_int(), ct.c_int(), ct.c_int64()
         check(lib().mdp_noise_tile_fp32(self.ctx.h, self.h, ct.byref(n), ct.byref(c), ct.byref(t)))
-        return dict(fft_n=n.value, cluster=c.value, n_tiles=t.value)
+        out = dict(fft_n=n.value, cluster=c.value, n_tiles=t.value)
+        if n.value:
+            out.update(self._plan(1))
+        return out
 
     def apply(self, vin, vout):
         check(lib().mdp_stbmm(self.ctx.h, self.h, ct.c_void_p(_ptr(vin)), ct.c_void_p(_ptr(vout))), "mdp_stbmm")
@@ -311,6 +343,38 @@ def gls_solve_mixed(ctx: Context, A: Pointing, N: Noise, signal, noise, tol=1e-8
           "mdp_gls_solve_mixed")
     n = info.n_map
     return x[:n], lst[:n], cond[:n // 3], hits[:n // 3], res[:info.outer_iterations + 1], info
+
+
+def gls_solve_multi(ctx: Context, A: Pointing, N: Noise, noise, signal=None, signal_col=-1, tol=1e-8, maxiter=500,
+                    inner_tol=1e-4, inner_maxiter=100, slots=0, use_graph=True, verbose=False):
+    """Multi-RHS mixed-precision solve of the columns noise[r] (+ signal on column signal_col).
+
+    noise: device tensor [nrhs, m] (float32 or float64, rows contiguous).  Returns (x [nrhs, n_map],
+    lstid, cond, hits, per-column info list, MultiInfo)."""
+    import torch
+    if noise.dim() != 2 or noise.stride(1) != 1:
+        raise ValueError("noise must be a [nrhs, m] tensor with contiguous rows")
+    nrhs = noise.shape[0]
+    n0 = A.shape()["n_map"]
+    x = torch.empty((nrhs, max(n0, 1)), dtype=torch.float64, device="cuda")
+    lst = torch.empty(max(n0, 1), dtype=torch.int32, device="cuda")
+    cond = torch.empty(max(n0 // 3, 1), dtype=torch.float64, device="cuda")
+    hits = torch.empty(max(n0 // 3, 1), dtype=torch.int32, device="cuda")
+    prm = MultiParams(tol, maxiter, inner_tol, inner_maxiter, slots, 1 if use_graph else 0, 1 if verbose else 0)
+    ci = (MultiColInfo * nrhs)()
+    info = MultiInfo()
+    fp32 = 1 if noise.dtype == torch.float32 else 0
+    if not fp32 and noise.dtype != torch.float64:
+        raise ValueError("noise must be float32 or float64")
+    check(lib().mdp_gls_solve_multi(ctx.h, A.h, N.h, nrhs, ct.c_void_p(noise.data_ptr()), fp32,
+                                    noise.stride(0), ct.c_void_p(_ptr(signal) if signal is not None else 0),
+                                    signal_col, ct.byref(prm), ct.c_void_p(x.data_ptr()),
+                                    ct.c_void_p(lst.data_ptr()), ct.c_void_p(cond.data_ptr()),
+                                    ct.c_void_p(hits.data_ptr()), ci, ct.byref(info)), "mdp_gls_solve_multi")
+    n = info.n_map
+    # the solutions are stored with stride n_map (after the cut)
+    xs = x.reshape(-1)[: nrhs * n].reshape(nrhs, n)
+    return xs, lst[:n], cond[:n // 3], hits[:n // 3], list(ci), info
 
 
 def mlmap_host(wl_pix, wl_weights, signal, noise, block_sizes, lam, invtt, nside, tol=1e-8, maxiter=500):

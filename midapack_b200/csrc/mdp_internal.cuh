@@ -91,6 +91,14 @@ struct mdp_context {
 };
 
 // ---------------------------------------------------------------- pointing
+struct mdp_pt_bins {
+    int     valid = 0;
+    int     bin_pix = 0;
+    int64_t nbins = 0;
+    DevBuf  start;   // int64 [nbins+1] offsets into perm
+    DevBuf  perm;    // uint32 [valid rows] sample index, grouped by bin
+};
+
 struct mdp_pointing {
     int64_t       m = 0;
     int           nnz = 0;
@@ -101,47 +109,50 @@ struct mdp_pointing {
     DevBuf        lindices;           // int32 [lcount]
     DevBuf        local;              // int32 [m*nnz] (general layout only)
     DevBuf        off;                // int32 [m]: map offset 3q, -1 trash row, -2 cut row (triplet layout)
-    // P^T by map bins (triplet layout): samples grouped by bins of bin_pix pixels
-    int           bins_valid = 0;
-    int           bin_pix = 0;
-    int64_t       nbins = 0;
-    DevBuf        bin_start;          // int64 [nbins+1] offsets into bin_perm
-    DevBuf        bin_perm;           // uint32 [valid rows] sample index, grouped by bin
+    // P^T by map bins (triplet layout): samples grouped by bins of bin_pix
+    // pixels; bins for one map, and finer bins for the column batches of the
+    // multi-RHS solver (bin_pix / columns)
+    mdp_pt_bins   bins;
+    mdp_pt_bins   mbins;
     DevBuf        w32;                // float [m*3] weights for the FP32 operator (built on first use)
     int64_t n_map() const { return lcount - (int64_t) nnz * trash_pix; }
 };
 
 // ---------------------------------------------------------------- noise
+// One tile plan of the inverse-noise operator: FP64 tiles (the operator of
+// the reference) or FP32 tiles (the inner operator of the mixed-precision
+// solver).  V = double2 or float2.
+struct mdp_tile_plan {
+    int     ready = 0;
+    int     log2_ml = 0;   // per-CTA complex points = 2^log2_ml
+    int     cluster = 1;   // CTAs per tile
+    int     threads = 0;   // threads per CTA
+    int     fft_n = 0;     // real FFT size N = 2 * cluster * 2^log2_ml
+    int     tuned = 0;     // 1 when picked by timing the candidates on the device
+    int64_t n_tiles = 0;
+    DevBuf  tile_start;    // int64 [n_tiles] first output row (global)
+    DevBuf  tile_block;    // int32 [n_tiles]
+    DevBuf  spectra;       // V [n_spec][N/4+1]: spectrum pairs in tile position order
+    DevBuf  ltw, twm, ttw; // packed local-pass, cross-CTA and twist twiddles
+};
+
 struct mdp_noise {
     int                  nb = 0;
     int                  lambda = 0;
     int64_t              nrow_end = 0;   // max(idv+n)
+    int64_t              max_block = 0;
     std::vector<int64_t> h_idv;
     std::vector<int32_t> h_n;
     std::vector<double>  h_T0;           // diagonal of each block
-    // tile plan
-    int     log2_ml = 0;   // per-CTA complex points = 2^log2_ml
-    int     cluster = 1;   // CTAs per tile
-    int     fft_n = 0;     // real FFT size N = 2 * cluster * 2^log2_ml
-    int64_t n_tiles = 0;
-    DevBuf  tile_start;    // int64 [n_tiles] first output row (global)
-    DevBuf  tile_block;    // int32 [n_tiles]
-    DevBuf  blk_start;     // int64 [nb]
-    DevBuf  blk_len;       // int32 [nb]
-    DevBuf  blk_spec;      // int32 [nb] index of the block's spectrum
-    DevBuf  blk_t0;        // double [nb] T_block[0]
-    DevBuf  spectra;       // double [n_spec][N/2+1]
-    DevBuf  twiddle;       // double2 [N/2]: exp(-2 pi i k / N)
-    DevBuf  means;         // double [nb]
-    int     n_spec = 0;
-    std::vector<double> h_Tuniq;  // [n_spec][lambda] distinct first rows
-    // FP32 plan (mixed-precision operator), built on first use
-    struct {
-        int     ready = 0;
-        int     log2_ml = 0, cluster = 1, fft_n = 0;
-        int64_t n_tiles = 0;
-        DevBuf  tile_start, tile_block, spectra, twiddle;
-    } f32;
+    DevBuf               blk_start;      // int64 [nb]
+    DevBuf               blk_len;        // int32 [nb]
+    DevBuf               blk_spec;       // int32 [nb] index of the block's spectrum
+    DevBuf               blk_t0;         // double [nb] T_block[0]
+    DevBuf               means;          // double [nb]
+    int                  n_spec = 0;
+    std::vector<double>  h_Tuniq;        // [n_spec][lambda] distinct first rows
+    mdp_tile_plan        p64;            // built at creation
+    mdp_tile_plan        p32;            // built on first FP32 use
 };
 
 // ---------------------------------------------------------------- block Jacobi state (solver.cu)
@@ -175,6 +186,10 @@ int mdp_matvec_blockmeans(mdp_context *ctx, const mdp_pointing *A, const mdp_noi
 // FP32 operator pieces (mixed precision)
 int mdp_noise_prepare_fp32(mdp_context *ctx, mdp_noise *N);
 int mdp_stbmm_impl32(mdp_context *ctx, mdp_noise *N, const float *d_in, float *d_out, const double *d_means);
+int mdp_stbmm32_batch(mdp_context *ctx, mdp_noise *N, const float *d_in, float *d_out, int ncols,
+                      int64_t col_stride, const double *d_means, const int *d_active);
+int mdp_noise_chunks(const mdp_noise *N, int *n_chunks, const int64_t **d_chunk_start, const int32_t **d_chunk_len,
+                     const int32_t **d_blk_chunk0, const int32_t **d_blk_nchunk, int *covers_all);
 int mdp_pointing_prepare_fp32(mdp_context *ctx, mdp_pointing *A);
 int mdp_matvec32_blockmeans(mdp_context *ctx, const mdp_pointing *A, const mdp_noise *N, const double *d_x,
                             float *d_y);
@@ -187,3 +202,6 @@ inline int grid_for(int64_t n, int threads, int max_blocks = 148 * 16) {
     if (b < 1) b = 1;
     return (int) b;
 }
+
+// sample lists of the pointing's rows grouped by bins of bin_pix pixels
+int mdp_build_bins(mdp_context *ctx, mdp_pointing *A, int bin_pix, mdp_pt_bins *B);

@@ -637,11 +637,12 @@ __global__ void bin_scatter_kernel(const int32_t *__restrict__ off, int64_t m, i
     }
 }
 
-static int build_bins(mdp_context *ctx, mdp_pointing *A) {
+int mdp_build_bins(mdp_context *ctx, mdp_pointing *A, int bin_pix, mdp_pt_bins *B) {
     const int64_t npix = A->n_map() / 3;
-    const int     bin3 = 3 * PT_BIN_PIX;
-    const int64_t nb = (npix + PT_BIN_PIX - 1) / PT_BIN_PIX;
+    const int     bin3 = 3 * bin_pix;
+    const int64_t nb = (npix + bin_pix - 1) / bin_pix;
     DevBuf        count, start, cursor;
+    B->valid = 0;
     MDP_TRY(count.alloc(4 * (nb + 1)));
     MDP_TRY(start.alloc(4 * (nb + 1)));
     MDP_TRY(cursor.alloc(4 * (nb + 1)));
@@ -652,20 +653,20 @@ static int build_bins(mdp_context *ctx, mdp_pointing *A) {
     MDP_CHECK_LAUNCH(ctx);
     uint32_t total = 0;
     MDP_TRY(mdp_exclusive_scan_u32(ctx, count.as<uint32_t>(), start.as<uint32_t>(), nb + 1, &total));
-    MDP_TRY(A->bin_perm.alloc(4 * std::max<int64_t>(total, 1)));
+    MDP_TRY(B->perm.alloc(4 * std::max<int64_t>(total, 1)));
     bin_scatter_kernel<<<g, 256, 0, ctx->stream>>>(A->off.as<int32_t>(), A->m, bin3, start.as<uint32_t>(),
-                                                   cursor.as<uint32_t>(), A->bin_perm.as<uint32_t>());
+                                                   cursor.as<uint32_t>(), B->perm.as<uint32_t>());
     MDP_CHECK_LAUNCH(ctx);
     std::vector<uint32_t> hs(nb + 1);
     MDP_CUDA(cudaMemcpyAsync(hs.data(), start.p, 4 * (nb + 1), cudaMemcpyDeviceToHost, ctx->stream));
     MDP_CUDA(cudaStreamSynchronize(ctx->stream));
     std::vector<int64_t> hs64(nb + 1);
     for (int64_t i = 0; i <= nb; i++) hs64[i] = hs[i];
-    MDP_TRY(A->bin_start.alloc(8 * (nb + 1)));
-    MDP_CUDA(cudaMemcpy(A->bin_start.p, hs64.data(), 8 * (nb + 1), cudaMemcpyHostToDevice));
-    A->nbins = nb;
-    A->bin_pix = PT_BIN_PIX;
-    A->bins_valid = 1;
+    MDP_TRY(B->start.alloc(8 * (nb + 1)));
+    MDP_CUDA(cudaMemcpy(B->start.p, hs64.data(), 8 * (nb + 1), cudaMemcpyHostToDevice));
+    B->nbins = nb;
+    B->bin_pix = bin_pix;
+    B->valid = 1;
     return MDP_OK;
 }
 
@@ -774,10 +775,10 @@ int mdp_trmatvec_launch(mdp_context *ctx, const mdp_pointing *A, const double *d
     MDP_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * A->n_map(), ctx->stream));
     if (use_bins(A)) {
         mdp_pointing *Am = const_cast<mdp_pointing *>(A);  // the bin list is a cache of the pointing
-        if (!Am->bins_valid) MDP_TRY(build_bins(ctx, Am));
-        if (A->nbins > 0) {
-            trmatvec_binned_kernel<<<(unsigned) (A->nbins * PT_SPLIT), 512, 0, ctx->stream>>>(
-                    A->off.as<int32_t>(), A->values, d_y, d_x, A->bin_start.as<int64_t>(), A->bin_perm.as<uint32_t>(),
+        if (!Am->bins.valid) MDP_TRY(mdp_build_bins(ctx, Am, PT_BIN_PIX, &Am->bins));
+        if (A->bins.nbins > 0) {
+            trmatvec_binned_kernel<<<(unsigned) (A->bins.nbins * PT_SPLIT), 512, 0, ctx->stream>>>(
+                    A->off.as<int32_t>(), A->values, d_y, d_x, A->bins.start.as<int64_t>(), A->bins.perm.as<uint32_t>(),
                     A->n_map());
             MDP_CHECK_LAUNCH(ctx);
         }
@@ -808,11 +809,11 @@ int mdp_trmatvec32_launch(mdp_context *ctx, mdp_pointing *A, const float *d_y, d
     MDP_TRY(mdp_pointing_prepare_fp32(ctx, A));
     MDP_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * A->n_map(), ctx->stream));
     if (use_bins(A)) {
-        if (!A->bins_valid) MDP_TRY(build_bins(ctx, A));
-        if (A->nbins > 0) {
-            trmatvec32_binned_kernel<<<(unsigned) (A->nbins * PT_SPLIT), 512, 0, ctx->stream>>>(
-                    A->off.as<int32_t>(), A->w32.as<float>(), d_y, d_x, A->bin_start.as<int64_t>(),
-                    A->bin_perm.as<uint32_t>(), A->n_map());
+        if (!A->bins.valid) MDP_TRY(mdp_build_bins(ctx, A, PT_BIN_PIX, &A->bins));
+        if (A->bins.nbins > 0) {
+            trmatvec32_binned_kernel<<<(unsigned) (A->bins.nbins * PT_SPLIT), 512, 0, ctx->stream>>>(
+                    A->off.as<int32_t>(), A->w32.as<float>(), d_y, d_x, A->bins.start.as<int64_t>(),
+                    A->bins.perm.as<uint32_t>(), A->n_map());
             MDP_CHECK_LAUNCH(ctx);
         }
         return MDP_OK;

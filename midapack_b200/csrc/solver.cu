@@ -588,7 +588,8 @@ int mdp_bj_build(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, BJState 
     MDP_CUDA(cudaStreamSynchronize(st));
     std::swap(A->lindices.p, lind2.p);
     std::swap(A->lindices.bytes, lind2.bytes);
-    A->bins_valid = 0;  // pixels were renumbered
+    A->bins.valid = 0;  // pixels were renumbered
+    A->mbins.valid = 0;
     A->trash_pix = 1;
     A->lcount = 3 * (int64_t) kept_pix + 3;
     // the reference pairs kept blocks with kept pixels in order; both counts

@@ -28,6 +28,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <tuple>
 
 #include "mdp_internal.cuh"
 
@@ -140,15 +141,15 @@ __device__ __forceinline__ void dit_set(V (&v)[R], V w) {
 }
 
 // one local pass of R = 2^k stages starting at group size L over smem s[0..ML);
-// tw[k] = exp(-2 pi i k / N) with N = 2^logN
+// wl[q] = W_L^q = exp(-2 pi i q / L), q < L/R, staged in shared memory
 template <typename V, int R, bool INVERSE>
-__device__ __forceinline__ void local_pass(V *s, int ML, int L, int logN_over_L, const V *__restrict__ tw) {
+__device__ __forceinline__ void local_pass(V *s, int ML, int L, const V *wl) {
     const int nsets = ML / R;
     const int stride = L / R;
     for (int set = threadIdx.x; set < nsets; set += blockDim.x) {
         const int g = set / stride, q = set - g * stride;
         const int base = g * L + q;
-        const V   w = __ldg(tw + ((int64_t) q << logN_over_L));  // W_L^q
+        const V   w = wl[q];
         V         v[R];
 #pragma unroll
         for (int i = 0; i < R; i++) v[i] = s[swzv(V{}, base + i * stride)];
@@ -160,43 +161,67 @@ __device__ __forceinline__ void local_pass(V *s, int ML, int L, int logN_over_L,
     __syncthreads();
 }
 
+// Pass p of the local transform starts at group size L = 2^(LOG_ML - 4p) and
+// needs W_L^q for q < L/R.  The per-pass twiddle tables are packed one after
+// the other (they depend on L only, not on the tile size); ltw_offset(l, p) is
+// where pass p's table starts and ltw_offset(l, passes) the packed size.
+__host__ __device__ constexpr int ltw_passes(int log_ml) { return (log_ml + 3) / 4; }
+__host__ __device__ constexpr int ltw_offset(int log_ml, int p) {
+    int off = 0;
+    for (int i = 0; i < p; i++) {
+        const int logL = log_ml - 4 * i;
+        off += 1 << (logL - (logL >= 4 ? 4 : logL));
+    }
+    return off;
+}
+__host__ __device__ constexpr int ltw_size(int log_ml) { return ltw_offset(log_ml, ltw_passes(log_ml)); }
+
 // all local stages of the per-CTA transform, 4 per pass; the schedule is
-// resolved at compile time (no local-memory tables)
+// resolved at compile time (no local-memory tables); stw = packed tables in
+// shared memory
 template <typename V, int LOG_ML, bool INVERSE>
-__device__ __forceinline__ void local_fft(V *s, int logN, const V *__restrict__ tw) {
-    constexpr int NP = (LOG_ML + 3) / 4;
+__device__ __forceinline__ void local_fft(V *s, const V *stw) {
+    constexpr int NP = ltw_passes(LOG_ML);
     constexpr int ML = 1 << LOG_ML;
 #pragma unroll
     for (int pi = 0; pi < NP; pi++) {
         const int p = INVERSE ? (NP - 1 - pi) : pi;
-        const int rem = LOG_ML - 4 * p;
-        const int k = rem >= 4 ? 4 : rem;
         const int logL = LOG_ML - 4 * p;
+        const int k = logL >= 4 ? 4 : logL;
         const int L = 1 << logL;
-        const int lno = logN - logL;
-        if (k == 4) local_pass<V, 16, INVERSE>(s, ML, L, lno, tw);
-        else if (k == 3) local_pass<V, 8, INVERSE>(s, ML, L, lno, tw);
-        else if (k == 2) local_pass<V, 4, INVERSE>(s, ML, L, lno, tw);
-        else local_pass<V, 2, INVERSE>(s, ML, L, lno, tw);
+        const V  *wl = stw + ltw_offset(LOG_ML, p);
+        if (k == 4) local_pass<V, 16, INVERSE>(s, ML, L, wl);
+        else if (k == 3) local_pass<V, 8, INVERSE>(s, ML, L, wl);
+        else if (k == 2) local_pass<V, 4, INVERSE>(s, ML, L, wl);
+        else local_pass<V, 2, INVERSE>(s, ML, L, wl);
     }
 }
 
 // ------------------------------------------------------------------ the tile kernel
+// The twist tables are in the order the product pass visits the spectrum:
+// entry e = rank * ML/2 + i is the pair (k, M-k) of position P = rank*ML + 2i,
+// k = bitrev(P); entry C*ML/2 is k = M/2.  Reading them is one coalesced
+// stream instead of three scattered gathers per pair.
 template <typename T>
 struct TileArgsT {
-    const T                  *vin;
-    T                        *vout;
-    const int64_t            *tile_start;  // first output row of the tile (global)
-    const int32_t            *tile_block;
-    const int64_t            *blk_start;
-    const int32_t            *blk_len;
-    const int32_t            *blk_spec;
-    const T                  *spectra;     // [n_spec][M+1]
-    const typename CT<T>::V  *tw;          // [M]
-    const double             *means;       // [nb] or nullptr
-    int                       lambda;
+    using V = typename CT<T>::V;
+    const T       *vin;
+    T             *vout;
+    const int64_t *tile_start;  // first output row of the tile (global)
+    const int32_t *tile_block;
+    const int64_t *blk_start;
+    const int32_t *blk_len;
+    const int32_t *blk_spec;
+    const V       *hpair;       // [n_spec][M/2+1]: ((H[k]+H[M-k])/2, (H[k]-H[M-k])/2)
+    const V       *ttw;         // [M/2+1]: W_N^k
+    const V       *ltw;         // packed local-pass twiddles W_L^q
+    const V       *twm;         // [ML]: W_M^q for the cross-CTA stages
+    const double  *means;       // [nb] or nullptr; [ncols][nb] for a column batch
+    int            lambda;
+    int            nb;          // blocks (stride of the per-column means)
+    int64_t        col_stride;  // rows between the columns of a batch (blockIdx.y = column)
+    const int     *active;      // [ncols] nonzero for the columns to apply, or nullptr (all)
 };
-typedef TileArgsT<double> TileArgs;
 
 template <typename T, int LOG_ML, int C>
 __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgsT<T> a) {
@@ -208,10 +233,17 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgsT<T> a) {
     constexpr int N = 2 * M;        // real samples per tile
     int           logM = LOG_ML;
     for (int c = C; c > 1; c >>= 1) logM++;
-    const int logN = logM + 1;
 
     const int     rank = (C > 1) ? (int) (blockIdx.x % C) : 0;
     const int64_t tile = (C > 1) ? (int64_t) (blockIdx.x / C) : (int64_t) blockIdx.x;
+    // column of a batch: every CTA of a cluster has the same blockIdx.y, so a
+    // skipped column leaves whole clusters before their first barrier
+    if (a.active && !a.active[blockIdx.y]) return;
+    if (blockIdx.y) {
+        a.vin += (int64_t) blockIdx.y * a.col_stride;
+        a.vout += (int64_t) blockIdx.y * a.col_stride;
+        if (a.means) a.means += (int64_t) blockIdx.y * a.nb;
+    }
     const int     blk = a.tile_block[tile];
     const int64_t bs = a.blk_start[blk];
     const int64_t be = bs + a.blk_len[blk];
@@ -220,6 +252,11 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgsT<T> a) {
     const int64_t ws = t0 - halo;               // window start (row of x[0])
     const int     E = N - 2 * halo;            // outputs per tile
     const T       mu = a.means ? (T) a.means[blk] : (T) 0;
+
+    // ---- stage the local-pass twiddles behind the tile
+    constexpr int NLTW = ltw_size(LOG_ML);
+    V            *stw = smem + ML;
+    for (int i = threadIdx.x; i < NLTW; i += blockDim.x) stw[i] = __ldg(a.ltw + i);
 
     // ---- load this CTA's 2*ML real samples of the window (zero outside the block)
     T            *sd = reinterpret_cast<T *>(smem);
@@ -249,7 +286,7 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgsT<T> a) {
             const int sq = swzv(V{}, q);
 #pragma unroll
             for (int c = 0; c < C; c++) v[c] = cluster.map_shared_rank(smem, c)[sq];
-            dif_set<V, C>(v, __ldg(a.tw + 2 * q));  // W_M^q = W_N^(2q)
+            dif_set<V, C>(v, __ldg(a.twm + q));
 #pragma unroll
             for (int c = 0; c < C; c++) cluster.map_shared_rank(smem, c)[sq] = v[c];
         }
@@ -258,30 +295,30 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgsT<T> a) {
         __syncthreads();
     }
 
-    local_fft<V, LOG_ML, false>(smem, logN, a.tw);
+    local_fft<V, LOG_ML, false>(smem, stw);
 
     if constexpr (C > 1) cg::this_cluster().sync();
 
     // ---- real-FFT untangle, spectrum product, re-tangle (bit-reversed storage)
-    const T *H = a.spectra + (int64_t) a.blk_spec[blk] * (M + 1);
     // Position P holds Z[rev(P)]; pairs (k, M-k) with k <= M/2 are handled by the
     // owner of rev(k).  k <= M/2 exactly for even local positions plus the single
     // position of k = M/2 (local index 1 of rank 0), so each thread walks even
-    // positions in batches of 4 with the spectrum and twiddle loads issued first.
+    // positions in batches of 4 with the table loads issued first.
     constexpr int NPAIR = ML / 2;
     const T       half = (T) 0.5;
+    const V      *HP = a.hpair + (int64_t) a.blk_spec[blk] * (C * NPAIR + 1);
     for (int i0 = threadIdx.x; i0 < NPAIR + 1; i0 += 4 * blockDim.x) {
         int  p1[4], p2[4];
-        T    hk[4], hm[4];
-        V    wk[4];
+        V    hc[4], wk[4];
         bool act[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             const int i = i0 + u * blockDim.x;
-            int       p = 2 * i;
+            int       p = 2 * i, e = rank * NPAIR + i;
             act[u] = i < NPAIR;
             if (i == NPAIR) {  // the k = M/2 pair: local position 1 of rank 0
                 p = 1;
+                e = C * NPAIR;
                 act[u] = (rank == 0);
             }
             const int P1 = rank * ML + p;
@@ -289,9 +326,8 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgsT<T> a) {
             const int k2 = (M - k) & (M - 1);
             p1[u] = p;
             p2[u] = (int) (__brev((unsigned) k2) >> (32 - logM));
-            hk[u] = act[u] ? __ldg(H + k) : (T) 0;
-            hm[u] = act[u] ? __ldg(H + (M - k)) : (T) 0;
-            wk[u] = act[u] ? __ldg(a.tw + k) : mkv(wk[u], (T) 1, (T) 0);
+            hc[u] = act[u] ? __ldg(HP + e) : mkv(hc[u], (T) 0, (T) 0);
+            wk[u] = act[u] ? __ldg(a.ttw + e) : mkv(wk[u], (T) 1, (T) 0);
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) {
@@ -304,7 +340,7 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgsT<T> a) {
             const V Z1 = *s1, Z2 = *s2;
             const V E0 = mkv(Z1, half * (Z1.x + Z2.x), half * (Z1.y - Z2.y));
             const V O0 = mkv(Z1, half * (Z1.y + Z2.y), -half * (Z1.x - Z2.x));
-            const T ca = half * (hk[u] + hm[u]), cb = half * (hk[u] - hm[u]);
+            const T ca = hc[u].x, cb = hc[u].y;
             const V wO = cmul(wk[u], O0);
             const V Ep = mkv(Z1, ca * E0.x + cb * wO.x, ca * E0.y + cb * wO.y);
             const V cE = cmulc(E0, wk[u]);  // conj(w) * E
@@ -317,7 +353,7 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgsT<T> a) {
     if constexpr (C > 1) cg::this_cluster().sync();
     else __syncthreads();
 
-    local_fft<V, LOG_ML, true>(smem, logN, a.tw);
+    local_fft<V, LOG_ML, true>(smem, stw);
 
     if constexpr (C > 1) {
         cg::cluster_group cluster = cg::this_cluster();
@@ -327,7 +363,7 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgsT<T> a) {
             const int sq = swzv(V{}, q);
 #pragma unroll
             for (int c = 0; c < C; c++) v[c] = cluster.map_shared_rank(smem, c)[sq];
-            dit_set<V, C>(v, __ldg(a.tw + 2 * q));  // W_M^q = W_N^(2q)
+            dit_set<V, C>(v, __ldg(a.twm + q));
 #pragma unroll
             for (int c = 0; c < C; c++) cluster.map_shared_rank(smem, c)[sq] = v[c];
         }
@@ -362,6 +398,73 @@ __global__ void spectrum_kernel(const double *__restrict__ T, int lambda, int N,
         }
         H[k] = T[0] + 2.0 * acc;
     }
+}
+
+// Twist table of one spectrum in tile position order (see TileArgsT); the
+// halves are formed in the tile's precision T from H rounded to T.
+template <typename T>
+__global__ void twist_pairs_kernel(const double *__restrict__ H, int M, int logM, int ML, int C,
+                                   typename CT<T>::V *__restrict__ out) {
+    const int npair = ML / 2, n = C * npair + 1;
+    const T   half = (T) 0.5;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        int k = M / 2;
+        if (e < C * npair) {
+            const int r = e / npair, i = e - r * npair;
+            k = (int) (__brev((unsigned) (r * ML + 2 * i)) >> (32 - logM));
+        }
+        const T hk = (T) H[k], hm = (T) H[M - k];
+        out[e] = mkv(out[e], half * (hk + hm), half * (hk - hm));
+    }
+}
+
+// exp(-2 pi i num / den) in long double, rounded to V
+static inline void host_cexp(long double num, long double den, double2 *o) {
+    const long double ang = -2.0L * 3.14159265358979323846264338327950288L * num / den;
+    *o = make_double2((double) cosl(ang), (double) sinl(ang));
+}
+static inline void host_cexp(long double num, long double den, float2 *o) {
+    const long double ang = -2.0L * 3.14159265358979323846264338327950288L * num / den;
+    *o = make_float2((float) cosl(ang), (float) sinl(ang));
+}
+
+// Twiddle tables of a tile plan (ML = 2^log_ml points per CTA, C CTAs, M = C*ML,
+// N = 2M): packed local-pass tables, W_M^q for q < ML, and the twist twiddles
+// W_N^k in tile position order.
+template <typename V>
+static int build_tile_twiddles(int log_ml, int C, DevBuf &ltw, DevBuf &twm, DevBuf &ttw) {
+    const int ML = 1 << log_ml, M = C * ML, N = 2 * M, npair = ML / 2;
+    int       logM = log_ml;
+    for (int c = C; c > 1; c >>= 1) logM++;
+    std::vector<V> l(ltw_size(log_ml)), m(ML), t(C * npair + 1);
+    for (int p = 0; p < ltw_passes(log_ml); p++) {
+        const int logL = log_ml - 4 * p, k = logL >= 4 ? 4 : logL, off = ltw_offset(log_ml, p);
+        for (int q = 0; q < (1 << (logL - k)); q++) host_cexp(q, (long double) (1 << logL), &l[off + q]);
+    }
+    for (int q = 0; q < ML; q++) host_cexp(q, M, &m[q]);
+    for (int e = 0; e < C * npair + 1; e++) {
+        int k = M / 2;
+        if (e < C * npair) {
+            const unsigned P = (unsigned) ((e / npair) * ML + 2 * (e % npair));
+            unsigned       r = 0;
+            for (int b = 0; b < logM; b++) r |= ((P >> b) & 1u) << (logM - 1 - b);
+            k = (int) r;
+        }
+        host_cexp(k, N, &t[e]);
+    }
+    MDP_TRY(ltw.alloc(sizeof(V) * l.size()));
+    MDP_TRY(twm.alloc(sizeof(V) * m.size()));
+    MDP_TRY(ttw.alloc(sizeof(V) * t.size()));
+    MDP_CUDA(cudaMemcpy(ltw.p, l.data(), sizeof(V) * l.size(), cudaMemcpyHostToDevice));
+    MDP_CUDA(cudaMemcpy(twm.p, m.data(), sizeof(V) * m.size(), cudaMemcpyHostToDevice));
+    MDP_CUDA(cudaMemcpy(ttw.p, t.data(), sizeof(V) * t.size(), cudaMemcpyHostToDevice));
+    return MDP_OK;
+}
+
+// dynamic shared memory of a tile kernel: the tile plus the staged twiddles
+template <typename V>
+static size_t tile_smem(int log_ml) {
+    return sizeof(V) * ((size_t) (1 << log_ml) + (size_t) ltw_size(log_ml));
 }
 
 // ------------------------------------------------------------------ block means and white noise
@@ -410,55 +513,339 @@ struct NoiseExtra {
 };
 static std::map<const mdp_noise *, NoiseExtra *> g_extra;
 
-static int choose_fft(int lambda, int64_t max_block, int *log_ml, int *cluster) {
-    const char *env = getenv("MDP_TOEPLITZ_FFT");  // force the real tile size N (power of two)
-    int         forced = env ? atoi(env) : 0;
-    double      best = 1e300;
-    int         bl = -1, bc = 1;
-    for (int C = 1; C <= 8; C <<= 1)
-        for (int lml = 6; lml <= 13; lml++) {
-            if (C > 1 && lml != 13) continue;
+// Tile kernels that exist, per precision: one CTA of 2^6 .. 2^LMAX complex
+// points, or clusters of 2, 4 or 8 CTAs of 2^(LMAX-1) or 2^LMAX points each
+// (LMAX = 13 for FP64 and 14 for FP32: 128 KiB of tile per CTA).
+template <typename T> struct TileLimits;
+template <> struct TileLimits<double> { static constexpr int LMAX = 13; };
+template <> struct TileLimits<float> { static constexpr int LMAX = 14; };
+
+template <typename T>
+using tile_fn_t = void (*)(TileArgsT<T>);
+
+template <typename T, int L>
+static tile_fn_t<T> pick_cluster(int C) {
+    switch (C) {
+        case 1: return toeplitz_tile_kernel<T, L, 1>;
+        case 2: return toeplitz_tile_kernel<T, L, 2>;
+        case 4: return toeplitz_tile_kernel<T, L, 4>;
+        case 8: return toeplitz_tile_kernel<T, L, 8>;
+    }
+    return nullptr;
+}
+
+template <typename T>
+static tile_fn_t<T> pick_kernel(int log_ml, int C) {
+    constexpr int LMAX = TileLimits<T>::LMAX;
+    if (log_ml == LMAX) return pick_cluster<T, LMAX>(C);
+    if (log_ml == LMAX - 1) return pick_cluster<T, LMAX - 1>(C);
+    if (C != 1) return nullptr;
+    switch (log_ml) {
+        case 6: return toeplitz_tile_kernel<T, 6, 1>;
+        case 7: return toeplitz_tile_kernel<T, 7, 1>;
+        case 8: return toeplitz_tile_kernel<T, 8, 1>;
+        case 9: return toeplitz_tile_kernel<T, 9, 1>;
+        case 10: return toeplitz_tile_kernel<T, 10, 1>;
+        case 11: return toeplitz_tile_kernel<T, 11, 1>;
+        case 12: return toeplitz_tile_kernel<T, 12, 1>;
+    }
+    return nullptr;
+}
+
+struct TileCand {
+    int log_ml, C, threads;
+};
+
+static int default_threads(int log_ml) { return std::min(512, std::max(64, (1 << log_ml) / 16)); }
+
+// every launchable configuration whose tile holds the band (E >= 1)
+template <typename T>
+static std::vector<TileCand> tile_candidates(int lambda) {
+    constexpr int         LMAX = TileLimits<T>::LMAX;
+    std::vector<TileCand> out;
+    for (int lml = 6; lml <= LMAX; lml++)
+        for (int C = 1; C <= 8; C <<= 1) {
+            if (C > 1 && lml < LMAX - 1) continue;
             const int64_t N = 2LL * C * (1LL << lml);
-            const int64_t E = N - 2LL * (lambda - 1);
-            if (E < 1) continue;
-            if (forced && N != forced) continue;
-            int logN = lml + 1;
-            for (int c = C; c > 1; c >>= 1) logN++;
-            // FFT work per useful output, a penalty for cluster traffic, and a
-            // penalty when a tile is much larger than the blocks it covers
-            double eff = (double) std::min<int64_t>(E, max_block);
-            double cost = (double) N / eff * (logN + 3) + (C > 1 ? 3.0 * std::log2((double) C) : 0.0);
-            if (E < N / 4 && !forced) cost *= 1.5;
-            if (cost < best) {
-                best = cost;
-                bl = lml;
-                bc = C;
-            }
+            if (N - 2LL * (lambda - 1) < 1) continue;
+            out.push_back({lml, C, default_threads(lml)});
+            if (default_threads(lml) == 512) out.push_back({lml, C, 256});  // 2 CTAs per SM when registers allow
         }
-    if (bl < 0) return MDP_EUNSUPPORTED;
-    *log_ml = bl;
-    *cluster = bc;
+    return out;
+}
+
+// cost model: FFT work per useful output, a penalty for cluster traffic, and
+// a penalty when a tile is much larger than the blocks it covers
+static double tile_model_cost(const TileCand &c, int lambda, int64_t max_block) {
+    const int64_t N = 2LL * c.C * (1LL << c.log_ml);
+    const int64_t E = N - 2LL * (lambda - 1);
+    int           logN = c.log_ml + 1;
+    for (int k = c.C; k > 1; k >>= 1) logN++;
+    const double eff = (double) std::min<int64_t>(E, std::max<int64_t>(max_block, 1));
+    double       cost = (double) N / eff * (logN + 3) + (c.C > 1 ? 3.0 * std::log2((double) c.C) : 0.0);
+    if (E < N / 4) cost *= 1.5;
+    if (c.threads != default_threads(c.log_ml)) cost *= 1.01;  // ties go to the default launch shape
+    return cost;
+}
+
+template <typename T>
+static int build_plan(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, const TileCand &c, bool spectra);
+template <typename T>
+static int launch_tiles(mdp_context *ctx, const mdp_noise *N, const mdp_tile_plan &P, const T *d_in, T *d_out,
+                        const double *d_means, int ncols = 1, int64_t col_stride = 0, const int *d_active = nullptr);
+
+// Autotuner.  The plans of a precision are keyed by the band (ceil log2 of
+// lambda) and the block length (ceil log2); the first noise operator with a
+// new key times every candidate kept by the screen below on a sample of its
+// own blocks (at most 2^24 rows, zero data: the tile kernels do the same work
+// whatever the values) and the fastest per useful row is kept for the process.
+struct TuneKey {
+    int prec, lam_bits, blk_bits, device;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(prec, lam_bits, blk_bits, device) < std::tie(o.prec, o.lam_bits, o.blk_bits, o.device);
+    }
+};
+static std::mutex                   g_tune_mu;
+static std::map<TuneKey, TileCand> g_tuned;
+
+static int ceil_log2(int64_t v) {
+    int b = 0;
+    while ((1LL << b) < v) b++;
+    return b;
+}
+
+template <typename T>
+static int tune_plan(mdp_context *ctx, const mdp_noise *N, const std::vector<TileCand> &cands, TileCand *best) {
+    // sample: whole blocks from the start, at most 2^24 rows (one long block is cut there)
+    const int64_t    cap = 1LL << 24;
+    std::vector<int64_t> idv;
+    std::vector<int32_t> len;
+    int64_t              rows = 0;
+    for (int b = 0; b < N->nb && rows < cap; b++) {
+        if (N->h_n[b] <= 0) continue;
+        const int64_t n = std::min<int64_t>(N->h_n[b], cap - rows);
+        if (n < N->h_n[b] && !idv.empty()) break;
+        idv.push_back(rows);
+        len.push_back((int32_t) n);
+        rows += n;
+    }
+    if (idv.empty()) return MDP_EUNSUPPORTED;
+    mdp_noise S;
+    S.nb = (int) idv.size();
+    S.lambda = N->lambda;
+    S.nrow_end = rows;
+    S.h_idv = idv;
+    S.h_n = len;
+    S.n_spec = 1;
+    std::vector<int32_t> spec(S.nb, 0);
+    MDP_TRY(S.blk_start.alloc(8 * S.nb));
+    MDP_TRY(S.blk_len.alloc(4 * S.nb));
+    MDP_TRY(S.blk_spec.alloc(4 * S.nb));
+    MDP_TRY(S.means.alloc(8 * S.nb));
+    MDP_CUDA(cudaMemcpy(S.blk_start.p, idv.data(), 8 * S.nb, cudaMemcpyHostToDevice));
+    MDP_CUDA(cudaMemcpy(S.blk_len.p, len.data(), 4 * S.nb, cudaMemcpyHostToDevice));
+    MDP_CUDA(cudaMemcpy(S.blk_spec.p, spec.data(), 4 * S.nb, cudaMemcpyHostToDevice));
+    MDP_CUDA(cudaMemset(S.means.p, 0, 8 * S.nb));
+    DevBuf in, out;
+    MDP_TRY(in.alloc(sizeof(T) * rows));
+    MDP_TRY(out.alloc(sizeof(T) * rows));
+    MDP_CUDA(cudaMemset(in.p, 0, sizeof(T) * rows));
+    cudaEvent_t e0, e1;
+    MDP_CUDA(cudaEventCreate(&e0));
+    MDP_CUDA(cudaEventCreate(&e1));
+    double bestt = 1e300;
+    int    rc = MDP_OK;
+    for (const TileCand &c : cands) {
+        mdp_tile_plan P;
+        if ((rc = build_plan<T>(ctx, &S, P, c, false))) break;
+        float ms = 0.f;
+        if ((rc = launch_tiles<T>(ctx, &S, P, in.as<T>(), out.as<T>(), S.means.as<double>()))) break;  // warm-up
+        cudaEventRecord(e0, ctx->stream);
+        for (int r = 0; r < 3; r++)
+            if ((rc = launch_tiles<T>(ctx, &S, P, in.as<T>(), out.as<T>(), S.means.as<double>()))) break;
+        if (rc) break;
+        cudaEventRecord(e1, ctx->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            rc = MDP_ECUDA;
+            mdp_set_error("tile autotuner: %s", cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        if (ms < bestt) {
+            bestt = ms;
+            *best = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
+// MDP_TOEPLITZ_PLAN[32]="log2_ml,cluster,threads" forces a plan;
+// MDP_TOEPLITZ_FFT[32]=N restricts the choice to tiles of N real samples (cost
+// model only); MDP_TOEPLITZ_TUNE=0 switches the autotuner off.
+template <typename T>
+static int choose_plan(mdp_context *ctx, const mdp_noise *N, TileCand *out, int *tuned) {
+    const bool  f32 = sizeof(T) == 4;
+    const char *plan = getenv(f32 ? "MDP_TOEPLITZ_PLAN32" : "MDP_TOEPLITZ_PLAN");
+    const char *fft = getenv(f32 ? "MDP_TOEPLITZ_FFT32" : "MDP_TOEPLITZ_FFT");
+    const char *tune = getenv("MDP_TOEPLITZ_TUNE");
+    *tuned = 0;
+    std::vector<TileCand> cands = tile_candidates<T>(N->lambda);
+    if (plan) {
+        TileCand c{0, 0, 0};
+        if (sscanf(plan, "%d,%d,%d", &c.log_ml, &c.C, &c.threads) != 3 || !pick_kernel<T>(c.log_ml, c.C) ||
+            c.threads < 32 || c.threads > 512 || (c.threads & 31) ||
+            2LL * c.C * (1LL << c.log_ml) - 2LL * (N->lambda - 1) < 1) {
+            mdp_set_error("invalid tile plan '%s' for lambda=%d", plan, N->lambda);
+            return MDP_EINVAL;
+        }
+        *out = c;
+        return MDP_OK;
+    }
+    const int forced = fft ? atoi(fft) : 0;
+    if (forced) {
+        std::vector<TileCand> keep;
+        for (const TileCand &c : cands)
+            if (2LL * c.C * (1LL << c.log_ml) == forced) keep.push_back(c);
+        cands.swap(keep);
+    }
+    if (cands.empty()) return MDP_EUNSUPPORTED;
+    std::sort(cands.begin(), cands.end(), [&](const TileCand &a, const TileCand &b) {
+        return tile_model_cost(a, N->lambda, N->max_block) < tile_model_cost(b, N->lambda, N->max_block);
+    });
+    *out = cands[0];
+    if (forced || (tune && atoi(tune) == 0) || cands.size() == 1) return MDP_OK;
+    // screen: tiles at least a quarter useful and not longer than twice the block plus the halo
+    std::vector<TileCand> screen;
+    for (const TileCand &c : cands) {
+        const int64_t Nn = 2LL * c.C * (1LL << c.log_ml), E = Nn - 2LL * (N->lambda - 1);
+        if (E * 4 >= Nn && E <= 2 * std::max<int64_t>(N->max_block, 1) + 2LL * N->lambda) screen.push_back(c);
+    }
+    if (screen.size() <= 1) return MDP_OK;
+    const TuneKey key{f32 ? 32 : 64, ceil_log2(N->lambda), ceil_log2(std::max<int64_t>(N->max_block, 1)),
+                      ctx->device};
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto                        it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+        const TileCand &c = it->second;
+        if (2LL * c.C * (1LL << c.log_ml) - 2LL * (N->lambda - 1) >= 1) {
+            *out = c;
+            *tuned = 1;
+            return MDP_OK;
+        }
+    }
+    TileCand best = screen[0];
+    MDP_TRY(tune_plan<T>(ctx, N, screen, &best));
+    g_tuned[key] = best;
+    *out = best;
+    *tuned = 1;
     return MDP_OK;
 }
 
-typedef void (*tile_fn)(TileArgs);
-static tile_fn pick_kernel(int log_ml, int C) {
-    if (C == 1) switch (log_ml) {
-            case 6: return toeplitz_tile_kernel<double, 6, 1>;
-            case 7: return toeplitz_tile_kernel<double, 7, 1>;
-            case 8: return toeplitz_tile_kernel<double, 8, 1>;
-            case 9: return toeplitz_tile_kernel<double, 9, 1>;
-            case 10: return toeplitz_tile_kernel<double, 10, 1>;
-            case 11: return toeplitz_tile_kernel<double, 11, 1>;
-            case 12: return toeplitz_tile_kernel<double, 12, 1>;
-            case 13: return toeplitz_tile_kernel<double, 13, 1>;
+// Builds a tile plan: the tile table over the operator's blocks, the twiddle
+// tables and (spectra = true) the spectrum pairs of every distinct block row.
+template <typename T>
+static int build_plan(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, const TileCand &c, bool spectra) {
+    using V = typename CT<T>::V;
+    P.log2_ml = c.log_ml;
+    P.cluster = c.C;
+    P.threads = c.threads;
+    const int M = c.C << c.log_ml;
+    P.fft_n = 2 * M;
+    const int64_t        E = (int64_t) P.fft_n - 2LL * (N->lambda - 1);
+    std::vector<int64_t> ts;
+    std::vector<int32_t> tb;
+    for (int b = 0; b < N->nb; b++)
+        for (int64_t o = 0; o < N->h_n[b]; o += E) {
+            ts.push_back(N->h_idv[b] + o);
+            tb.push_back(b);
         }
-    if (log_ml == 13) switch (C) {
-            case 2: return toeplitz_tile_kernel<double, 13, 2>;
-            case 4: return toeplitz_tile_kernel<double, 13, 4>;
-            case 8: return toeplitz_tile_kernel<double, 13, 8>;
+    P.n_tiles = (int64_t) ts.size();
+    if (P.n_tiles * P.cluster > 0x7fffffffLL) {
+        mdp_set_error("noise operator: %lld tiles exceed one launch", (long long) P.n_tiles);
+        return MDP_EUNSUPPORTED;
+    }
+    MDP_TRY(P.tile_start.alloc(8 * std::max<size_t>(ts.size(), 1)));
+    MDP_TRY(P.tile_block.alloc(4 * std::max<size_t>(tb.size(), 1)));
+    if (!ts.empty()) {
+        MDP_CUDA(cudaMemcpy(P.tile_start.p, ts.data(), 8 * ts.size(), cudaMemcpyHostToDevice));
+        MDP_CUDA(cudaMemcpy(P.tile_block.p, tb.data(), 4 * tb.size(), cudaMemcpyHostToDevice));
+    }
+    MDP_TRY(build_tile_twiddles<V>(c.log_ml, c.C, P.ltw, P.twm, P.ttw));
+    const int64_t npair = (int64_t) M / 2 + 1;
+    MDP_TRY(P.spectra.alloc(sizeof(V) * (size_t) N->n_spec * npair));
+    if (spectra) {
+        // H[k], k <= M, in FP64 from the twiddles exp(-2 pi i k / N) (long double on the host)
+        std::vector<double2> tw(M);
+        for (int k = 0; k < M; k++) host_cexp(k, P.fft_n, &tw[k]);
+        DevBuf tw64, dH, dT;
+        MDP_TRY(tw64.alloc(sizeof(double2) * M));
+        MDP_TRY(dH.alloc(sizeof(double) * (M + 1)));
+        MDP_TRY(dT.alloc(sizeof(double) * N->lambda));
+        MDP_CUDA(cudaMemcpy(tw64.p, tw.data(), sizeof(double2) * M, cudaMemcpyHostToDevice));
+        int logM = c.log_ml;
+        for (int k = c.C; k > 1; k >>= 1) logM++;
+        for (int u = 0; u < N->n_spec; u++) {
+            MDP_CUDA(cudaMemcpy(dT.p, N->h_Tuniq.data() + (size_t) u * N->lambda, sizeof(double) * N->lambda,
+                                cudaMemcpyHostToDevice));
+            spectrum_kernel<<<grid_for(M + 1, 128, 4096), 128, 0, ctx->stream>>>(
+                    dT.as<double>(), N->lambda, P.fft_n, tw64.as<double2>(), dH.as<double>());
+            MDP_CHECK_LAUNCH(ctx);
+            twist_pairs_kernel<T><<<grid_for(npair, 256, 1024), 256, 0, ctx->stream>>>(
+                    dH.as<double>(), M, logM, 1 << c.log_ml, c.C, P.spectra.as<V>() + (size_t) u * npair);
+            MDP_CHECK_LAUNCH(ctx);
+            MDP_CUDA(cudaStreamSynchronize(ctx->stream));
         }
-    return nullptr;
+    } else {
+        MDP_CUDA(cudaMemset(P.spectra.p, 0, sizeof(V) * (size_t) N->n_spec * npair));
+    }
+    tile_fn_t<T> fn = pick_kernel<T>(c.log_ml, c.C);
+    if (!fn) return MDP_EUNSUPPORTED;
+    MDP_CUDA(cudaFuncSetAttribute((const void *) fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int) tile_smem<V>(c.log_ml)));
+    if (c.C > 1) MDP_CUDA(cudaFuncSetAttribute((const void *) fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    P.ready = 1;
+    return MDP_OK;
+}
+
+template <typename T>
+static int launch_tiles(mdp_context *ctx, const mdp_noise *N, const mdp_tile_plan &P, const T *d_in, T *d_out,
+                        const double *d_means, int ncols, int64_t col_stride, const int *d_active) {
+    using V = typename CT<T>::V;
+    if (P.n_tiles == 0 || ncols < 1) return MDP_OK;
+    if (ncols > 65535) return MDP_EUNSUPPORTED;
+    TileArgsT<T> a;
+    a.vin = d_in;
+    a.vout = d_out;
+    a.tile_start = P.tile_start.as<int64_t>();
+    a.tile_block = P.tile_block.as<int32_t>();
+    a.blk_start = N->blk_start.as<int64_t>();
+    a.blk_len = N->blk_len.as<int32_t>();
+    a.blk_spec = N->blk_spec.as<int32_t>();
+    a.hpair = P.spectra.as<V>();
+    a.ttw = P.ttw.as<V>();
+    a.ltw = P.ltw.as<V>();
+    a.twm = P.twm.as<V>();
+    a.means = d_means;
+    a.lambda = N->lambda;
+    a.nb = N->nb;
+    a.col_stride = col_stride;
+    a.active = d_active;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned) (P.n_tiles * P.cluster), (unsigned) ncols);
+    cfg.blockDim = dim3(P.threads);
+    cfg.dynamicSmemBytes = tile_smem<V>(P.log2_ml);
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = P.cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    MDP_CUDA(cudaLaunchKernelEx(&cfg, pick_kernel<T>(P.log2_ml, P.cluster), a));
+    MDP_CHECK_LAUNCH(ctx);
+    return MDP_OK;
 }
 
 extern "C" int mdp_noise_create(mdp_context *ctx, int nb_blocks, const int64_t *h_idv, const int32_t *h_n, int lambda,
@@ -487,10 +874,11 @@ extern "C" int mdp_noise_create(mdp_context *ctx, int nb_blocks, const int64_t *
         }
         max_block = std::max<int64_t>(max_block, h_n[b]);
     }
-    mdp_noise *N = new mdp_noise();
+    mdp_noise  *N = new mdp_noise();
     NoiseExtra *X = new NoiseExtra();
     N->nb = nb_blocks;
     N->lambda = lambda;
+    N->max_block = max_block;
     N->h_idv.assign(h_idv, h_idv + nb_blocks);
     N->h_n.assign(h_n, h_n + nb_blocks);
     N->h_T0.resize(nb_blocks);
@@ -507,7 +895,6 @@ extern "C" int mdp_noise_create(mdp_context *ctx, int nb_blocks, const int64_t *
         return rc;
     };
     int rc;
-    std::vector<int32_t> h_len(N->h_n);
     if ((rc = N->blk_start.alloc(8 * nb_blocks)) || (rc = N->blk_len.alloc(4 * nb_blocks)) ||
         (rc = N->blk_t0.alloc(8 * nb_blocks)) || (rc = N->means.alloc(8 * nb_blocks)) ||
         (rc = N->blk_spec.alloc(4 * nb_blocks)))
@@ -541,36 +928,6 @@ extern "C" int mdp_noise_create(mdp_context *ctx, int nb_blocks, const int64_t *
     cudaMemcpy(X->blk_nchunk.p, cn.data(), 4 * nb_blocks, cudaMemcpyHostToDevice);
 
     if (lambda > 1) {
-        if ((rc = choose_fft(lambda, max_block, &N->log2_ml, &N->cluster))) {
-            mdp_set_error("mdp_noise_create: no FFT tile fits lambda=%d", lambda);
-            return fail(rc);
-        }
-        const int M = N->cluster << N->log2_ml;
-        N->fft_n = 2 * M;
-        const int64_t E = (int64_t) N->fft_n - 2LL * (lambda - 1);
-        std::vector<int64_t> ts;
-        std::vector<int32_t> tb;
-        for (int b = 0; b < nb_blocks; b++)
-            for (int64_t o = 0; o < h_n[b]; o += E) {
-                ts.push_back(h_idv[b] + o);
-                tb.push_back(b);
-            }
-        N->n_tiles = (int64_t) ts.size();
-        if ((rc = N->tile_start.alloc(8 * std::max<size_t>(ts.size(), 1))) ||
-            (rc = N->tile_block.alloc(4 * std::max<size_t>(tb.size(), 1))))
-            return fail(rc);
-        if (!ts.empty()) {
-            cudaMemcpy(N->tile_start.p, ts.data(), 8 * ts.size(), cudaMemcpyHostToDevice);
-            cudaMemcpy(N->tile_block.p, tb.data(), 4 * tb.size(), cudaMemcpyHostToDevice);
-        }
-        // twiddles exp(-2 pi i k / N), k < N/2, in long double then rounded
-        std::vector<double2> tw(M);
-        for (int k = 0; k < M; k++) {
-            long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double) k / (long double) N->fft_n;
-            tw[k] = make_double2((double) cosl(ang), (double) sinl(ang));
-        }
-        if ((rc = N->twiddle.alloc(sizeof(double2) * M))) return fail(rc);
-        cudaMemcpy(N->twiddle.p, tw.data(), sizeof(double2) * M, cudaMemcpyHostToDevice);
         // distinct block rows share one spectrum
         std::vector<int32_t> spec_of(nb_blocks);
         std::vector<int>     uniq;
@@ -592,21 +949,12 @@ extern "C" int mdp_noise_create(mdp_context *ctx, int nb_blocks, const int64_t *
         for (int u = 0; u < N->n_spec; u++)
             memcpy(N->h_Tuniq.data() + (size_t) u * lambda, h_T + (size_t) uniq[u] * lambda, sizeof(double) * lambda);
         cudaMemcpy(N->blk_spec.p, spec_of.data(), 4 * nb_blocks, cudaMemcpyHostToDevice);
-        if ((rc = N->spectra.alloc(sizeof(double) * (size_t) N->n_spec * (M + 1)))) return fail(rc);
-        DevBuf dT;
-        if ((rc = dT.alloc(sizeof(double) * lambda))) return fail(rc);
-        for (int u = 0; u < N->n_spec; u++) {
-            cudaMemcpy(dT.p, h_T + (size_t) uniq[u] * lambda, sizeof(double) * lambda, cudaMemcpyHostToDevice);
-            spectrum_kernel<<<grid_for(M + 1, 128, 4096), 128, 0, ctx->stream>>>(
-                    dT.as<double>(), lambda, N->fft_n, N->twiddle.as<double2>(),
-                    N->spectra.as<double>() + (size_t) u * (M + 1));
-            ctx->launches++;
-            cudaStreamSynchronize(ctx->stream);
+        TileCand c;
+        if ((rc = choose_plan<double>(ctx, N, &c, &N->p64.tuned))) {
+            if (rc == MDP_EUNSUPPORTED) mdp_set_error("mdp_noise_create: no FFT tile fits lambda=%d", lambda);
+            return fail(rc);
         }
-        tile_fn fn = pick_kernel(N->log2_ml, N->cluster);
-        size_t  smem = sizeof(double2) << N->log2_ml;
-        cudaFuncSetAttribute((const void *) fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-        if (N->cluster > 1) cudaFuncSetAttribute((const void *) fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if ((rc = build_plan<double>(ctx, N, N->p64, c, true))) return fail(rc);
     }
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
@@ -630,9 +978,9 @@ extern "C" void mdp_noise_destroy(mdp_noise *N) {
 
 extern "C" int mdp_noise_tile(const mdp_noise *N, int *fft_size, int *cluster_ctas, int64_t *n_tiles) {
     if (!N) return MDP_EINVAL;
-    if (fft_size) *fft_size = N->fft_n;
-    if (cluster_ctas) *cluster_ctas = N->cluster;
-    if (n_tiles) *n_tiles = N->n_tiles;
+    if (fft_size) *fft_size = N->p64.fft_n;
+    if (cluster_ctas) *cluster_ctas = N->p64.cluster;
+    if (n_tiles) *n_tiles = N->p64.n_tiles;
     return MDP_OK;
 }
 
@@ -668,38 +1016,7 @@ int mdp_stbmm_impl(mdp_context *ctx, const mdp_noise *N, const double *d_in, dou
         MDP_TRY(mdp_block_means(ctx, N, d_in, N->means.as<double>()));
         d_means = N->means.as<double>();
     }
-    if (N->n_tiles == 0) return MDP_OK;
-    TileArgs a;
-    a.vin = d_in;
-    a.vout = d_out;
-    a.tile_start = N->tile_start.as<int64_t>();
-    a.tile_block = N->tile_block.as<int32_t>();
-    a.blk_start = N->blk_start.as<int64_t>();
-    a.blk_len = N->blk_len.as<int32_t>();
-    a.blk_spec = N->blk_spec.as<int32_t>();
-    a.spectra = N->spectra.as<double>();
-    a.tw = N->twiddle.as<double2>();
-    a.means = d_means;
-    a.lambda = N->lambda;
-    tile_fn  fn = pick_kernel(N->log2_ml, N->cluster);
-    size_t   smem = sizeof(double2) << N->log2_ml;
-    int      threads = std::min(512, std::max(64, (1 << N->log2_ml) / 16));
-    if (N->n_tiles * N->cluster > 0x7fffffffLL) return MDP_EUNSUPPORTED;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned) (N->n_tiles * N->cluster));
-    cfg.blockDim = dim3(threads);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = ctx->stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = N->cluster;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    MDP_CUDA(cudaLaunchKernelEx(&cfg, fn, a));
-    MDP_CHECK_LAUNCH(ctx);
-    return MDP_OK;
+    return launch_tiles<double>(ctx, N, N->p64, d_in, d_out, d_means);
 }
 
 // y = P x fused with the block-mean partial sums of y: one CTA per 65536-row
@@ -752,123 +1069,15 @@ int mdp_matvec_blockmeans(mdp_context *ctx, const mdp_pointing *A, const mdp_noi
 }
 
 // ------------------------------------------------------------------ FP32 operator
-typedef void (*tile_fn32)(TileArgsT<float>);
-static tile_fn32 pick_kernel32(int log_ml, int C) {
-    if (C == 1) switch (log_ml) {
-            case 6: return toeplitz_tile_kernel<float, 6, 1>;
-            case 7: return toeplitz_tile_kernel<float, 7, 1>;
-            case 8: return toeplitz_tile_kernel<float, 8, 1>;
-            case 9: return toeplitz_tile_kernel<float, 9, 1>;
-            case 10: return toeplitz_tile_kernel<float, 10, 1>;
-            case 11: return toeplitz_tile_kernel<float, 11, 1>;
-            case 12: return toeplitz_tile_kernel<float, 12, 1>;
-            case 13: return toeplitz_tile_kernel<float, 13, 1>;
-            case 14: return toeplitz_tile_kernel<float, 14, 1>;
-        }
-    if (log_ml == 14) switch (C) {
-            case 2: return toeplitz_tile_kernel<float, 14, 2>;
-            case 4: return toeplitz_tile_kernel<float, 14, 4>;
-            case 8: return toeplitz_tile_kernel<float, 14, 8>;
-        }
-    return nullptr;
-}
-
-// FP32 tiles hold 2^14 complex points per CTA (128 KiB); same cost model as FP64
-static int choose_fft32(int lambda, int64_t max_block, int *log_ml, int *cluster) {
-    const char *env = getenv("MDP_TOEPLITZ_FFT32");
-    int         forced = env ? atoi(env) : 0;
-    double      best = 1e300;
-    int         bl = -1, bc = 1;
-    for (int C = 1; C <= 8; C <<= 1)
-        for (int lml = 6; lml <= 14; lml++) {
-            if (C > 1 && lml != 14) continue;
-            const int64_t N = 2LL * C * (1LL << lml);
-            const int64_t E = N - 2LL * (lambda - 1);
-            if (E < 1) continue;
-            if (forced && N != forced) continue;
-            int logN = lml + 1;
-            for (int c = C; c > 1; c >>= 1) logN++;
-            double eff = (double) std::min<int64_t>(E, max_block);
-            double cost = (double) N / eff * (logN + 3) + (C > 1 ? 3.0 * std::log2((double) C) : 0.0);
-            if (E < N / 4 && !forced) cost *= 1.5;
-            if (cost < best) {
-                best = cost;
-                bl = lml;
-                bc = C;
-            }
-        }
-    if (bl < 0) return MDP_EUNSUPPORTED;
-    *log_ml = bl;
-    *cluster = bc;
-    return MDP_OK;
-}
-
-__global__ void to_float_kernel(const double *__restrict__ in, float *__restrict__ out, int64_t n) {
-    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
-        out[i] = (float) in[i];
-}
-
 int mdp_noise_prepare_fp32(mdp_context *ctx, mdp_noise *N) {
-    if (N->f32.ready) return MDP_OK;
+    if (N->p32.ready) return MDP_OK;
     if (N->lambda == 1) {
-        N->f32.ready = 1;
+        N->p32.ready = 1;
         return MDP_OK;
     }
-    int64_t max_block = 0;
-    for (int b = 0; b < N->nb; b++) max_block = std::max<int64_t>(max_block, N->h_n[b]);
-    MDP_TRY(choose_fft32(N->lambda, max_block, &N->f32.log2_ml, &N->f32.cluster));
-    const int     M = N->f32.cluster << N->f32.log2_ml;
-    const int     Nn = 2 * M;
-    const int64_t E = (int64_t) Nn - 2LL * (N->lambda - 1);
-    N->f32.fft_n = Nn;
-    std::vector<int64_t> ts;
-    std::vector<int32_t> tb;
-    for (int b = 0; b < N->nb; b++)
-        for (int64_t o = 0; o < N->h_n[b]; o += E) {
-            ts.push_back(N->h_idv[b] + o);
-            tb.push_back(b);
-        }
-    N->f32.n_tiles = (int64_t) ts.size();
-    MDP_TRY(N->f32.tile_start.alloc(8 * std::max<size_t>(ts.size(), 1)));
-    MDP_TRY(N->f32.tile_block.alloc(4 * std::max<size_t>(tb.size(), 1)));
-    if (!ts.empty()) {
-        MDP_CUDA(cudaMemcpy(N->f32.tile_start.p, ts.data(), 8 * ts.size(), cudaMemcpyHostToDevice));
-        MDP_CUDA(cudaMemcpy(N->f32.tile_block.p, tb.data(), 4 * tb.size(), cudaMemcpyHostToDevice));
-    }
-    // twiddles: long double on the host, FP64 copy for the spectra, FP32 copy for the tiles
-    std::vector<double2> tw(M);
-    std::vector<float2>  twf(M);
-    for (int k = 0; k < M; k++) {
-        long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double) k / (long double) Nn;
-        tw[k] = make_double2((double) cosl(ang), (double) sinl(ang));
-        twf[k] = make_float2((float) cosl(ang), (float) sinl(ang));
-    }
-    DevBuf tw64, spec64, dT;
-    MDP_TRY(tw64.alloc(sizeof(double2) * M));
-    MDP_TRY(N->f32.twiddle.alloc(sizeof(float2) * M));
-    MDP_CUDA(cudaMemcpy(tw64.p, tw.data(), sizeof(double2) * M, cudaMemcpyHostToDevice));
-    MDP_CUDA(cudaMemcpy(N->f32.twiddle.p, twf.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
-    MDP_TRY(spec64.alloc(sizeof(double) * (size_t) N->n_spec * (M + 1)));
-    MDP_TRY(N->f32.spectra.alloc(sizeof(float) * (size_t) N->n_spec * (M + 1)));
-    MDP_TRY(dT.alloc(sizeof(double) * N->lambda));
-    for (int u = 0; u < N->n_spec; u++) {
-        MDP_CUDA(cudaMemcpy(dT.p, N->h_Tuniq.data() + (size_t) u * N->lambda, sizeof(double) * N->lambda,
-                            cudaMemcpyHostToDevice));
-        spectrum_kernel<<<grid_for(M + 1, 128, 4096), 128, 0, ctx->stream>>>(
-                dT.as<double>(), N->lambda, Nn, tw64.as<double2>(), spec64.as<double>() + (size_t) u * (M + 1));
-        MDP_CHECK_LAUNCH(ctx);
-    }
-    const int64_t ns = (int64_t) N->n_spec * (M + 1);
-    to_float_kernel<<<grid_for(ns, 256, 1024), 256, 0, ctx->stream>>>(spec64.as<double>(), N->f32.spectra.as<float>(), ns);
-    MDP_CHECK_LAUNCH(ctx);
-    MDP_CUDA(cudaStreamSynchronize(ctx->stream));
-    tile_fn32 fn = pick_kernel32(N->f32.log2_ml, N->f32.cluster);
-    const int smem = (int) (sizeof(float2) << N->f32.log2_ml);
-    MDP_CUDA(cudaFuncSetAttribute((const void *) fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    if (N->f32.cluster > 1)
-        MDP_CUDA(cudaFuncSetAttribute((const void *) fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    N->f32.ready = 1;
-    return MDP_OK;
+    TileCand c;
+    MDP_TRY(choose_plan<float>(ctx, N, &c, &N->p32.tuned));
+    return build_plan<float>(ctx, N, N->p32, c, true);
 }
 
 __global__ void white32_kernel(const float *__restrict__ vin, float *__restrict__ vout,
@@ -907,35 +1116,30 @@ int mdp_stbmm_impl32(mdp_context *ctx, mdp_noise *N, const float *d_in, float *d
         }
         d_means = N->means.as<double>();
     }
-    if (N->f32.n_tiles == 0) return MDP_OK;
-    TileArgsT<float> a;
-    a.vin = d_in;
-    a.vout = d_out;
-    a.tile_start = N->f32.tile_start.as<int64_t>();
-    a.tile_block = N->f32.tile_block.as<int32_t>();
-    a.blk_start = N->blk_start.as<int64_t>();
-    a.blk_len = N->blk_len.as<int32_t>();
-    a.blk_spec = N->blk_spec.as<int32_t>();
-    a.spectra = N->f32.spectra.as<float>();
-    a.tw = N->f32.twiddle.as<float2>();
-    a.means = d_means;
-    a.lambda = N->lambda;
-    tile_fn32 fn = pick_kernel32(N->f32.log2_ml, N->f32.cluster);
-    if (N->f32.n_tiles * N->f32.cluster > 0x7fffffffLL) return MDP_EUNSUPPORTED;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned) (N->f32.n_tiles * N->f32.cluster));
-    cfg.blockDim = dim3(std::min(512, std::max(64, (1 << N->f32.log2_ml) / 16)));
-    cfg.dynamicSmemBytes = sizeof(float2) << N->f32.log2_ml;
-    cfg.stream = ctx->stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = N->f32.cluster;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    MDP_CUDA(cudaLaunchKernelEx(&cfg, fn, a));
-    MDP_CHECK_LAUNCH(ctx);
+    return launch_tiles<float>(ctx, N, N->p32, d_in, d_out, d_means);
+}
+
+// FP32 N^-1 over a batch of columns (column c at in + c*col_stride, its
+// block means at d_means + c*nb, all given); columns with d_active[c] == 0
+// are left untouched.  The blocks must cover rows [0, nrow_end) and lambda > 1.
+int mdp_stbmm32_batch(mdp_context *ctx, mdp_noise *N, const float *d_in, float *d_out, int ncols,
+                      int64_t col_stride, const double *d_means, const int *d_active) {
+    NoiseExtra *X = g_extra.at(N);
+    if (!X->covers_all || N->lambda == 1 || !d_means) return MDP_EUNSUPPORTED;
+    MDP_TRY(mdp_noise_prepare_fp32(ctx, N));
+    return launch_tiles<float>(ctx, N, N->p32, d_in, d_out, d_means, ncols, col_stride, d_active);
+}
+
+// chunks of the block-mean reduction (65536 rows each, in block order)
+int mdp_noise_chunks(const mdp_noise *N, int *n_chunks, const int64_t **d_chunk_start, const int32_t **d_chunk_len,
+                     const int32_t **d_blk_chunk0, const int32_t **d_blk_nchunk, int *covers_all) {
+    NoiseExtra *X = g_extra.at(N);
+    *n_chunks = X->n_chunks;
+    *d_chunk_start = X->chunk_start.as<int64_t>();
+    *d_chunk_len = X->chunk_len.as<int32_t>();
+    *d_blk_chunk0 = X->blk_chunk0.as<int32_t>();
+    *d_blk_nchunk = X->blk_nchunk.as<int32_t>();
+    *covers_all = X->covers_all ? 1 : 0;
     return MDP_OK;
 }
 
@@ -991,9 +1195,22 @@ extern "C" int mdp_noise_tile_fp32(mdp_context *ctx, mdp_noise *N, int *fft_size
     if (!ctx || !N) return MDP_EINVAL;
     MDP_CUDA(cudaSetDevice(ctx->device));
     MDP_TRY(mdp_noise_prepare_fp32(ctx, N));
-    if (fft_size) *fft_size = N->f32.fft_n;
-    if (cluster_ctas) *cluster_ctas = N->f32.cluster;
-    if (n_tiles) *n_tiles = N->f32.n_tiles;
+    if (fft_size) *fft_size = N->p32.fft_n;
+    if (cluster_ctas) *cluster_ctas = N->p32.cluster;
+    if (n_tiles) *n_tiles = N->p32.n_tiles;
+    return MDP_OK;
+}
+
+extern "C" int mdp_noise_plan(mdp_context *ctx, mdp_noise *N, int fp32, int *log2_cta_points, int *cluster_ctas,
+                              int *threads, int *tuned) {
+    if (!ctx || !N) return MDP_EINVAL;
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    if (fp32) MDP_TRY(mdp_noise_prepare_fp32(ctx, N));
+    const mdp_tile_plan &P = fp32 ? N->p32 : N->p64;
+    if (log2_cta_points) *log2_cta_points = P.log2_ml;
+    if (cluster_ctas) *cluster_ctas = P.cluster;
+    if (threads) *threads = P.threads;
+    if (tuned) *tuned = P.tuned;
     return MDP_OK;
 }
 

@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
 
 
 def main(argv=None):
@@ -21,6 +22,9 @@ def main(argv=None):
     ap.add_argument("--gaps", type=float, default=0.01)
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--ops", default="P,Ninv,Pt")
+    ap.add_argument("--plans", default="",
+                    help="';'-separated tile plans 'log2_cta_points,cluster,threads' to time N^-1 with "
+                         "(FP64 for Ninv, FP32 for Ninv32); empty: the plan the library picks")
     a = ap.parse_args(argv)
     import torch
 
@@ -31,21 +35,16 @@ def main(argv=None):
     ns = wl.n_samples
     ctx = mb.Context(0)
     P = mb.Pointing(ctx, wl.pix, wl.weights, ns, 3)
-    N = mb.Noise(ctx, wl.block_sizes, wl.lam, wl.invtt)
     n = P.shape()["n_map"]
     x = torch.randn(n, dtype=torch.float64, device="cuda")
     y = torch.empty(ns, dtype=torch.float64, device="cuda")
     z = torch.empty(ns, dtype=torch.float64, device="cuda")
     xo = torch.empty(n, dtype=torch.float64, device="cuda")
     P.matvec(x, y)
-    tile = N.tile()
-    ops = {"P": (lambda: P.matvec(x, y), ns * 36 + n * 8),
-           "Ninv": (lambda: N.apply(y, z), ns * 24 + tile["n_tiles"] * (tile["fft_n"] // 2 + 1) * 8),
-           "Pt": (lambda: P.trmatvec(z, xo), ns * 36 + n * 8)}
-    out = {"samples": ns, "unknowns": n, "tile": tile}
+    y32, z32 = y.float(), torch.empty(ns, dtype=torch.float32, device="cuda")
     s = torch.cuda.current_stream()
-    for name in a.ops.split(","):
-        fn, nbytes = ops[name]
+
+    def timed(fn):
         for _ in range(2):
             fn()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -55,8 +54,33 @@ def main(argv=None):
             fn()
         e1.record(s)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / a.reps
-        out[name] = {"ms": round(ms, 4), "algorithmic_GBps": round(nbytes / ms / 1e6, 1)}
+        return e0.elapsed_time(e1) / a.reps
+
+    out = {"samples": ns, "unknowns": n}
+    plans = [p for p in a.plans.split(";") if p] or [None]
+    for name in a.ops.split(","):
+        if name in ("P", "Pt"):
+            fn = (lambda: P.matvec(x, y)) if name == "P" else (lambda: P.trmatvec(z, xo))
+            ms = timed(fn)
+            out[name] = {"ms": round(ms, 4), "algorithmic_GBps": round((ns * 36 + n * 8) / ms / 1e6, 1)}
+            continue
+        fp32 = name == "Ninv32"
+        var = "MDP_TOEPLITZ_PLAN32" if fp32 else "MDP_TOEPLITZ_PLAN"
+        res = []
+        for plan in plans:
+            if plan:
+                os.environ[var] = plan
+            try:
+                N = mb.Noise(ctx, wl.block_sizes, wl.lam, wl.invtt)
+                tile = N.tile_fp32() if fp32 else N.tile()
+            finally:
+                os.environ.pop(var, None)
+            sz = 4 if fp32 else 8
+            nbytes = ns * 3 * sz + tile["n_tiles"] * (tile["fft_n"] // 4 + 1) * 2 * sz
+            ms = timed((lambda: N.apply_fp32(y32, z32)) if fp32 else (lambda: N.apply(y, z)))
+            res.append({"plan": plan, "tile": tile, "ms": round(ms, 4), "algorithmic_GBps": round(nbytes / ms / 1e6, 1)})
+            N.close()
+        out[name] = res if len(res) > 1 else res[0]
     print(json.dumps(out), flush=True)
 
 

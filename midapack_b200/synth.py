@@ -153,6 +153,31 @@ def make_workload(name: str, width: int, height: int, n_det: int, n_samp: int, b
     return wl
 
 
+def mc_noise(n_det: int, n_samp: int, nrhs: int, fknee: float = 1.0, seed: int = 0) -> np.ndarray:
+    """Monte-Carlo noise realisations with the workload's PSD: [nrhs, n_det*n_samp]
+    float32 (the columns of a multi-RHS solve; FP32 values are exact inputs)."""
+    rng = np.random.default_rng(seed)
+    out = np.empty((nrhs, n_det * n_samp), dtype=np.float32)
+    for r in range(nrhs):
+        out[r] = np.concatenate([noise_tod(n_samp, fknee, rng) for _ in range(n_det)]).astype(np.float32)
+    return out
+
+
+def mc_noise_torch(n_det: int, n_samp: int, nrhs: int, fknee: float = 1.0, seed: int = 0, device: str = "cuda"):
+    """Device version of mc_noise for large workloads: [nrhs, n_det*n_samp] float32."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    out = torch.empty((nrhs, n_det * n_samp), dtype=torch.float32, device=device)
+    f = torch.fft.rfftfreq(n_samp, 1.0 / FS, dtype=torch.float32, device=device)
+    amp = torch.sqrt(1.0 + fknee / (f + F_MIN))
+    for r in range(nrhs):
+        white = torch.randn((n_det, n_samp), dtype=torch.float32, device=device, generator=g)
+        out[r] = torch.fft.irfft(torch.fft.rfft(white, dim=1) * amp, n=n_samp, dim=1).reshape(-1)
+    return out
+
+
 # Configurations of the reference workload family, by sizes.
 CONFIGS = {
     # plain FP64 PCG, CPU-runnable: 256x192 grid, 4 det x 2^20, lambda 2^12, one block per det

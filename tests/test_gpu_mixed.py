@@ -73,8 +73,17 @@ def test_mixed_solve_matches_fp64(gpu_ctx, case):
     (x64, l64, h64, i64), (x32, l32, h32, i32) = outs
     assert np.array_equal(l64, l32) and np.array_equal(h64, h32)
     assert i32.outer_iterations >= 1 and i32.fp64_applications == i32.outer_iterations + 1
-    for k in range(3):
-        assert _rel(x32[k::3], x64[k::3]) < 1e-8, (k, _rel(x32[k::3], x64[k::3]))
     o = R.pcg(wl.pix, wl.weights, wl.signal, wl.noise, wl.block_sizes, wl.lam, wl.invtt, tol=1e-12, maxiter=900)
+    # With flagged samples the cut rewrites the samples of the pixel after the
+    # rank-one one (precond.c:521 against mappraiser.c:130-142), so the rank-one
+    # pixel stays in the system: its Q/U directions are an exact null space of
+    # P^T N^-1 P, where every solver keeps whatever its rounding put there.  The
+    # maps are compared on the determined pixels.
+    W, _ = R.local_W(o.bj.A, wl.block_sizes, wl.lam, wl.invtt)
+    ev = np.linalg.eigvalsh(W)
+    det = np.repeat(ev[:, 0] > 1e-6 * ev[:, 2], 3)
+    assert case != "cut_gaps" or not det.all()
     for k in range(3):
-        assert _rel(x32[k::3], o.x[k::3]) < 1e-8
+        sel = det[k::3]
+        assert _rel(x32[k::3][sel], x64[k::3][sel]) < 1e-8, (k, _rel(x32[k::3][sel], x64[k::3][sel]))
+        assert _rel(x32[k::3][sel], o.x[k::3][sel]) < 1e-8
