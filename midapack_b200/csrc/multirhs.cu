@@ -88,11 +88,13 @@ __device__ __forceinline__ double mr_sum(const MRed *R, int k) {
 }
 
 // ---------------------------------------------------------------- operator kernels
-// Y[j] = P h_j (FP32 weights, h_j FP64 rounded to FP32) for the running slots,
-// with FP64 partial sums per 65536-row chunk (block means of N^-1)
+// Y[j] = P h_j (FP32 weights, FP32 copy of h_j) for the running slots, with
+// FP64 partial sums per 65536-row chunk (block means of N^-1).  The FP32 copy
+// of the slot directions (12 bytes per pixel and slot) keeps the gathered map
+// L2-resident for 8 slots of a few million pixels.
 template <int G>
 __global__ void __launch_bounds__(512) mr_matvec32_kernel(const int32_t *__restrict__ off, const float *__restrict__ w,
-                                                          const double *__restrict__ H, const int *__restrict__ run,
+                                                          const float *__restrict__ H, const int *__restrict__ run,
                                                           float *__restrict__ Y, int64_t m,
                                                           const int64_t *__restrict__ chunk_start,
                                                           const int32_t *__restrict__ chunk_len, int n_chunks,
@@ -114,14 +116,35 @@ __global__ void __launch_bounds__(512) mr_matvec32_kernel(const int32_t *__restr
             w1 = w[3 * t + 1];
             w2 = w[3 * t + 2];
         }
-        const double *h = H + (int64_t) (o >= 0 ? o : 0) * G;  // pixel p = o/3 starts at 3pG = oG
+        const float *h = H + (int64_t) (o >= 0 ? o : 0) * G;  // pixel p = o/3 starts at 3pG = oG
+        float        hv[3 * G];
+        if (o >= 0) {
+            if constexpr (G % 4 == 0) {  // 12G bytes at a 48-byte multiple: float4 loads
+#pragma unroll
+                for (int q = 0; q < 3 * G / 4; q++) {
+                    const float4 f = __ldg(reinterpret_cast<const float4 *>(h) + q);
+                    hv[4 * q] = f.x;
+                    hv[4 * q + 1] = f.y;
+                    hv[4 * q + 2] = f.z;
+                    hv[4 * q + 3] = f.w;
+                }
+            } else if constexpr (G % 2 == 0) {
+#pragma unroll
+                for (int q = 0; q < 3 * G / 2; q++) {
+                    const float2 f = __ldg(reinterpret_cast<const float2 *>(h) + q);
+                    hv[2 * q] = f.x;
+                    hv[2 * q + 1] = f.y;
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 3 * G; q++) hv[q] = __ldg(h + q);
+            }
+        }
 #pragma unroll
         for (int j = 0; j < G; j++) {
             if (!act[j]) continue;
             float v = 0.0f;
-            if (o >= 0)
-                v = w0 * (float) __ldg(h + 3 * j) + w1 * (float) __ldg(h + 3 * j + 1) +
-                    w2 * (float) __ldg(h + 3 * j + 2);
+            if (o >= 0) v = w0 * hv[3 * j] + w1 * hv[3 * j + 1] + w2 * hv[3 * j + 2];
             Y[(int64_t) j * m + t] = v;
             acc[j] += (double) v;
         }
@@ -154,7 +177,16 @@ __global__ void mr_means_kernel(const double *__restrict__ partial, int n_chunks
 
 // Q (interleaved, zeroed) += P^T Z_j for the running slots: bins of
 // MR_BIN_PIX/G pixels, FP64 products and shared-memory sums, one global atomic
-// per map entry of the bin
+// per map entry of the bin.  The shared tile is slot-major, row r = 3j+k holds
+// the bin's pixels, with the pixel index XORed by r mod 32: the atomics of a
+// warp (consecutive samples, mostly distinct pixels of one row) and the flush
+// (consecutive map entries, i.e. consecutive rows at one pixel) both spread
+// over the banks.
+template <int G>
+__device__ __forceinline__ int mr_acc_index(int r, int pl) {
+    return r * (MR_BIN_PIX / G) + (pl ^ (r & 31));
+}
+
 template <int G>
 __global__ void __launch_bounds__(512) mr_trmatvec32_kernel(const int32_t *__restrict__ off,
                                                             const float *__restrict__ w,
@@ -163,6 +195,7 @@ __global__ void __launch_bounds__(512) mr_trmatvec32_kernel(const int32_t *__res
                                                             const int64_t *__restrict__ bin_start,
                                                             const uint32_t *__restrict__ perm, int64_t npix) {
     constexpr int BP = MR_BIN_PIX / G;
+    static_assert(BP % 32 == 0, "bins must hold a multiple of 32 pixels");
     __shared__ double acc[3 * MR_BIN_PIX];
     bool              act[G];
 #pragma unroll
@@ -179,41 +212,49 @@ __global__ void __launch_bounds__(512) mr_trmatvec32_kernel(const int32_t *__res
         const int64_t t = perm[i];
         const int     pl = off[t] / 3 - (int) p0;
         const double  w0 = (double) w[3 * t], w1 = (double) w[3 * t + 1], w2 = (double) w[3 * t + 2];
-        double       *s = acc + pl * 3 * G;
 #pragma unroll
         for (int j = 0; j < G; j++) {
             if (!act[j]) continue;
             const double v = (double) Z[(int64_t) j * m + t];
-            atomicAdd(s + 3 * j, w0 * v);
-            atomicAdd(s + 3 * j + 1, w1 * v);
-            atomicAdd(s + 3 * j + 2, w2 * v);
+            atomicAdd(acc + mr_acc_index<G>(3 * j, pl), w0 * v);
+            atomicAdd(acc + mr_acc_index<G>(3 * j + 1, pl), w1 * v);
+            atomicAdd(acc + mr_acc_index<G>(3 * j + 2, pl), w2 * v);
         }
     }
     __syncthreads();
     const int64_t base = p0 * 3 * G;
     const int64_t lim = min((int64_t) 3 * MR_BIN_PIX, npix * 3 * G - base);
     for (int i = threadIdx.x; i < lim; i += blockDim.x) {
-        const double v = acc[i];
+        const int    pl = i / (3 * G), r = i - pl * 3 * G;  // map entry (p0 + pl, j, k), r = 3j + k
+        const double v = acc[mr_acc_index<G>(r, pl)];
         if (v != 0.0) atomicAdd(Q + base + i, v);
     }
 }
 
 // ---------------------------------------------------------------- PCG kernels (interleaved)
-// h = gamma_j h + Cg_j for the slots that continue
+// h = gamma_j h + Cg_j for the slots that continue; H32 = FP32 copy of h for
+// every running slot
 template <int G>
-__global__ void mr_direction_kernel(double *__restrict__ H, const double *__restrict__ CG, int64_t npix,
-                                    const int *__restrict__ run, const SlotScal *__restrict__ S) {
+__global__ void mr_direction_kernel(double *__restrict__ H, float *__restrict__ H32, const double *__restrict__ CG,
+                                    int64_t npix, const int *__restrict__ run, const SlotScal *__restrict__ S) {
     double gam[G];
-    bool   act[G];
+    bool   act[G], on[G];
 #pragma unroll
     for (int j = 0; j < G; j++) {
-        act[j] = run[j] && S[j].cont;
+        on[j] = run[j] != 0;
+        act[j] = on[j] && S[j].cont;
         gam[j] = S[j].gamma;
     }
     const int64_t n = npix * 3 * G;
     for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
         const int j = (int) ((i / 3) % G);
-        if (act[j]) H[i] = H[i] * gam[j] + CG[i];
+        if (!on[j]) continue;
+        double h = H[i];
+        if (act[j]) {
+            h = h * gam[j] + CG[i];
+            H[i] = h;
+        }
+        H32[i] = (float) h;
     }
 }
 
@@ -386,6 +427,7 @@ struct Batch {
     int     G = 0;
     int64_t m = 0, npix = 0, nmap = 0;
     DevBuf  H, Q, G1, G2, CG, DL;  // [npix][G][3]
+    DevBuf  H32;                   // FP32 copy of H
     DevBuf  Y, Z;                  // FP32 [G][m]
     DevBuf  partial, means;        // [G][n_chunks], [G][nb]
     DevBuf  run;                   // int [G]
@@ -396,7 +438,7 @@ struct Batch {
 };
 
 template <int G>
-int launch_apply32(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, Batch &B, const double *h) {
+int launch_apply32(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, Batch &B, const float *h) {
     cudaStream_t st = ctx->stream;
     const int   *run = B.run.as<int>();
     mr_matvec32_kernel<G><<<B.n_chunks, 512, 0, st>>>(A->off.as<int32_t>(), A->w32.as<float>(), h, run, B.Y.as<float>(),
@@ -429,9 +471,9 @@ int launch_iteration(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, Batch &B, 
     SlotScal    *S = B.scal.as<SlotScal>();
     MRed        *R = B.red.as<MRed>();
     const int    gv = grid_for(B.npix * 3 * G, 256, ctx->sm_count * 8);
-    mr_direction_kernel<G><<<gv, 256, 0, st>>>(B.H.as<double>(), B.CG.as<double>(), B.npix, run, S);
+    mr_direction_kernel<G><<<gv, 256, 0, st>>>(B.H.as<double>(), B.H32.as<float>(), B.CG.as<double>(), B.npix, run, S);
     MDP_CHECK_LAUNCH(ctx);
-    MDP_TRY(launch_apply32<G>(ctx, A, N, B, B.H.as<double>()));
+    MDP_TRY(launch_apply32<G>(ctx, A, N, B, B.H32.as<float>()));
     mr_coeff_kernel<G><<<MR_BLOCKS, MR_THREADS, 0, st>>>(B.H.as<double>(), B.Q.as<double>(), B.npix, run, S, R);
     MDP_CHECK_LAUNCH(ctx);
     mr_update_kernel<G><<<MR_BLOCKS, MR_THREADS, 0, st>>>(inv, B.DL.as<double>(), B.H.as<double>(), B.Q.as<double>(),
@@ -451,6 +493,8 @@ int alloc_batch(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, int G, int64_t 
     const size_t nv = sizeof(double) * (size_t) std::max<int64_t>(npix, 1) * 3 * G;
     for (DevBuf *b : {&B.H, &B.Q, &B.G1, &B.G2, &B.CG, &B.DL}) MDP_TRY(b->alloc(nv));
     for (DevBuf *b : {&B.H, &B.Q, &B.G1, &B.G2, &B.CG, &B.DL}) MDP_CUDA(cudaMemsetAsync(b->p, 0, nv, ctx->stream));
+    MDP_TRY(B.H32.alloc(nv / 2));
+    MDP_CUDA(cudaMemsetAsync(B.H32.p, 0, nv / 2, ctx->stream));
     MDP_TRY(B.Y.alloc(sizeof(float) * (size_t) A->m * G));
     MDP_TRY(B.Z.alloc(sizeof(float) * (size_t) A->m * G));
     MDP_TRY(B.partial.alloc(sizeof(double) * (size_t) std::max(B.n_chunks, 1) * G));
@@ -472,13 +516,13 @@ int time_apply(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, int64_t npix, fl
     MDP_TRY(alloc_batch(ctx, A, N, G, npix, B));
     std::vector<int> ones(G, 1);
     MDP_CUDA(cudaMemcpyAsync(B.run.p, ones.data(), sizeof(int) * G, cudaMemcpyHostToDevice, ctx->stream));
-    MDP_TRY(launch_apply32<G>(ctx, A, N, B, B.H.as<double>()));  // warm-up
+    MDP_TRY(launch_apply32<G>(ctx, A, N, B, B.H32.as<float>()));  // warm-up
     cudaEvent_t e0, e1;
     MDP_CUDA(cudaEventCreate(&e0));
     MDP_CUDA(cudaEventCreate(&e1));
     cudaEventRecord(e0, ctx->stream);
     int rc = MDP_OK;
-    for (int r = 0; r < 2 && rc == MDP_OK; r++) rc = launch_apply32<G>(ctx, A, N, B, B.H.as<double>());
+    for (int r = 0; r < 2 && rc == MDP_OK; r++) rc = launch_apply32<G>(ctx, A, N, B, B.H32.as<float>());
     cudaEventRecord(e1, ctx->stream);
     cudaEventSynchronize(e1);
     float ms = 0.f;

@@ -187,9 +187,11 @@ CONFIGS = {
     "c2_64det_2p24_2048x1536_lam16384": dict(width=2048, height=1536, n_det=64, n_samp=1 << 24,
                                              block_len=1 << 20, lam=1 << 14, fknee=1.0, seed=20261205,
                                              gap_frac=0.01),
-    # multi-RHS: 1024x768 grid, 16 det x 2^23, lambda 2^13
+    # multi-RHS: 1024x768 grid, 16 det x 2^23, lambda 2^13, 1% flagged samples as at scale (without flags
+    # P^T N^-1 P is singular: a constant offset is in its null space, and noise-only columns stall above 1e-8)
     "c4_16det_2p23_1024x768_lam8192": dict(width=1024, height=768, n_det=16, n_samp=1 << 23,
-                                           block_len=1 << 23, lam=1 << 13, fknee=1.0, seed=20261207),
+                                           block_len=1 << 23, lam=1 << 13, fknee=1.0, seed=20261207,
+                                           gap_frac=0.01),
 }
 
 
