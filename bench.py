@@ -31,8 +31,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 CONFIG = "c2_64det_2p24_2048x1536_lam16384"
-METRIC = ("time-to-map at 1e-8 residual, GLS PCG on 1 B200 (64 det x 2^24 samples, 2048x1536 px, lambda 2^14, "
-          "1% gaps); value = mixed precision, config.fp64 = plain FP64")
+MULTI_CONFIG = "c4_16det_2p23_1024x768_lam8192"
+METRIC = "time-to-map at 1e-8 residual, mixed vs FP64 on 1 B200; served p50/p99 latency"
 TOL = 1e-8
 MAXITER = 500
 
@@ -50,6 +50,16 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--inner-tol", type=float, default=1e-4)
     ap.add_argument("--no-compare", action="store_true", help="skip timing the other precision")
+    ap.add_argument("--no-multi", action="store_true", help="skip the multi-RHS part")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving part")
+    ap.add_argument("--only", default="", choices=["", "multi", "serve"],
+                    help="run only the multi-RHS or only the serving part (prints their JSON)")
+    ap.add_argument("--multi-rhs", type=int, default=128, help="right-hand sides of the multi-RHS part")
+    ap.add_argument("--multi-fp64-cols", type=int, default=2, help="columns timed with the plain FP64 path")
+    ap.add_argument("--serve-requests", type=int, default=256)
+    ap.add_argument("--serve-rate", type=float, default=50.0, help="mean Poisson arrival rate, solves/s")
+    ap.add_argument("--serve-datasets", type=int, default=16)
+    ap.add_argument("--serve-slots", type=int, default=4)
     return ap.parse_args()
 
 
@@ -151,6 +161,137 @@ def cpu_reference(wl_host, iterations: int, sample_dets: int, full_samples: int,
     return {"op_seconds_sample": t, "per_iter_full_s": per_iter_full, "time_to_map_s": per_iter_full * (iterations + 1)}
 
 
+def bench_multi(args, device):
+    """Multi-RHS configuration: 16 det x 2^23 samples, 1024x768 px, lambda 2^13,
+    1% flagged samples; args.multi_rhs columns = 1 signal+noise + Monte-Carlo
+    noise realisations (FP32 values, same PSD), solved by the multi-RHS mixed
+    solver; the plain FP64 path times args.multi_fp64_cols columns one by one."""
+    import torch
+    import midapack_b200 as mb
+    from midapack_b200 import synth
+    cfg = synth.CONFIGS[MULTI_CONFIG]
+    wl = synth.make_workload_torch(MULTI_CONFIG, **cfg)
+    m = wl.n_samples
+    noise = synth.mc_noise_torch(wl.n_det, wl.n_samp, args.multi_rhs, wl.fknee, seed=20261211)
+    ctx = mb.Context(device)
+    # warm-up: plans, tuner and bins on a separate pointing of the same data
+    P0 = mb.Pointing(ctx, wl.pix, wl.weights, m, 3)
+    N0 = mb.Noise(ctx, wl.block_sizes, wl.lam, wl.invtt)
+    mb.gls_solve_multi(ctx, P0, N0, noise[:2], signal=wl.signal, signal_col=0, tol=TOL, maxiter=3, slots=0)
+    del P0, N0
+    torch.cuda.synchronize()
+    P = mb.Pointing(ctx, wl.pix, wl.weights, m, 3)
+    N = mb.Noise(ctx, wl.block_sizes, wl.lam, wl.invtt)
+    l0 = ctx.launches
+    t0 = time.perf_counter()
+    x, lst, cond, hits, ci, info = mb.gls_solve_multi(ctx, P, N, noise, signal=wl.signal, signal_col=0, tol=TOL,
+                                                      maxiter=MAXITER, slots=0, use_graph=True)
+    torch.cuda.synchronize()
+    t_multi = time.perf_counter() - t0
+    launches = ctx.launches - l0
+    xs = x[: min(args.multi_fp64_cols, args.multi_rhs)].cpu().numpy()
+    del x
+    fp64 = []
+    errs = {"multi_mixed": {"I": 0.0, "Q": 0.0, "U": 0.0}, "fp64_path": {"I": 0.0, "Q": 0.0, "U": 0.0}}
+    for c in range(min(args.multi_fp64_cols, args.multi_rhs)):
+        P1 = mb.Pointing(ctx, wl.pix, wl.weights, m, 3)
+        N1 = mb.Noise(ctx, wl.block_sizes, wl.lam, wl.invtt)
+        sig = wl.signal if c == 0 else torch.zeros_like(wl.signal)
+        nz = noise[c].double()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        x1, l1, _, _, _, i1 = mb.gls_solve(ctx, P1, N1, sig, nz, tol=TOL, maxiter=MAXITER)
+        torch.cuda.synchronize()
+        fp64.append((time.perf_counter() - t0, i1.iterations, bool(i1.converged)))
+        x1 = x1.cpu().numpy()
+        # FP64 oracle of the column: the plain FP64 path at tol 1e-12 (untimed)
+        xo = mb.gls_solve(ctx, P1, N1, sig, nz, tol=1e-12, maxiter=4 * MAXITER)[0].cpu().numpy()
+        for tag, xv in (("multi_mixed", xs[c]), ("fp64_path", x1)):
+            for k, name in enumerate("IQU"):
+                errs[tag][name] = max(errs[tag][name],
+                                      float(np.linalg.norm(xv[k::3] - xo[k::3]) / np.linalg.norm(xo[k::3])))
+        del P1, N1, nz, sig
+    t64 = float(np.mean([f[0] for f in fp64]))
+    out = {"workload": MULTI_CONFIG, "rhs": args.multi_rhs, "columns": "1 signal+noise + "
+           f"{args.multi_rhs - 1} Monte-Carlo noise realisations (FP32 values)",
+           "time_s": round(t_multi, 3), "solves_per_s": round(args.multi_rhs / t_multi, 3),
+           "fp64_path": {"seconds_per_solve": round(t64, 4), "solves_per_s": round(1.0 / t64, 3),
+                         "columns_timed": len(fp64), "iterations": [f[1] for f in fp64],
+                         "converged": all(f[2] for f in fp64)},
+           "speedup_vs_fp64": round(t64 * args.multi_rhs / t_multi, 3),
+           "slots": info.slots, "graph": bool(info.graph), "batched_iterations": info.batched_iterations,
+           "inner_iterations_mean": round(info.total_iterations / args.multi_rhs, 1),
+           "fp64_applications": info.fp64_applications, "converged": sum(c.converged for c in ci),
+           "precond_s": round(info.precond_seconds, 3), "map_rel_err_vs_fp64_oracle": errs,
+           "oracle": "plain FP64 path at tol 1e-12 on the timed FP64 columns",
+           "fft_tile_fp32": N.tile_fp32(), "gpu_launches": int(launches)}
+    del P, N, noise, wl
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out
+
+
+def bench_serving(args, device):
+    """Serving configuration: Poisson arrivals (args.serve_rate per second) of
+    independent solves on args.serve_datasets resident datasets drawn
+    log-uniformly (detectors 1-32, samples/det 2^18-2^23, grid side 64-1024 at
+    4:3, lambda 2^8-2^14, f_knee uniform 0.1-5 Hz, 1% flagged samples); each
+    request is its dataset's signal plus a fresh noise realisation, mixed
+    precision to 1e-8; the same stream again with the plain FP64 path."""
+    import torch
+    from midapack_b200 import serve
+    specs = serve.draw_specs(args.serve_datasets, seed=20261208)
+    n = args.serve_requests
+    offsets = serve.poisson_arrivals(n, args.serve_rate, seed=20261209)
+    pick = np.random.default_rng(20261210).integers(0, len(specs), n)
+    ex = serve.GpuExecutor(device, keep_maps=lambda rid: rid < 32)
+    srv = serve.Server(ex, slots=args.serve_slots, work_budget=48 << 30, dataset_budget=96 << 30)
+    t0 = time.perf_counter()
+    for s in specs:
+        srv.preload(s)
+    # untimed warm-up: every slot solves the largest dataset once per precision,
+    # so that the slots' work buffers have their final sizes before timing
+    big = max(specs, key=lambda s: s.n_samples)
+    for prec in ("fp64", "mixed"):
+        warm = [srv.submit(serve.Request(-1 - k, big, noise_seed=k, precision=prec, tol=TOL))
+                for k in range(args.serve_slots)]
+        for tk in warm:
+            tk.wait(1800.0)
+    t_pre = time.perf_counter() - t0
+    out = {"requests": n, "rate_per_s": args.serve_rate, "datasets": len(specs), "slots": args.serve_slots,
+           "dataset_samples": [s.n_samples for s in specs], "preload_and_warmup_s": round(t_pre, 2)}
+    res = {}
+    for prec in ("fp64", "mixed"):
+        reqs = [serve.Request(i, specs[pick[i]], noise_seed=1000 + i, precision=prec, tol=TOL) for i in range(n)]
+        srv.max_running = 0
+        r = serve.run_stream(srv, reqs, offsets, timeout=1800.0)
+        st = serve.latency_stats(r)
+        st["max_concurrent"] = srv.max_running
+        st["errors"] = sum(1 for x in r if x.error)
+        out[prec] = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in st.items()}
+        res[prec] = r
+    # FP64 oracle (tol 1e-12) for the requests whose maps were kept: the error
+    # of each path's map, max over the requests, per I/Q/U
+    n_or = min(8, n)
+    oracle = [serve.Request(i, specs[pick[i]], noise_seed=1000 + i, precision="fp64", tol=1e-12, maxiter=2000)
+              for i in range(n_or)]
+    ores = [tk.wait(1800.0) for tk in [srv.submit(r) for r in oracle]]
+    srv.close()
+    for prec in ("mixed", "fp64"):
+        errs = {"I": 0.0, "Q": 0.0, "U": 0.0}
+        for a, o in zip(res[prec][:n_or], ores):
+            if a.x is None or o.x is None:
+                continue
+            for k, name in enumerate("IQU"):
+                errs[name] = max(errs[name], float(np.linalg.norm(a.x[k::3] - o.x[k::3]) / np.linalg.norm(o.x[k::3])))
+        out[prec]["map_rel_err_vs_fp64_oracle"] = errs
+    out["oracle"] = f"plain FP64 path at tol 1e-12 on the first {n_or} requests"
+    out["speedup_solves_per_s"] = round(out["mixed"]["solves_per_s"] / out["fp64"]["solves_per_s"], 3)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -158,6 +299,10 @@ def main():
     if args.impl == "reference" and rank != 0:
         return 0
     torch.cuda.set_device(local)
+    if args.only:
+        r = bench_multi(args, local) if args.only == "multi" else bench_serving(args, local)
+        print(json.dumps({args.only: r}), flush=True)
+        return 0
     if world > 1:
         import torch.distributed as dist
         from datetime import timedelta
@@ -288,6 +433,13 @@ def main():
     e2e = run_e2e(args, wl, world, pinned) if pinned else None
     pinned = None
 
+    # multi-RHS and serving configurations (one GPU: rank 0 of a single-process run)
+    multi = serve_out = None
+    if world == 1 and not args.no_multi:
+        multi = bench_multi(args, local)
+    if world == 1 and not args.no_serve:
+        serve_out = bench_serving(args, local)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(ms / 1e3 * 1.0, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
@@ -311,6 +463,10 @@ def main():
             line["e2e"] = e2e
         if cpu:
             line["cpu_baseline"] = cpu
+        if multi:
+            line["multi_rhs"] = multi
+        if serve_out:
+            line["serving"] = serve_out
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()

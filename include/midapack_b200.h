@@ -41,6 +41,11 @@ const char *mdp_last_error(void);
 /* ---- context: one device, one stream ---------------------------------- */
 int      mdp_context_create(int device, mdp_context **out);
 void     mdp_context_destroy(mdp_context *ctx);
+/* The solves keep their work buffers (TOD- and map-sized) in the context for
+ * its next solve, so that repeated solves do not cudaMalloc/cudaFree (which
+ * synchronise the device); mdp_context_trim frees them (after synchronising
+ * the context's stream). */
+int      mdp_context_trim(mdp_context *ctx);
 /* queue work on an existing cudaStream_t (e.g. the caller's; pass cudaStreamLegacy,
  * i.e. (void *) 1, for the legacy default stream); NULL = a stream of its own */
 int      mdp_context_set_stream(mdp_context *ctx, void *cuda_stream);
@@ -154,8 +159,9 @@ int mdp_gls_solve(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const d
  * FP64, then solves A delta = g approximately with block-Jacobi PCG whose
  * operator P^T N^-1 P runs with FP32 weights, FP32 TOD and FP32 Toeplitz FFTs
  * (dot products, PCG scalars, the 3x3 blocks and the map stay FP64), until the
- * inner residual drops by inner_tol or inner_maxiter iterations, and adds delta
- * to x.  info->iterations counts inner iterations; h_res_rel (optional,
+ * inner residual drops by inner_tol (or by the reduction still needed, with a
+ * factor 2 margin, when that is smaller) or inner_maxiter iterations, and adds
+ * delta to x.  info->iterations counts inner iterations; h_res_rel (optional,
  * maxiter+1 entries) receives sqrt(res/res0) after each refinement step. */
 int mdp_gls_solve_mixed(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *d_signal,
                         const double *d_noise, const mdp_solve_params *params, double inner_tol, int inner_maxiter,

@@ -60,6 +60,7 @@ _SIGS = {
     "mdp_last_error": (ct.c_char_p, []),
     "mdp_context_create": (ct.c_int, [ct.c_int, ct.POINTER(ct.c_void_p)]),
     "mdp_context_destroy": (None, [ct.c_void_p]),
+    "mdp_context_trim": (ct.c_int, [ct.c_void_p]),
     "mdp_context_set_stream": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
     "mdp_context_stream": (ct.c_void_p, [ct.c_void_p]),
     "mdp_synchronize": (ct.c_int, [ct.c_void_p]),
@@ -187,6 +188,10 @@ class Context:
         n = (ct.c_int64 * 4)()
         check(lib().mdp_profile_read(self.h, ms, n), "mdp_profile_read")
         return {k: (ms[i], n[i]) for i, k in enumerate(("P", "Ninv", "Pt", "vec"))}
+
+    def trim(self):
+        """Frees the work buffers the context keeps between solves."""
+        check(lib().mdp_context_trim(self.h), "mdp_context_trim")
 
     @property
     def launches(self) -> int:

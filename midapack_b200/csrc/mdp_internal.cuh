@@ -82,6 +82,10 @@ struct mdp_context {
     DevBuf       scalars;   // device scalars of the solver
     DevBuf       scratch;   // large temporary (stbmm in place, scans)
     DevBuf       scratch2;
+    // work buffers of the solves, kept for the context's next solve (a context
+    // runs one solve at a time): no cudaMalloc/cudaFree, which would
+    // synchronise the device, in the solves of a serving loop
+    DevBuf       ws[12];
     double      *h_pinned = nullptr;  // pinned host scalars
     // optional per-operator timing inside the solver (CUDA events on the stream)
     int          profile = 0;
@@ -90,6 +94,17 @@ struct mdp_context {
     cudaEvent_t  ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
+// ---------------------------------------------------------------- block Jacobi state (solver.cu)
+// Kept blocks after the rcond cut, in their original order; block k pairs
+// with pixel k of the re-initialised pointing.
+struct BJState {
+    DevBuf  inv;    // [npix][9] inverse blocks, row-major
+    DevBuf  W;      // [npix][9] P^T diag(N^-1) P blocks
+    DevBuf  rcond;  // [npix]
+    DevBuf  hits;   // [npix]
+    int64_t npix = 0;
+    int64_t ncut = 0;
+};
 // ---------------------------------------------------------------- pointing
 struct mdp_pt_bins {
     int     valid = 0;
@@ -115,6 +130,12 @@ struct mdp_pointing {
     mdp_pt_bins   bins;
     mdp_pt_bins   mbins;
     DevBuf        w32;                // float [m*3] weights for the FP32 operator (built on first use)
+    // block-Jacobi preconditioner of the device-API solves, kept with the
+    // pointing: built (and the rcond cut applied) by the first solve, reused
+    // by later solves with the same noise operator
+    BJState      *bj_cache = nullptr;
+    uint64_t      bj_noise_uid = 0;
+    ~mdp_pointing() { delete bj_cache; }
     int64_t n_map() const { return lcount - (int64_t) nnz * trash_pix; }
 };
 
@@ -137,6 +158,7 @@ struct mdp_tile_plan {
 };
 
 struct mdp_noise {
+    uint64_t             uid = 0;        // unique per created operator
     int                  nb = 0;
     int                  lambda = 0;
     int64_t              nrow_end = 0;   // max(idv+n)
@@ -153,20 +175,18 @@ struct mdp_noise {
     std::vector<double>  h_Tuniq;        // [n_spec][lambda] distinct first rows
     mdp_tile_plan        p64;            // built at creation
     mdp_tile_plan        p32;            // built on first FP32 use
+    // 65536-row chunks of the deterministic block-mean reduction
+    int                  n_chunks = 0;
+    bool                 covers_all = true;  // blocks tile rows [0, nrow_end) without holes
+    DevBuf               chunk_start;    // int64 [n_chunks]
+    DevBuf               chunk_len;      // int32 [n_chunks]
+    DevBuf               blk_chunk0;     // int32 [nb] first chunk of each block
+    DevBuf               blk_nchunk;     // int32 [nb]
+    DevBuf               partial;        // double [n_chunks] chunk sums
 };
 
-// ---------------------------------------------------------------- block Jacobi state (solver.cu)
-// Kept blocks after the rcond cut, in their original order; block k pairs
-// with pixel k of the re-initialised pointing.
-struct BJState {
-    DevBuf  inv;    // [npix][9] inverse blocks, row-major
-    DevBuf  W;      // [npix][9] P^T diag(N^-1) P blocks
-    DevBuf  rcond;  // [npix]
-    DevBuf  hits;   // [npix]
-    int64_t npix = 0;
-    int64_t ncut = 0;
-};
 int mdp_bj_build(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, BJState *bj);
+int mdp_bj_cached(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const BJState **bj);
 int mdp_pcg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *inv, int64_t npix,
                 const double *d_signal, const double *d_noise, const mdp_solve_params *params, double *d_x,
                 double *h_res_rel, mdp_solve_info *info);

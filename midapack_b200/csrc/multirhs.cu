@@ -724,9 +724,13 @@ int run_multi(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, const BJState &bj
                 if ((rc = load(j))) break;
             } else {
                 inner_it[j] = 0;
+                // inner target of this refinement: inner_tol, or the reduction
+                // still needed (factor 2 margin) when that is smaller
+                const double need = 0.5 * prm->tol / std::sqrt(res / ci[col].res0);
+                const double it = std::max(prm->inner_tol, std::min(need, 0.5));
                 mr_slot_init_kernel<G><<<MR_BLOCKS, MR_THREADS, 0, st>>>(inv, rv.as<double>(), j, bufs[parity],
                                                                          B.CG.as<double>(), B.H.as<double>(),
-                                                                         B.DL.as<double>(), npix, itol2,
+                                                                         B.DL.as<double>(), npix, it * it,
                                                                          B.run.as<int>(), S, R);
                 MDP_CHECK_LAUNCH(ctx);
             }
@@ -777,8 +781,9 @@ extern "C" int mdp_gls_solve_multi(mdp_context *ctx, mdp_pointing *A, const mdp_
     }
     MDP_CUDA(cudaSetDevice(ctx->device));
     auto    tp0 = std::chrono::steady_clock::now();
-    BJState bj;
-    MDP_TRY(mdp_bj_build(ctx, A, N, &bj));
+    const BJState *bjp = nullptr;
+    MDP_TRY(mdp_bj_cached(ctx, A, N, &bjp));
+    const BJState &bj = *bjp;
     cudaStream_t st = ctx->stream;
     if (d_lstid)
         MDP_CUDA(cudaMemcpyAsync(d_lstid, A->lindices.as<int32_t>() + 3 * A->trash_pix, 4 * A->n_map(),

@@ -67,6 +67,16 @@ extern "C" int mdp_context_create(int device, mdp_context **out) {
     return MDP_OK;
 }
 
+extern "C" int mdp_context_trim(mdp_context *ctx) {
+    if (!ctx) return MDP_EINVAL;
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    MDP_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (DevBuf &b : ctx->ws) b.release();
+    ctx->scratch.release();
+    ctx->scratch2.release();
+    return MDP_OK;
+}
+
 extern "C" void mdp_context_destroy(mdp_context *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);

@@ -607,7 +607,8 @@ int mdp_pcg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const dou
     const int64_t m = A->m;
     const int64_t n = 3 * npix;
     const int64_t nmap = A->n_map();  // >= n
-    DevBuf        tod_a, tod_b, gb1, gb2, hb, qb, cgb, scal;
+    DevBuf &tod_a = ctx->ws[0], &tod_b = ctx->ws[1], &gb1 = ctx->ws[2], &gb2 = ctx->ws[3], &hb = ctx->ws[4],
+           &qb = ctx->ws[5], &cgb = ctx->ws[6], &scal = ctx->ws[7];
     int           rc;
     if ((rc = tod_a.alloc(8 * m)) || (rc = tod_b.alloc(8 * m)) || (rc = gb1.alloc(8 * nmap)) ||
         (rc = gb2.alloc(8 * nmap)) || (rc = hb.alloc(8 * nmap)) || (rc = qb.alloc(8 * nmap)) ||
@@ -711,10 +712,11 @@ extern "C" int mdp_gls_solve(mdp_context *ctx, mdp_pointing *A, const mdp_noise 
         return MDP_EINVAL;
     }
     MDP_CUDA(cudaSetDevice(ctx->device));
-    auto    tp0 = std::chrono::steady_clock::now();
-    BJState bj;
-    MDP_TRY(mdp_bj_build(ctx, A, N, &bj));
-    cudaStream_t st = ctx->stream;
+    auto           tp0 = std::chrono::steady_clock::now();
+    const BJState *bjp = nullptr;
+    MDP_TRY(mdp_bj_cached(ctx, A, N, &bjp));
+    const BJState &bj = *bjp;
+    cudaStream_t   st = ctx->stream;
     if (d_lstid)
         MDP_CUDA(cudaMemcpyAsync(d_lstid, A->lindices.as<int32_t>() + 3 * A->trash_pix, 4 * A->n_map(),
                                  cudaMemcpyDeviceToDevice, st));
@@ -735,6 +737,29 @@ extern "C" int mdp_gls_solve(mdp_context *ctx, mdp_pointing *A, const mdp_noise 
     return MDP_OK;
 }
 
+// The device-API solves keep the preconditioner with the pointing: the first
+// solve builds it and applies the cut to the pointing; a later solve with the
+// same noise operator reuses it; another noise operator rebuilds it on the
+// already cut pointing.
+int mdp_bj_cached(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const BJState **out) {
+    if (A->bj_cache && A->bj_noise_uid == N->uid) {
+        *out = A->bj_cache;
+        return MDP_OK;
+    }
+    delete A->bj_cache;
+    A->bj_cache = nullptr;
+    BJState *bj = new BJState();
+    int      rc = mdp_bj_build(ctx, A, N, bj);
+    if (rc != MDP_OK) {
+        delete bj;
+        return rc;
+    }
+    A->bj_cache = bj;
+    A->bj_noise_uid = N->uid;
+    *out = bj;
+    return MDP_OK;
+}
+
 // ================================================================= mixed precision
 extern "C" int mdp_gls_solve_mixed(mdp_context *ctx, mdp_pointing *A, const mdp_noise *Nc, const double *d_signal,
                                    const double *d_noise, const mdp_solve_params *params, double inner_tol,
@@ -750,10 +775,11 @@ extern "C" int mdp_gls_solve_mixed(mdp_context *ctx, mdp_pointing *A, const mdp_
         return MDP_EINVAL;
     }
     MDP_CUDA(cudaSetDevice(ctx->device));
-    auto    tp0 = std::chrono::steady_clock::now();
-    BJState bj;
-    MDP_TRY(mdp_bj_build(ctx, A, N, &bj));
-    cudaStream_t st = ctx->stream;
+    auto           tp0 = std::chrono::steady_clock::now();
+    const BJState *bjp = nullptr;
+    MDP_TRY(mdp_bj_cached(ctx, A, N, &bjp));
+    const BJState &bj = *bjp;
+    cudaStream_t   st = ctx->stream;
     if (d_lstid)
         MDP_CUDA(cudaMemcpyAsync(d_lstid, A->lindices.as<int32_t>() + 3 * A->trash_pix, 4 * A->n_map(),
                                  cudaMemcpyDeviceToDevice, st));
@@ -766,7 +792,9 @@ extern "C" int mdp_gls_solve_mixed(mdp_context *ctx, mdp_pointing *A, const mdp_
 
     const int64_t m = A->m, npix = bj.npix, n = 3 * npix, nmap = A->n_map();
     const double *inv = bj.inv.as<double>();
-    DevBuf        tod_a, tod_b, f_a, f_b, rb, gb1, gb2, hb, qb, cgb, db, scal;
+    DevBuf &tod_a = ctx->ws[0], &tod_b = ctx->ws[1], &f_a = ctx->ws[8], &f_b = ctx->ws[9], &rb = ctx->ws[10],
+           &gb1 = ctx->ws[2], &gb2 = ctx->ws[3], &hb = ctx->ws[4], &qb = ctx->ws[5], &cgb = ctx->ws[6],
+           &db = ctx->ws[11], &scal = ctx->ws[7];
     int           rc;
     if ((rc = tod_a.alloc(8 * m)) || (rc = tod_b.alloc(8 * m)) || (rc = f_a.alloc(4 * m)) || (rc = f_b.alloc(4 * m)) ||
         (rc = rb.alloc(8 * nmap)) || (rc = gb1.alloc(8 * nmap)) || (rc = gb2.alloc(8 * nmap)) ||
@@ -823,6 +851,10 @@ extern "C" int mdp_gls_solve_mixed(mdp_context *ctx, mdp_pointing *A, const mdp_
         MDP_CHECK_LAUNCH(ctx);
         MDP_TRY(fetch());
         const double rin0 = hs->res;
+        // inner target: inner_tol, or the reduction still needed (with a
+        // factor 2 margin) when that is smaller
+        const double need = 0.5 * params->tol / std::sqrt(res / res0);
+        const double itol = std::max(inner_tol, std::min(need, 0.5));
         for (int j = 1; j <= inner_maxiter && inner_total < params->maxiter; j++) {
             std::swap(g, gp);
             if (prof) cudaEventRecord(ctx->ev[0], st);
@@ -852,7 +884,7 @@ extern "C" int mdp_gls_solve_mixed(mdp_context *ctx, mdp_pointing *A, const mdp_
                 mdp_set_error("mdp_gls_solve_mixed: inner residual became %f", hs->res);
                 return MDP_ENAN;
             }
-            if (hs->res <= inner_tol * inner_tol * rin0) break;
+            if (hs->res <= itol * itol * rin0) break;
             pcg_direction_kernel<<<gn, 256, 0, st>>>(h, Cg, n, S);
             MDP_CHECK_LAUNCH(ctx);
         }

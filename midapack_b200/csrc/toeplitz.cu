@@ -24,6 +24,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -506,13 +507,6 @@ __global__ void white_kernel(const double *__restrict__ vin, double *__restrict_
 }
 
 // ------------------------------------------------------------------ plan
-struct NoiseExtra {
-    DevBuf chunk_start, chunk_len, blk_chunk0, blk_nchunk, partial;
-    int    n_chunks = 0;
-    bool   covers_all = true;
-};
-static std::map<const mdp_noise *, NoiseExtra *> g_extra;
-
 // Tile kernels that exist, per precision: one CTA of 2^6 .. 2^LMAX complex
 // points, or clusters of 2, 4 or 8 CTAs of 2^(LMAX-1) or 2^LMAX points each
 // (LMAX = 13 for FP64 and 14 for FP32: 128 KiB of tile per CTA).
@@ -874,8 +868,9 @@ extern "C" int mdp_noise_create(mdp_context *ctx, int nb_blocks, const int64_t *
         }
         max_block = std::max<int64_t>(max_block, h_n[b]);
     }
+    static std::atomic<uint64_t> next_uid{1};
     mdp_noise  *N = new mdp_noise();
-    NoiseExtra *X = new NoiseExtra();
+    N->uid = next_uid++;
     N->nb = nb_blocks;
     N->lambda = lambda;
     N->max_block = max_block;
@@ -885,12 +880,11 @@ extern "C" int mdp_noise_create(mdp_context *ctx, int nb_blocks, const int64_t *
     int64_t expect = 0;
     for (int b = 0; b < nb_blocks; b++) {
         N->h_T0[b] = h_T[(size_t) b * lambda];
-        if (h_idv[b] != expect) X->covers_all = false;
+        if (h_idv[b] != expect) N->covers_all = false;
         expect = h_idv[b] + h_n[b];
     }
     N->nrow_end = expect;
     auto fail = [&](int rc) {
-        delete X;
         delete N;
         return rc;
     };
@@ -915,17 +909,17 @@ extern "C" int mdp_noise_create(mdp_context *ctx, int nb_blocks, const int64_t *
         }
         cn[b] = (int32_t) cs.size() - c0[b];
     }
-    X->n_chunks = (int) cs.size();
-    if ((rc = X->chunk_start.alloc(8 * std::max<size_t>(cs.size(), 1))) ||
-        (rc = X->chunk_len.alloc(4 * std::max<size_t>(cl.size(), 1))) || (rc = X->blk_chunk0.alloc(4 * nb_blocks)) ||
-        (rc = X->blk_nchunk.alloc(4 * nb_blocks)) || (rc = X->partial.alloc(8 * std::max<size_t>(cs.size(), 1))))
+    N->n_chunks = (int) cs.size();
+    if ((rc = N->chunk_start.alloc(8 * std::max<size_t>(cs.size(), 1))) ||
+        (rc = N->chunk_len.alloc(4 * std::max<size_t>(cl.size(), 1))) || (rc = N->blk_chunk0.alloc(4 * nb_blocks)) ||
+        (rc = N->blk_nchunk.alloc(4 * nb_blocks)) || (rc = N->partial.alloc(8 * std::max<size_t>(cs.size(), 1))))
         return fail(rc);
     if (!cs.empty()) {
-        cudaMemcpy(X->chunk_start.p, cs.data(), 8 * cs.size(), cudaMemcpyHostToDevice);
-        cudaMemcpy(X->chunk_len.p, cl.data(), 4 * cl.size(), cudaMemcpyHostToDevice);
+        cudaMemcpy(N->chunk_start.p, cs.data(), 8 * cs.size(), cudaMemcpyHostToDevice);
+        cudaMemcpy(N->chunk_len.p, cl.data(), 4 * cl.size(), cudaMemcpyHostToDevice);
     }
-    cudaMemcpy(X->blk_chunk0.p, c0.data(), 4 * nb_blocks, cudaMemcpyHostToDevice);
-    cudaMemcpy(X->blk_nchunk.p, cn.data(), 4 * nb_blocks, cudaMemcpyHostToDevice);
+    cudaMemcpy(N->blk_chunk0.p, c0.data(), 4 * nb_blocks, cudaMemcpyHostToDevice);
+    cudaMemcpy(N->blk_nchunk.p, cn.data(), 4 * nb_blocks, cudaMemcpyHostToDevice);
 
     if (lambda > 1) {
         // distinct block rows share one spectrum
@@ -961,20 +955,11 @@ extern "C" int mdp_noise_create(mdp_context *ctx, int nb_blocks, const int64_t *
         mdp_set_error("mdp_noise_create: %s", cudaGetErrorString(e));
         return fail(MDP_ECUDA);
     }
-    g_extra[N] = X;
     *out = N;
     return MDP_OK;
 }
 
-extern "C" void mdp_noise_destroy(mdp_noise *N) {
-    if (!N) return;
-    auto it = g_extra.find(N);
-    if (it != g_extra.end()) {
-        delete it->second;
-        g_extra.erase(it);
-    }
-    delete N;
-}
+extern "C" void mdp_noise_destroy(mdp_noise *N) { delete N; }
 
 extern "C" int mdp_noise_tile(const mdp_noise *N, int *fft_size, int *cluster_ctas, int64_t *n_tiles) {
     if (!N) return MDP_EINVAL;
@@ -985,16 +970,15 @@ extern "C" int mdp_noise_tile(const mdp_noise *N, int *fft_size, int *cluster_ct
 }
 
 int mdp_block_means(mdp_context *ctx, const mdp_noise *N, const double *d_v, double *d_means) {
-    NoiseExtra *X = g_extra.at(N);
-    if (X->n_chunks == 0) {
+    if (N->n_chunks == 0) {
         MDP_CUDA(cudaMemsetAsync(d_means, 0, 8 * N->nb, ctx->stream));
         return MDP_OK;
     }
-    block_partial_sums<double><<<X->n_chunks, 512, 0, ctx->stream>>>(d_v, X->chunk_start.as<int64_t>(),
-                                                             X->chunk_len.as<int32_t>(), X->partial.as<double>());
+    block_partial_sums<double><<<N->n_chunks, 512, 0, ctx->stream>>>(d_v, N->chunk_start.as<int64_t>(),
+                                                             N->chunk_len.as<int32_t>(), N->partial.as<double>());
     MDP_CHECK_LAUNCH(ctx);
     block_means_final<<<grid_for(N->nb, 128, 1024), 128, 0, ctx->stream>>>(
-            X->partial.as<double>(), X->blk_chunk0.as<int32_t>(), X->blk_nchunk.as<int32_t>(), N->blk_len.as<int32_t>(),
+            N->partial.as<double>(), N->blk_chunk0.as<int32_t>(), N->blk_nchunk.as<int32_t>(), N->blk_len.as<int32_t>(),
             N->nb, d_means);
     MDP_CHECK_LAUNCH(ctx);
     return MDP_OK;
@@ -1002,8 +986,7 @@ int mdp_block_means(mdp_context *ctx, const mdp_noise *N, const double *d_v, dou
 
 // out = N^-1 in (in != out required); d_means: precomputed block means or nullptr to compute here
 int mdp_stbmm_impl(mdp_context *ctx, const mdp_noise *N, const double *d_in, double *d_out, const double *d_means) {
-    NoiseExtra *X = g_extra.at(N);
-    if (!X->covers_all)
+    if (!N->covers_all)
         MDP_CUDA(cudaMemcpyAsync(d_out, d_in, sizeof(double) * N->nrow_end, cudaMemcpyDeviceToDevice, ctx->stream));
     if (N->lambda == 1) {
         dim3 grid(std::max(1, std::min(64, (int) ((N->h_n.empty() ? 1 : N->h_n[0]) / 256 + 1))), N->nb);
@@ -1054,15 +1037,14 @@ __global__ void __launch_bounds__(512) matvec_chunk_sums_kernel(const int32_t *_
 // not in the triplet layout; the caller then runs P and N^-1 separately.
 int mdp_matvec_blockmeans(mdp_context *ctx, const mdp_pointing *A, const mdp_noise *N, const double *d_x,
                           double *d_y) {
-    NoiseExtra *X = g_extra.at(N);
-    if (!A->triplet || !X->covers_all || N->lambda == 1 || N->nrow_end != A->m || X->n_chunks == 0)
+    if (!A->triplet || !N->covers_all || N->lambda == 1 || N->nrow_end != A->m || N->n_chunks == 0)
         return MDP_EUNSUPPORTED;
-    matvec_chunk_sums_kernel<<<X->n_chunks, 512, 0, ctx->stream>>>(A->off.as<int32_t>(), A->values, d_x, d_y,
-                                                                   X->chunk_start.as<int64_t>(),
-                                                                   X->chunk_len.as<int32_t>(), X->partial.as<double>());
+    matvec_chunk_sums_kernel<<<N->n_chunks, 512, 0, ctx->stream>>>(A->off.as<int32_t>(), A->values, d_x, d_y,
+                                                                   N->chunk_start.as<int64_t>(),
+                                                                   N->chunk_len.as<int32_t>(), N->partial.as<double>());
     MDP_CHECK_LAUNCH(ctx);
     block_means_final<<<grid_for(N->nb, 128, 1024), 128, 0, ctx->stream>>>(
-            X->partial.as<double>(), X->blk_chunk0.as<int32_t>(), X->blk_nchunk.as<int32_t>(), N->blk_len.as<int32_t>(),
+            N->partial.as<double>(), N->blk_chunk0.as<int32_t>(), N->blk_nchunk.as<int32_t>(), N->blk_len.as<int32_t>(),
             N->nb, N->means.as<double>());
     MDP_CHECK_LAUNCH(ctx);
     return MDP_OK;
@@ -1093,9 +1075,8 @@ __global__ void white32_kernel(const float *__restrict__ vin, float *__restrict_
 // out = N^-1 in with the FP32 tile kernels; d_means (FP64 block means of in)
 // may be given (fused into the producer of in) or nullptr
 int mdp_stbmm_impl32(mdp_context *ctx, mdp_noise *N, const float *d_in, float *d_out, const double *d_means) {
-    NoiseExtra *X = g_extra.at(N);
     MDP_TRY(mdp_noise_prepare_fp32(ctx, N));
-    if (!X->covers_all)
+    if (!N->covers_all)
         MDP_CUDA(cudaMemcpyAsync(d_out, d_in, sizeof(float) * N->nrow_end, cudaMemcpyDeviceToDevice, ctx->stream));
     if (N->lambda == 1) {
         dim3 grid(64, N->nb);
@@ -1105,12 +1086,12 @@ int mdp_stbmm_impl32(mdp_context *ctx, mdp_noise *N, const float *d_in, float *d
         return MDP_OK;
     }
     if (!d_means) {
-        if (X->n_chunks > 0) {
-            block_partial_sums<float><<<X->n_chunks, 512, 0, ctx->stream>>>(
-                    d_in, X->chunk_start.as<int64_t>(), X->chunk_len.as<int32_t>(), X->partial.as<double>());
+        if (N->n_chunks > 0) {
+            block_partial_sums<float><<<N->n_chunks, 512, 0, ctx->stream>>>(
+                    d_in, N->chunk_start.as<int64_t>(), N->chunk_len.as<int32_t>(), N->partial.as<double>());
             MDP_CHECK_LAUNCH(ctx);
             block_means_final<<<grid_for(N->nb, 128, 1024), 128, 0, ctx->stream>>>(
-                    X->partial.as<double>(), X->blk_chunk0.as<int32_t>(), X->blk_nchunk.as<int32_t>(),
+                    N->partial.as<double>(), N->blk_chunk0.as<int32_t>(), N->blk_nchunk.as<int32_t>(),
                     N->blk_len.as<int32_t>(), N->nb, N->means.as<double>());
             MDP_CHECK_LAUNCH(ctx);
         }
@@ -1124,8 +1105,7 @@ int mdp_stbmm_impl32(mdp_context *ctx, mdp_noise *N, const float *d_in, float *d
 // are left untouched.  The blocks must cover rows [0, nrow_end) and lambda > 1.
 int mdp_stbmm32_batch(mdp_context *ctx, mdp_noise *N, const float *d_in, float *d_out, int ncols,
                       int64_t col_stride, const double *d_means, const int *d_active) {
-    NoiseExtra *X = g_extra.at(N);
-    if (!X->covers_all || N->lambda == 1 || !d_means) return MDP_EUNSUPPORTED;
+    if (!N->covers_all || N->lambda == 1 || !d_means) return MDP_EUNSUPPORTED;
     MDP_TRY(mdp_noise_prepare_fp32(ctx, N));
     return launch_tiles<float>(ctx, N, N->p32, d_in, d_out, d_means, ncols, col_stride, d_active);
 }
@@ -1133,13 +1113,12 @@ int mdp_stbmm32_batch(mdp_context *ctx, mdp_noise *N, const float *d_in, float *
 // chunks of the block-mean reduction (65536 rows each, in block order)
 int mdp_noise_chunks(const mdp_noise *N, int *n_chunks, const int64_t **d_chunk_start, const int32_t **d_chunk_len,
                      const int32_t **d_blk_chunk0, const int32_t **d_blk_nchunk, int *covers_all) {
-    NoiseExtra *X = g_extra.at(N);
-    *n_chunks = X->n_chunks;
-    *d_chunk_start = X->chunk_start.as<int64_t>();
-    *d_chunk_len = X->chunk_len.as<int32_t>();
-    *d_blk_chunk0 = X->blk_chunk0.as<int32_t>();
-    *d_blk_nchunk = X->blk_nchunk.as<int32_t>();
-    *covers_all = X->covers_all ? 1 : 0;
+    *n_chunks = N->n_chunks;
+    *d_chunk_start = N->chunk_start.as<int64_t>();
+    *d_chunk_len = N->chunk_len.as<int32_t>();
+    *d_blk_chunk0 = N->blk_chunk0.as<int32_t>();
+    *d_blk_nchunk = N->blk_nchunk.as<int32_t>();
+    *covers_all = N->covers_all ? 1 : 0;
     return MDP_OK;
 }
 
@@ -1176,15 +1155,14 @@ __global__ void __launch_bounds__(512) matvec32_chunk_sums_kernel(const int32_t 
 
 int mdp_matvec32_blockmeans(mdp_context *ctx, const mdp_pointing *A, const mdp_noise *N, const double *d_x,
                             float *d_y) {
-    NoiseExtra *X = g_extra.at(N);
-    if (!A->triplet || !A->w32.p || !X->covers_all || N->lambda == 1 || N->nrow_end != A->m || X->n_chunks == 0)
+    if (!A->triplet || !A->w32.p || !N->covers_all || N->lambda == 1 || N->nrow_end != A->m || N->n_chunks == 0)
         return MDP_EUNSUPPORTED;
-    matvec32_chunk_sums_kernel<<<X->n_chunks, 512, 0, ctx->stream>>>(A->off.as<int32_t>(), A->w32.as<float>(), d_x, d_y,
-                                                                     X->chunk_start.as<int64_t>(),
-                                                                     X->chunk_len.as<int32_t>(), X->partial.as<double>());
+    matvec32_chunk_sums_kernel<<<N->n_chunks, 512, 0, ctx->stream>>>(A->off.as<int32_t>(), A->w32.as<float>(), d_x, d_y,
+                                                                     N->chunk_start.as<int64_t>(),
+                                                                     N->chunk_len.as<int32_t>(), N->partial.as<double>());
     MDP_CHECK_LAUNCH(ctx);
     block_means_final<<<grid_for(N->nb, 128, 1024), 128, 0, ctx->stream>>>(
-            X->partial.as<double>(), X->blk_chunk0.as<int32_t>(), X->blk_nchunk.as<int32_t>(), N->blk_len.as<int32_t>(),
+            N->partial.as<double>(), N->blk_chunk0.as<int32_t>(), N->blk_nchunk.as<int32_t>(), N->blk_len.as<int32_t>(),
             N->nb, N->means.as<double>());
     MDP_CHECK_LAUNCH(ctx);
     return MDP_OK;
@@ -1281,11 +1259,10 @@ extern "C" int mdp_stbmm_noalloc(mdp_context *ctx, const mdp_noise *N, const dou
         mdp_set_error("mdp_stbmm_noalloc: in-place application needs a copy of the input; pass d_out != d_in");
         return MDP_EINVAL;
     }
-    NoiseExtra   *X = g_extra.at(N);
-    const int64_t need = (int64_t) X->n_chunks + N->nb;
+    const int64_t need = (int64_t) N->n_chunks + N->nb;
     if (N->lambda > 1 && need > MDP_NOALLOC_SCRATCH_DOUBLES) {
         mdp_set_error("mdp_stbmm_noalloc: %lld scratch doubles needed (%d blocks, %d 65536-row chunks), limit %d",
-                      (long long) need, N->nb, X->n_chunks, MDP_NOALLOC_SCRATCH_DOUBLES);
+                      (long long) need, N->nb, N->n_chunks, MDP_NOALLOC_SCRATCH_DOUBLES);
         return MDP_EINVAL;
     }
     MDP_CUDA(cudaSetDevice(ctx->device));
@@ -1293,13 +1270,13 @@ extern "C" int mdp_stbmm_noalloc(mdp_context *ctx, const mdp_noise *N, const dou
     MDP_TRY(noalloc_scratch(ctx->device, &scratch));
     if (N->lambda == 1) return mdp_stbmm_impl(ctx, N, d_in, d_out, nullptr);  // no mean removal, no scratch
     double *partial = scratch;                 // [n_chunks], each written before it is read
-    double *means = scratch + X->n_chunks;     // [nb], each written before it is read
-    if (X->n_chunks > 0) {
-        block_partial_sums<double><<<X->n_chunks, 512, 0, ctx->stream>>>(d_in, X->chunk_start.as<int64_t>(),
-                                                                 X->chunk_len.as<int32_t>(), partial);
+    double *means = scratch + N->n_chunks;     // [nb], each written before it is read
+    if (N->n_chunks > 0) {
+        block_partial_sums<double><<<N->n_chunks, 512, 0, ctx->stream>>>(d_in, N->chunk_start.as<int64_t>(),
+                                                                 N->chunk_len.as<int32_t>(), partial);
         MDP_CHECK_LAUNCH(ctx);
         block_means_final<<<grid_for(N->nb, 128, 1024), 128, 0, ctx->stream>>>(
-                partial, X->blk_chunk0.as<int32_t>(), X->blk_nchunk.as<int32_t>(), N->blk_len.as<int32_t>(), N->nb,
+                partial, N->blk_chunk0.as<int32_t>(), N->blk_nchunk.as<int32_t>(), N->blk_len.as<int32_t>(), N->nb,
                 means);
         MDP_CHECK_LAUNCH(ctx);
     } else {
