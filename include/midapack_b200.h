@@ -102,11 +102,13 @@ int  mdp_noise_tile_fp32(mdp_context *ctx, mdp_noise *N, int *fft_size, int *clu
 /* Launch shape of a tile plan (fp32 = 0: FP64 tiles, 1: FP32 tiles, built on
  * first use): 2^log2_cta_points complex points per CTA, CTAs per cluster,
  * threads per CTA, and whether the autotuner picked it (1) by timing the
- * candidate plans on this device, or the cost model did (0).  The autotuner
- * runs once per precision, band (ceil log2 lambda) and block length class;
+ * candidate plans on this device, or the cost model did (0).  A split plan
+ * (three kernels, four-step FFT of 2^split_log_m1 x 2^split_log_m2 points)
+ * reports split_log_m1 > 0 and cluster 0.  The autotuner runs once per
+ * precision, band (ceil log2 lambda) and block length class;
  * MDP_TOEPLITZ_TUNE=0 switches it off. */
 int  mdp_noise_plan(mdp_context *ctx, mdp_noise *N, int fp32, int *log2_cta_points, int *cluster_ctas,
-                    int *threads, int *tuned);
+                    int *threads, int *tuned, int *split_log_m1, int *split_log_m2);
 /* No counterpart in the reference.  out = N^-1 in like mdp_stbmm, but the call
  * allocates no device memory: for callers that cannot call cudaMalloc while
  * they apply the operator (a memory arena or pool that owns the device memory,

@@ -89,7 +89,8 @@ _SIGS = {
                                        ct.c_int64, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                        ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "mdp_noise_plan": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_int, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int),
-                                  ct.POINTER(ct.c_int), ct.POINTER(ct.c_int)]),
+                                  ct.POINTER(ct.c_int), ct.POINTER(ct.c_int), ct.POINTER(ct.c_int),
+                                  ct.POINTER(ct.c_int)]),
     "mdp_gls_solve": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                  ct.POINTER(SolveParams), ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                  c_f64p, ct.POINTER(SolveInfo)]),
@@ -271,8 +272,11 @@ class Noise:
               "mdp_noise_create")
 
     def _plan(self, fp32: int):
-        lm, c, th, tu = ct.c_int(), ct.c_int(), ct.c_int(), ct.c_int()
-        check(lib().mdp_noise_plan(self.ctx.h, self.h, fp32, ct.byref(lm), ct.byref(c), ct.byref(th), ct.byref(tu)))
+        lm, c, th, tu, s1, s2 = (ct.c_int() for _ in range(6))
+        check(lib().mdp_noise_plan(self.ctx.h, self.h, fp32, ct.byref(lm), ct.byref(c), ct.byref(th), ct.byref(tu),
+                                   ct.byref(s1), ct.byref(s2)))
+        if s1.value:
+            return dict(split=[1 << s1.value, 1 << s2.value], tuned=bool(tu.value))
         return dict(cta_points=1 << lm.value, threads=th.value, tuned=bool(tu.value))
 
     def tile(self):

@@ -145,6 +145,10 @@ struct mdp_pointing {
 // solver).  V = double2 or float2.
 struct mdp_tile_plan {
     int     ready = 0;
+    int     split = 0;     // 0: one kernel (one CTA or cluster per tile); 1: three-kernel four-step FFT
+    int     log_m1 = 0, log_m2 = 0;  // split: M = 2^log_m1 * 2^log_m2 complex points per tile
+    DevBuf  scratch;       // split: [n_tiles][M] complex work array
+    DevBuf  ltw2, wa, wb;  // split: row-pass twiddles, W_M factor tables
     int     log2_ml = 0;   // per-CTA complex points = 2^log2_ml
     int     cluster = 1;   // CTAs per tile
     int     threads = 0;   // threads per CTA

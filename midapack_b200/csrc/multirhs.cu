@@ -628,6 +628,7 @@ int run_multi(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, const BJState &bj
     // the batched iteration as two CUDA graphs (g and gp alternate)
     cudaGraphExec_t gx[2] = {nullptr, nullptr};
     bool            graphs = prm->use_graph != 0;
+    uint64_t        graph_launches = 0;  // kernels in one replay
     if (graphs) {
         // captured on a private stream (the context stream may be the legacy
         // default stream, which cannot be captured); replayed on the context stream
@@ -649,6 +650,7 @@ int run_multi(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, const BJState &bj
             int         rc = launch_iteration<G>(ctx, A, N, B, inv, bufs[k ^ 1], bufs[k], hs);
             cudaError_t e = cudaStreamEndCapture(cap, &graph);
             ctx->stream = st;
+            graph_launches = ctx->launches - l0;
             ctx->launches = l0;
             cudaError_t ei = (rc == MDP_OK && e == cudaSuccess && graph) ? cudaGraphInstantiate(&gx[k], graph, 0)
                                                                          : cudaErrorUnknown;
@@ -685,8 +687,7 @@ int run_multi(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, const BJState &bj
                 rc = MDP_ECUDA;
                 break;
             }
-            // launches of the graph: direction, P, means, N^-1, (memset), P^T, coeff, update
-            ctx->launches += 7;
+            ctx->launches += graph_launches;
         } else if ((rc = launch_iteration<G>(ctx, A, N, B, inv, gnew, gold, hs))) {
             break;
         }

@@ -262,20 +262,29 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgsT<T> a) {
     // ---- load this CTA's 2*ML real samples of the window (zero outside the block)
     T            *sd = reinterpret_cast<T *>(smem);
     const int64_t r0 = ws + (int64_t) rank * 2 * ML;
-    // batches of 8 independent loads per thread keep many HBM requests in flight
-    for (int j0 = threadIdx.x; j0 < 2 * ML; j0 += 8 * blockDim.x) {
-        T v[8];
-#pragma unroll
-        for (int u = 0; u < 8; u++) {
-            const int     j = j0 + u * blockDim.x;
-            const int64_t row = r0 + j;
-            v[u] = (j < 2 * ML && row >= bs && row < be) ? __ldg(a.vin + row) : mu;
+    // Asynchronous element copies global -> shared (no register staging, the
+    // whole part in flight at once), zero-filled outside the block, into the
+    // swizzled layout; then the block mean is removed in place.
+    {
+        const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(sd));
+        for (int j = threadIdx.x; j < 2 * ML; j += blockDim.x) {
+            const int64_t  row = r0 + j;
+            const bool     in = row >= bs && row < be;
+            const T       *src = in ? a.vin + row : a.vin;
+            const uint32_t dst = sbase + (uint32_t) (sizeof(T) * (2 * swzv(V{}, j >> 1) + (j & 1)));
+            if constexpr (sizeof(T) == 4)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(src), "r"(in ? 4 : 0)
+                             : "memory");
+            else
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(in ? 8 : 0)
+                             : "memory");
         }
-#pragma unroll
-        for (int u = 0; u < 8; u++) {
-            const int j = j0 + u * blockDim.x;
-            if (j < 2 * ML) sd[2 * swzv(V{}, j >> 1) + (j & 1)] = v[u] - mu;
-        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        if (mu != (T) 0)
+            for (int j = threadIdx.x; j < 2 * ML; j += blockDim.x) {
+                const int64_t row = r0 + j;
+                if (row >= bs && row < be) sd[2 * swzv(V{}, j >> 1) + (j & 1)] -= mu;
+            }
     }
 
     if constexpr (C > 1) {
@@ -380,6 +389,296 @@ __global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgsT<T> a) {
     }
 }
 
+// ------------------------------------------------------------------ split tiles
+// The same overlap-save tile product as toeplitz_tile_kernel, as a four-step
+// FFT in three kernels with the tile's spectrum in a global scratch array
+// (M = M1*M2 complex points per tile, z[M2*j1 + j2] = x[2j] + i x[2j+1]):
+//   split_cols_kernel  (forward)  per column j2: M1-point DFT over j1, times
+//                      W_M^(j2 k1) -> Y[k1][j2]
+//   split_rows_kernel  per row pair (k1, M1-k1): M2-point DFT of both rows,
+//                      the real-FFT untangle / spectrum product / re-tangle of
+//                      the pairs (k, M-k) (k = k1 + M1 k2 and M-k lie in the
+//                      paired rows), inverse DFT of both rows, times W_M^(-j2 k1)
+//   split_cols_kernel  (inverse)  per column: inverse M1-point DFT over k1
+//                      (as conj(DFT(conj)) ), store of the tile's central
+//                      outputs scaled by 1/M
+// Every CTA is small (tens of KiB of shared memory, several per SM) and none
+// waits on another CTA: the latency of one CTA's loads is hidden by the others.
+// Shared layout of a batch of sequences: element i of sequence b at
+// b*L + (i ^ (b & min(L,32)-1)), so that a warp working on 32 sequences at the
+// same position spreads over all banks.
+template <int L>
+__device__ __forceinline__ int sq_idx(int b, int i) {
+    constexpr int XM = (L < 32 ? L : 32) - 1;
+    return b * L + (i ^ (b & XM));
+}
+
+// one DIF (or DIT) pass of radix R at group size G over nseq sequences of length L
+template <typename V, int R, int L, bool INVERSE>
+__device__ __forceinline__ void seq_pass(V *s, int nseq, int G, const V *wl) {
+    const int stride = G / R;
+    const int nsets = nseq * (L / R);
+    for (int t = threadIdx.x; t < nsets; t += blockDim.x) {
+        const int b = t % nseq;
+        const int r = t / nseq;
+        const int g = r / stride, q = r - g * stride;
+        const int base = g * G + q;
+        const V   w = wl[q];
+        V         v[R];
+#pragma unroll
+        for (int i = 0; i < R; i++) v[i] = s[sq_idx<L>(b, base + i * stride)];
+        if (INVERSE) dit_set<V, R>(v, w);
+        else dif_set<V, R>(v, w);
+#pragma unroll
+        for (int i = 0; i < R; i++) s[sq_idx<L>(b, base + i * stride)] = v[i];
+    }
+    __syncthreads();
+}
+
+// full length-L transform of nseq sequences (DIF: natural in, bit-reversed out;
+// INVERSE: DIT with conjugate twiddles, bit-reversed in, natural out)
+template <typename V, int LOG_L, bool INVERSE>
+__device__ __forceinline__ void seq_fft(V *s, int nseq, const V *stw) {
+    constexpr int NP = ltw_passes(LOG_L);
+    constexpr int L = 1 << LOG_L;
+#pragma unroll
+    for (int pi = 0; pi < NP; pi++) {
+        const int p = INVERSE ? (NP - 1 - pi) : pi;
+        const int logG = LOG_L - 4 * p;
+        const int k = logG >= 4 ? 4 : logG;
+        const int G = 1 << logG;
+        const V  *wl = stw + ltw_offset(LOG_L, p);
+        if (k == 4) seq_pass<V, 16, L, INVERSE>(s, nseq, G, wl);
+        else if (k == 3) seq_pass<V, 8, L, INVERSE>(s, nseq, G, wl);
+        else if (k == 2) seq_pass<V, 4, L, INVERSE>(s, nseq, G, wl);
+        else seq_pass<V, 2, L, INVERSE>(s, nseq, G, wl);
+    }
+}
+
+template <typename T>
+struct SplitArgsT {
+    using V = typename CT<T>::V;
+    const T       *vin;
+    T             *vout;
+    V             *Y;           // [n_tiles][M1][M2] scratch
+    const int64_t *tile_start;
+    const int32_t *tile_block;
+    const int64_t *blk_start;
+    const int32_t *blk_len;
+    const int32_t *blk_spec;
+    const V       *hpair;       // [n_spec][M/2+1] in split pair order
+    const V       *ttw;         // [M/2+1] W_N^k in split pair order
+    const V       *ltw1, *ltw2; // packed pass twiddles of the M1- and M2-point transforms
+    const V       *wa, *wb;     // W_M^e = wa[e >> 8] * wb[e & 255]
+    const double  *means;
+    int            lambda;
+    int            nb;
+    int64_t        col_stride;
+    const int     *active;
+    int            log_m1, log_m2;
+};
+
+template <typename V>
+__device__ __forceinline__ V split_tw(const V *wa, const V *wb, int e) {  // W_M^e
+    return cmul(wa[e >> 8], wb[e & 255]);
+}
+
+// threads of a split kernel working on `work` complex points (one radix-16 set each)
+__host__ __device__ constexpr int split_nt(int work) { return work / 16 < 64 ? 64 : (work / 16 > 512 ? 512 : work / 16); }
+
+// forward (INV = false) or inverse (INV = true) column transforms of one tile:
+// CW consecutive columns per CTA
+template <typename T, int LOG_M1, int CW, bool INV>
+__global__ void __launch_bounds__(split_nt(CW << LOG_M1)) split_cols_kernel(SplitArgsT<T> a) {
+    using V = typename CT<T>::V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V            *s = reinterpret_cast<V *>(smem_raw);
+    constexpr int M1 = 1 << LOG_M1;
+    constexpr int NT = split_nt(CW * M1);      // == blockDim.x
+    constexpr int EPT = (CW * M1 + NT - 1) / NT;  // elements per thread
+    const int     M2 = 1 << a.log_m2;
+    const int     M = M1 * M2;
+    const int     ncg = M2 / CW;
+    const int64_t tile = blockIdx.x / ncg;
+    const int     c0 = (int) (blockIdx.x % ncg) * CW;
+    if (a.active && !a.active[blockIdx.y]) return;
+    if (blockIdx.y) {
+        a.vin += (int64_t) blockIdx.y * a.col_stride;
+        a.vout += (int64_t) blockIdx.y * a.col_stride;
+        if (a.means) a.means += (int64_t) blockIdx.y * a.nb;
+    }
+    V *Y = a.Y + (tile * M);
+    // stage the pass twiddles and the W_M factor tables
+    constexpr int NLTW = ltw_size(LOG_M1);
+    V            *stw = s + CW * M1;
+    V            *swa = stw + NLTW;
+    V            *swb = swa + ((M >> 8) > 0 ? (M >> 8) : 1);
+    for (int i = threadIdx.x; i < NLTW; i += blockDim.x) stw[i] = __ldg(a.ltw1 + i);
+    for (int i = threadIdx.x; i < (M >> 8); i += blockDim.x) swa[i] = __ldg(a.wa + i);
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) swb[i] = __ldg(a.wb + i);
+    const int     blk = a.tile_block[tile];
+    const int64_t bs = a.blk_start[blk];
+    const int64_t be = bs + a.blk_len[blk];
+    const int64_t t0 = a.tile_start[tile];
+    const int64_t ws = t0 - (a.lambda - 1);
+    // all loads of a thread are issued before its shared-memory stores
+    if (!INV) {
+        const T mu = a.means ? (T) a.means[blk] : (T) 0;
+        // element (j1, c): samples ws + 2(M2 j1 + c0 + c) + {0, 1}
+        T x0[EPT], x1[EPT];
+#pragma unroll
+        for (int u = 0; u < EPT; u++) {
+            const int     e = threadIdx.x + u * NT;
+            const int     c = e % CW, j1 = e / CW;
+            const int64_t row = ws + 2 * ((int64_t) M2 * j1 + c0 + c);
+            const bool    ok = e < CW * M1;
+            x0[u] = (ok && row >= bs && row < be) ? __ldg(a.vin + row) - mu : (T) 0;
+            x1[u] = (ok && row + 1 >= bs && row + 1 < be) ? __ldg(a.vin + row + 1) - mu : (T) 0;
+        }
+#pragma unroll
+        for (int u = 0; u < EPT; u++) {
+            const int e = threadIdx.x + u * NT;
+            if (e < CW * M1) s[sq_idx<M1>(e % CW, e / CW)] = mkv(V{}, x0[u], x1[u]);
+        }
+    } else {
+        // Y'[k1][c0 + c], conjugated: the inverse DFT is conj(DFT(conj(.)))
+        V y[EPT];
+#pragma unroll
+        for (int u = 0; u < EPT; u++) {
+            const int e = threadIdx.x + u * NT;
+            if (e < CW * M1) y[u] = Y[(int64_t) (e / CW) * M2 + c0 + e % CW];
+        }
+#pragma unroll
+        for (int u = 0; u < EPT; u++) {
+            const int e = threadIdx.x + u * NT;
+            if (e < CW * M1) s[sq_idx<M1>(e % CW, e / CW)] = mkv(y[u], y[u].x, -y[u].y);
+        }
+    }
+    __syncthreads();
+    seq_fft<V, LOG_M1, false>(s, CW, stw);
+    if (!INV) {
+        // position p holds k1 = rev(p): Y[k1][j2] = W_M^(j2 k1) * value
+        for (int e = threadIdx.x; e < CW * M1; e += blockDim.x) {
+            const int c = e % CW, p = e / CW;
+            const int k1 = (int) (__brev((unsigned) p) >> (32 - LOG_M1));
+            const int j2 = c0 + c;
+            const V   v = s[sq_idx<M1>(c, p)];
+            Y[(int64_t) k1 * M2 + j2] = cmul(v, split_tw(swa, swb, (int) (((int64_t) j2 * k1) & (M - 1))));
+        }
+    } else {
+        // position p holds j1 = rev(p): z'[M2 j1 + j2] = conj(value) / M, samples 2(M2 j1 + j2) + {0, 1}
+        const int     E = 2 * M - 2 * (a.lambda - 1);
+        const int64_t out_end = min(t0 + (int64_t) E, be);
+        const T       scale = (T) 1 / (T) M;
+        for (int e = threadIdx.x; e < CW * M1; e += blockDim.x) {
+            const int     c = e % CW, p = e / CW;
+            const int     j1 = (int) (__brev((unsigned) p) >> (32 - LOG_M1));
+            const V       v = s[sq_idx<M1>(c, p)];
+            const int64_t row = ws + 2 * ((int64_t) M2 * j1 + c0 + c);
+            if (row >= t0 && row < out_end) a.vout[row] = v.x * scale;
+            if (row + 1 >= t0 && row + 1 < out_end) a.vout[row + 1] = -v.y * scale;
+        }
+    }
+}
+
+// row pairs of one tile: pair rp = 0 holds the self-paired rows 0 and M1/2,
+// pair rp > 0 the rows rp and M1 - rp; RP pairs (2 RP rows) per CTA
+template <typename T, int LOG_M2, int RP>
+__global__ void __launch_bounds__(split_nt(2 * RP << LOG_M2)) split_rows_kernel(SplitArgsT<T> a) {
+    using V = typename CT<T>::V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V            *s = reinterpret_cast<V *>(smem_raw);
+    constexpr int M2 = 1 << LOG_M2;
+    constexpr int NT = split_nt(2 * RP * M2);          // == blockDim.x
+    constexpr int EPT = (2 * RP * M2 + NT - 1) / NT;  // elements per thread
+    const int     M1 = 1 << a.log_m1;
+    const int     M = M1 * M2;
+    const int     npg = (M1 / 2) / RP;  // CTAs per tile
+    const int64_t tile = blockIdx.x / npg;
+    const int     rp0 = (int) (blockIdx.x % npg) * RP;
+    if (a.active && !a.active[blockIdx.y]) return;
+    V *Y = a.Y + (tile * M);
+    constexpr int NLTW = ltw_size(LOG_M2);
+    V            *stw = s + 2 * RP * M2;
+    V            *swa = stw + NLTW;
+    V            *swb = swa + ((M >> 8) > 0 ? (M >> 8) : 1);
+    for (int i = threadIdx.x; i < NLTW; i += blockDim.x) stw[i] = __ldg(a.ltw2 + i);
+    for (int i = threadIdx.x; i < (M >> 8); i += blockDim.x) swa[i] = __ldg(a.wa + i);
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) swb[i] = __ldg(a.wb + i);
+    const V *HP = a.hpair + (int64_t) a.blk_spec[a.tile_block[tile]] * (M / 2 + 1);
+    // slot r = 2 (rp - rp0) + {0: row A, 1: row B}
+    auto row_of = [&](int r) {
+        const int rp = rp0 + (r >> 1);
+        if (rp == 0) return (r & 1) ? M1 / 2 : 0;
+        return (r & 1) ? M1 - rp : rp;
+    };
+    {
+        V y[EPT];
+#pragma unroll
+        for (int u = 0; u < EPT; u++) {
+            const int e = threadIdx.x + u * NT;
+            if (e < 2 * RP * M2) y[u] = Y[(int64_t) row_of(e / M2) * M2 + e % M2];
+        }
+#pragma unroll
+        for (int u = 0; u < EPT; u++) {
+            const int e = threadIdx.x + u * NT;
+            if (e < 2 * RP * M2) s[sq_idx<M2>(e / M2, e % M2)] = y[u];
+        }
+    }
+    __syncthreads();
+    seq_fft<V, LOG_M2, false>(s, 2 * RP, stw);
+    // pairs (k, M-k): position p of row A with position M2-1-p of row B, or
+    // inside rows 0 and M1/2 for rp = 0 (table entries in the same order)
+    const T   half = (T) 0.5;
+    const int npairs = RP * M2 + (rp0 == 0 ? 1 : 0);
+    for (int i = threadIdx.x; i < npairs; i += blockDim.x) {
+        int pr, pa, pb, ra, rb;  // table entry, positions, slots
+        if (rp0 == 0 && i < M2 + 1) {
+            pr = i;
+            if (i < M2 / 2 + 1) {  // row 0: like a single tile of M2 points
+                ra = rb = 0;
+                int p = 2 * i;
+                if (i == M2 / 2) p = 1;
+                const int k2 = (int) (__brev((unsigned) p) >> (32 - LOG_M2));
+                pa = p;
+                pb = (int) (__brev((unsigned) ((M2 - k2) & (M2 - 1))) >> (32 - LOG_M2));
+            } else {  // row M1/2: k2 with M2-1-k2
+                ra = rb = 1;
+                pa = i - (M2 / 2 + 1);
+                pb = M2 - 1 - pa;
+            }
+        } else {
+            const int ii = (rp0 == 0) ? i - (M2 + 1) : i;
+            const int rl = (rp0 == 0 ? 1 : 0) + ii / M2;  // pair within the CTA
+            pa = ii % M2;
+            pb = M2 - 1 - pa;
+            ra = 2 * rl;
+            rb = 2 * rl + 1;
+            pr = (rp0 + rl == 0) ? 0 : (M2 + 1) + (rp0 + rl - 1) * M2 + pa;
+        }
+        const V hc = __ldg(HP + pr), wk = __ldg(a.ttw + pr);
+        V      *s1 = s + sq_idx<M2>(ra, pa), *s2 = s + sq_idx<M2>(rb, pb);
+        const V Z1 = *s1, Z2 = *s2;
+        const V E0 = mkv(Z1, half * (Z1.x + Z2.x), half * (Z1.y - Z2.y));
+        const V O0 = mkv(Z1, half * (Z1.y + Z2.y), -half * (Z1.x - Z2.x));
+        const T ca = hc.x, cb = hc.y;
+        const V wO = cmul(wk, O0);
+        const V Ep = mkv(Z1, ca * E0.x + cb * wO.x, ca * E0.y + cb * wO.y);
+        const V cE = cmulc(E0, wk);
+        const V Op = mkv(Z1, cb * cE.x + ca * O0.x, cb * cE.y + ca * O0.y);
+        *s1 = mkv(Z1, Ep.x - Op.y, Ep.y + Op.x);
+        if (s2 != s1) *s2 = mkv(Z1, Ep.x + Op.y, -Ep.y + Op.x);
+    }
+    __syncthreads();
+    seq_fft<V, LOG_M2, true>(s, 2 * RP, stw);
+    for (int e = threadIdx.x; e < 2 * RP * M2; e += blockDim.x) {
+        const int r = e / M2, j2 = e % M2;
+        const int k1 = row_of(r);
+        const V   v = s[sq_idx<M2>(r, j2)];
+        Y[(int64_t) k1 * M2 + j2] = cmulc(v, split_tw(swa, swb, (int) (((int64_t) j2 * k1) & (M - 1))));
+    }
+}
+
 // ------------------------------------------------------------------ spectra
 // H[k] = T0 + 2 sum_{i<lambda} T[i] cos(2 pi i k / N), k = 0..N/2: the DFT of
 // the circulant embedding, which is real and even.
@@ -415,6 +714,19 @@ __global__ void twist_pairs_kernel(const double *__restrict__ H, int M, int logM
             k = (int) (__brev((unsigned) (r * ML + 2 * i)) >> (32 - logM));
         }
         const T hk = (T) H[k], hm = (T) H[M - k];
+        out[e] = mkv(out[e], half * (hk + hm), half * (hk - hm));
+    }
+}
+
+// spectrum pairs of the split tiles in their pair order: kidx[e] = k of the
+// first element of pair e
+template <typename T>
+__global__ void split_pairs_kernel(const double *__restrict__ H, int M, const int32_t *__restrict__ kidx, int n,
+                                   typename CT<T>::V *__restrict__ out) {
+    const T half = (T) 0.5;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int k = kidx[e];
+        const T   hk = (T) H[k], hm = (T) H[M - k];
         out[e] = mkv(out[e], half * (hk + hm), half * (hk - hm));
     }
 }
@@ -548,9 +860,34 @@ static tile_fn_t<T> pick_kernel(int log_ml, int C) {
 
 struct TileCand {
     int log_ml, C, threads;
+    int split = 0, log_m1 = 0, log_m2 = 0;  // split plan: M = 2^log_m1 * 2^log_m2
 };
 
+static int64_t cand_N(const TileCand &c) {
+    return c.split ? (2LL << (c.log_m1 + c.log_m2)) : 2LL * c.C * (1LL << c.log_ml);
+}
+
+// split plans: columns of M1 <= 256 points, rows of 32 <= M2 <= 512 points
+static bool split_shape(int logM, int *lm1, int *lm2) {
+    int a = std::min(8, logM / 2), b = logM - a;
+    if (b > 9) return false;
+    if (b < 5) {
+        b = 5;
+        a = logM - 5;
+    }
+    if (a < 4) return false;
+    *lm1 = a;
+    *lm2 = b;
+    return true;
+}
+
 static int default_threads(int log_ml) { return std::min(512, std::max(64, (1 << log_ml) / 16)); }
+
+static int ceil_log2_i(int64_t v) {
+    int b = 0;
+    while ((1LL << b) < v) b++;
+    return b;
+}
 
 // every launchable configuration whose tile holds the band (E >= 1)
 template <typename T>
@@ -565,20 +902,30 @@ static std::vector<TileCand> tile_candidates(int lambda) {
             out.push_back({lml, C, default_threads(lml)});
             if (default_threads(lml) == 512) out.push_back({lml, C, 256});  // 2 CTAs per SM when registers allow
         }
+    for (int logM = 9; logM <= 17; logM++) {
+        TileCand c{0, 0, 0, 1, 0, 0};
+        if (!split_shape(logM, &c.log_m1, &c.log_m2)) continue;
+        if (cand_N(c) - 2LL * (lambda - 1) < 1) continue;
+        out.push_back(c);
+    }
     return out;
 }
 
 // cost model: FFT work per useful output, a penalty for cluster traffic, and
 // a penalty when a tile is much larger than the blocks it covers
 static double tile_model_cost(const TileCand &c, int lambda, int64_t max_block) {
-    const int64_t N = 2LL * c.C * (1LL << c.log_ml);
+    const int64_t N = cand_N(c);
     const int64_t E = N - 2LL * (lambda - 1);
-    int           logN = c.log_ml + 1;
-    for (int k = c.C; k > 1; k >>= 1) logN++;
-    const double eff = (double) std::min<int64_t>(E, std::max<int64_t>(max_block, 1));
-    double       cost = (double) N / eff * (logN + 3) + (c.C > 1 ? 3.0 * std::log2((double) c.C) : 0.0);
+    const int     logN = ceil_log2_i(N);
+    const double  eff = (double) std::min<int64_t>(E, std::max<int64_t>(max_block, 1));
+    double        cost = (double) N / eff * (logN + 3);
+    if (c.split) {
+        cost *= 1.3;  // scratch round trips; the timed choice decides
+    } else {
+        if (c.C > 1) cost += 3.0 * std::log2((double) c.C);
+        if (c.threads != default_threads(c.log_ml)) cost *= 1.01;  // ties go to the default launch shape
+    }
     if (E < N / 4) cost *= 1.5;
-    if (c.threads != default_threads(c.log_ml)) cost *= 1.01;  // ties go to the default launch shape
     return cost;
 }
 
@@ -674,7 +1021,8 @@ static int tune_plan(mdp_context *ctx, const mdp_noise *N, const std::vector<Til
     return rc;
 }
 
-// MDP_TOEPLITZ_PLAN[32]="log2_ml,cluster,threads" forces a plan;
+// MDP_TOEPLITZ_PLAN[32]="log2_ml,cluster,threads" (one-kernel tiles) or
+// "s,log_m1,log_m2" (split tiles) forces a plan;
 // MDP_TOEPLITZ_FFT[32]=N restricts the choice to tiles of N real samples (cost
 // model only); MDP_TOEPLITZ_TUNE=0 switches the autotuner off.
 template <typename T>
@@ -687,9 +1035,16 @@ static int choose_plan(mdp_context *ctx, const mdp_noise *N, TileCand *out, int 
     std::vector<TileCand> cands = tile_candidates<T>(N->lambda);
     if (plan) {
         TileCand c{0, 0, 0};
-        if (sscanf(plan, "%d,%d,%d", &c.log_ml, &c.C, &c.threads) != 3 || !pick_kernel<T>(c.log_ml, c.C) ||
-            c.threads < 32 || c.threads > 512 || (c.threads & 31) ||
-            2LL * c.C * (1LL << c.log_ml) - 2LL * (N->lambda - 1) < 1) {
+        bool     ok;
+        if (plan[0] == 's') {  // "s,log_m1,log_m2": split plan
+            c.split = 1;
+            ok = sscanf(plan + 1, ",%d,%d", &c.log_m1, &c.log_m2) == 2 && c.log_m1 >= 4 && c.log_m1 <= 8 &&
+                 c.log_m2 >= 5 && c.log_m2 <= 9;
+        } else {
+            ok = sscanf(plan, "%d,%d,%d", &c.log_ml, &c.C, &c.threads) == 3 && pick_kernel<T>(c.log_ml, c.C) &&
+                 c.threads >= 32 && c.threads <= 512 && !(c.threads & 31);
+        }
+        if (!ok || cand_N(c) - 2LL * (N->lambda - 1) < 1) {
             mdp_set_error("invalid tile plan '%s' for lambda=%d", plan, N->lambda);
             return MDP_EINVAL;
         }
@@ -700,7 +1055,7 @@ static int choose_plan(mdp_context *ctx, const mdp_noise *N, TileCand *out, int 
     if (forced) {
         std::vector<TileCand> keep;
         for (const TileCand &c : cands)
-            if (2LL * c.C * (1LL << c.log_ml) == forced) keep.push_back(c);
+            if (cand_N(c) == forced && !c.split) keep.push_back(c);
         cands.swap(keep);
     }
     if (cands.empty()) return MDP_EUNSUPPORTED;
@@ -712,7 +1067,7 @@ static int choose_plan(mdp_context *ctx, const mdp_noise *N, TileCand *out, int 
     // screen: tiles at least a quarter useful and not longer than twice the block plus the halo
     std::vector<TileCand> screen;
     for (const TileCand &c : cands) {
-        const int64_t Nn = 2LL * c.C * (1LL << c.log_ml), E = Nn - 2LL * (N->lambda - 1);
+        const int64_t Nn = cand_N(c), E = Nn - 2LL * (N->lambda - 1);
         if (E * 4 >= Nn && E <= 2 * std::max<int64_t>(N->max_block, 1) + 2LL * N->lambda) screen.push_back(c);
     }
     if (screen.size() <= 1) return MDP_OK;
@@ -722,7 +1077,7 @@ static int choose_plan(mdp_context *ctx, const mdp_noise *N, TileCand *out, int 
     auto                        it = g_tuned.find(key);
     if (it != g_tuned.end()) {
         const TileCand &c = it->second;
-        if (2LL * c.C * (1LL << c.log_ml) - 2LL * (N->lambda - 1) >= 1) {
+        if (cand_N(c) - 2LL * (N->lambda - 1) >= 1) {
             *out = c;
             *tuned = 1;
             return MDP_OK;
@@ -736,15 +1091,193 @@ static int choose_plan(mdp_context *ctx, const mdp_noise *N, TileCand *out, int 
     return MDP_OK;
 }
 
+// ---- split plans: kernels, shapes and tables
+template <typename T> struct SplitShape;
+template <> struct SplitShape<float> { static constexpr int CW = 32, RP = 4; };
+template <> struct SplitShape<double> { static constexpr int CW = 16, RP = 2; };
+
+template <typename T, bool INV>
+static const void *pick_cols(int log_m1) {
+    constexpr int CW = SplitShape<T>::CW;
+    switch (log_m1) {
+        case 4: return (const void *) split_cols_kernel<T, 4, CW, INV>;
+        case 5: return (const void *) split_cols_kernel<T, 5, CW, INV>;
+        case 6: return (const void *) split_cols_kernel<T, 6, CW, INV>;
+        case 7: return (const void *) split_cols_kernel<T, 7, CW, INV>;
+        case 8: return (const void *) split_cols_kernel<T, 8, CW, INV>;
+    }
+    return nullptr;
+}
+
+template <typename T>
+static const void *pick_rows(int log_m2) {
+    constexpr int RP = SplitShape<T>::RP;
+    switch (log_m2) {
+        case 5: return (const void *) split_rows_kernel<T, 5, RP>;
+        case 6: return (const void *) split_rows_kernel<T, 6, RP>;
+        case 7: return (const void *) split_rows_kernel<T, 7, RP>;
+        case 8: return (const void *) split_rows_kernel<T, 8, RP>;
+        case 9: return (const void *) split_rows_kernel<T, 9, RP>;
+    }
+    return nullptr;
+}
+
+template <typename V>
+static size_t split_cols_smem(int log_m1, int log_m2, int CW) {
+    const int M = 1 << (log_m1 + log_m2);
+    return sizeof(V) * ((size_t) CW * (1 << log_m1) + ltw_size(log_m1) + std::max(1, M >> 8) + 256);
+}
+template <typename V>
+static size_t split_rows_smem(int log_m1, int log_m2, int RP) {
+    const int M = 1 << (log_m1 + log_m2);
+    return sizeof(V) * ((size_t) 2 * RP * (1 << log_m2) + ltw_size(log_m2) + std::max(1, M >> 8) + 256);
+}
+
+static int rev_bits(int v, int bits) {
+    int r = 0;
+    for (int b = 0; b < bits; b++) r |= ((v >> b) & 1) << (bits - 1 - b);
+    return r;
+}
+
+// k of the first element of each pair, in the order split_rows_kernel visits them
+static std::vector<int32_t> split_pair_k(int log_m1, int log_m2) {
+    const int            M1 = 1 << log_m1, M2 = 1 << log_m2;
+    std::vector<int32_t> k;
+    k.reserve((size_t) M1 * M2 / 2 + 1);
+    for (int i = 0; i < M2 / 2 + 1; i++) {  // row 0
+        const int p = (i == M2 / 2) ? 1 : 2 * i;
+        k.push_back(M1 * rev_bits(p, log_m2));
+    }
+    for (int pa = 0; pa < M2 / 2; pa++) k.push_back(M1 / 2 + M1 * rev_bits(pa, log_m2));  // row M1/2
+    for (int rp = 1; rp < M1 / 2; rp++)
+        for (int pa = 0; pa < M2; pa++) k.push_back(rp + M1 * rev_bits(pa, log_m2));
+    return k;
+}
+
+template <typename T>
+static int build_split_tables(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, bool spectra) {
+    using V = typename CT<T>::V;
+    const int M = 1 << (P.log_m1 + P.log_m2), Nn = 2 * M;
+    std::vector<V> l1(ltw_size(P.log_m1)), l2(ltw_size(P.log_m2)), wa(std::max(1, M >> 8)), wb(256);
+    auto           pack = [](std::vector<V> &l, int log_l) {
+        for (int p = 0; p < ltw_passes(log_l); p++) {
+            const int logG = log_l - 4 * p, k = logG >= 4 ? 4 : logG, off = ltw_offset(log_l, p);
+            for (int q = 0; q < (1 << (logG - k)); q++) host_cexp(q, (long double) (1 << logG), &l[off + q]);
+        }
+    };
+    pack(l1, P.log_m1);
+    pack(l2, P.log_m2);
+    for (size_t i = 0; i < wa.size(); i++) host_cexp((long double) (256 * i), M, &wa[i]);
+    for (int j = 0; j < 256; j++) host_cexp(j, M, &wb[j]);
+    const std::vector<int32_t> kidx = split_pair_k(P.log_m1, P.log_m2);
+    const int                  npair = (int) kidx.size();
+    std::vector<V>             tt(npair);
+    for (int e = 0; e < npair; e++) host_cexp(kidx[e], Nn, &tt[e]);
+    MDP_TRY(P.ltw.alloc(sizeof(V) * l1.size()));
+    MDP_TRY(P.ltw2.alloc(sizeof(V) * l2.size()));
+    MDP_TRY(P.wa.alloc(sizeof(V) * wa.size()));
+    MDP_TRY(P.wb.alloc(sizeof(V) * wb.size()));
+    MDP_TRY(P.ttw.alloc(sizeof(V) * npair));
+    MDP_CUDA(cudaMemcpy(P.ltw.p, l1.data(), sizeof(V) * l1.size(), cudaMemcpyHostToDevice));
+    MDP_CUDA(cudaMemcpy(P.ltw2.p, l2.data(), sizeof(V) * l2.size(), cudaMemcpyHostToDevice));
+    MDP_CUDA(cudaMemcpy(P.wa.p, wa.data(), sizeof(V) * wa.size(), cudaMemcpyHostToDevice));
+    MDP_CUDA(cudaMemcpy(P.wb.p, wb.data(), sizeof(V) * wb.size(), cudaMemcpyHostToDevice));
+    MDP_CUDA(cudaMemcpy(P.ttw.p, tt.data(), sizeof(V) * npair, cudaMemcpyHostToDevice));
+    MDP_TRY(P.spectra.alloc(sizeof(V) * (size_t) N->n_spec * npair));
+    MDP_TRY(P.scratch.alloc(sizeof(V) * (size_t) std::max<int64_t>(P.n_tiles, 1) * M));
+    if (spectra) {
+        std::vector<double2> tw(M);
+        for (int k = 0; k < M; k++) host_cexp(k, Nn, &tw[k]);
+        DevBuf tw64, dH, dT, dk;
+        MDP_TRY(tw64.alloc(sizeof(double2) * M));
+        MDP_TRY(dH.alloc(sizeof(double) * (M + 1)));
+        MDP_TRY(dT.alloc(sizeof(double) * N->lambda));
+        MDP_TRY(dk.alloc(sizeof(int32_t) * npair));
+        MDP_CUDA(cudaMemcpy(tw64.p, tw.data(), sizeof(double2) * M, cudaMemcpyHostToDevice));
+        MDP_CUDA(cudaMemcpy(dk.p, kidx.data(), sizeof(int32_t) * npair, cudaMemcpyHostToDevice));
+        for (int u = 0; u < N->n_spec; u++) {
+            MDP_CUDA(cudaMemcpy(dT.p, N->h_Tuniq.data() + (size_t) u * N->lambda, sizeof(double) * N->lambda,
+                                cudaMemcpyHostToDevice));
+            spectrum_kernel<<<grid_for(M + 1, 128, 4096), 128, 0, ctx->stream>>>(dT.as<double>(), N->lambda, Nn,
+                                                                                tw64.as<double2>(), dH.as<double>());
+            MDP_CHECK_LAUNCH(ctx);
+            split_pairs_kernel<T><<<grid_for(npair, 256, 1024), 256, 0, ctx->stream>>>(
+                    dH.as<double>(), M, dk.as<int32_t>(), npair, P.spectra.as<V>() + (size_t) u * npair);
+            MDP_CHECK_LAUNCH(ctx);
+            MDP_CUDA(cudaStreamSynchronize(ctx->stream));
+        }
+    } else {
+        MDP_CUDA(cudaMemset(P.spectra.p, 0, sizeof(V) * (size_t) N->n_spec * npair));
+    }
+    constexpr int CW = SplitShape<T>::CW, RP = SplitShape<T>::RP;
+    const size_t  sc = split_cols_smem<V>(P.log_m1, P.log_m2, CW), sr = split_rows_smem<V>(P.log_m1, P.log_m2, RP);
+    for (const void *fn : {pick_cols<T, false>(P.log_m1), pick_cols<T, true>(P.log_m1)}) {
+        if (!fn) return MDP_EUNSUPPORTED;
+        MDP_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sc));
+    }
+    const void *fr = pick_rows<T>(P.log_m2);
+    if (!fr) return MDP_EUNSUPPORTED;
+    MDP_CUDA(cudaFuncSetAttribute(fr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sr));
+    return MDP_OK;
+}
+
+template <typename T>
+static int launch_split(mdp_context *ctx, const mdp_noise *N, const mdp_tile_plan &P, const T *d_in, T *d_out,
+                        const double *d_means, int ncols, int64_t col_stride, const int *d_active) {
+    using V = typename CT<T>::V;
+    constexpr int CW = SplitShape<T>::CW, RP = SplitShape<T>::RP;
+    const int     M1 = 1 << P.log_m1, M2 = 1 << P.log_m2;
+    const int64_t gc = P.n_tiles * (M2 / CW), gr = P.n_tiles * (M1 / 2 / RP);
+    if (gc > 0x7fffffffLL || gr > 0x7fffffffLL) return MDP_EUNSUPPORTED;
+    const int    tc = split_nt(CW * M1), tr = split_nt(2 * RP * M2);  // the kernels' compile-time thread counts
+    const size_t sc = split_cols_smem<V>(P.log_m1, P.log_m2, CW), sr = split_rows_smem<V>(P.log_m1, P.log_m2, RP);
+    // the columns of a batch share the scratch array: one column after the other
+    for (int c = 0; c < ncols; c++) {
+        SplitArgsT<T> a;
+        a.vin = d_in + (int64_t) c * col_stride;
+        a.vout = d_out + (int64_t) c * col_stride;
+        a.Y = P.scratch.as<V>();
+        a.tile_start = P.tile_start.as<int64_t>();
+        a.tile_block = P.tile_block.as<int32_t>();
+        a.blk_start = N->blk_start.as<int64_t>();
+        a.blk_len = N->blk_len.as<int32_t>();
+        a.blk_spec = N->blk_spec.as<int32_t>();
+        a.hpair = P.spectra.as<V>();
+        a.ttw = P.ttw.as<V>();
+        a.ltw1 = P.ltw.as<V>();
+        a.ltw2 = P.ltw2.as<V>();
+        a.wa = P.wa.as<V>();
+        a.wb = P.wb.as<V>();
+        a.means = d_means ? d_means + (int64_t) c * N->nb : nullptr;
+        a.lambda = N->lambda;
+        a.nb = N->nb;
+        a.col_stride = 0;
+        a.active = d_active ? d_active + c : nullptr;
+        a.log_m1 = P.log_m1;
+        a.log_m2 = P.log_m2;
+        void *args[] = {&a};
+        MDP_CUDA(cudaLaunchKernel(pick_cols<T, false>(P.log_m1), dim3((unsigned) gc), dim3(tc), args, sc, ctx->stream));
+        MDP_CHECK_LAUNCH(ctx);
+        MDP_CUDA(cudaLaunchKernel(pick_rows<T>(P.log_m2), dim3((unsigned) gr), dim3(tr), args, sr, ctx->stream));
+        MDP_CHECK_LAUNCH(ctx);
+        MDP_CUDA(cudaLaunchKernel(pick_cols<T, true>(P.log_m1), dim3((unsigned) gc), dim3(tc), args, sc, ctx->stream));
+        MDP_CHECK_LAUNCH(ctx);
+    }
+    return MDP_OK;
+}
+
 // Builds a tile plan: the tile table over the operator's blocks, the twiddle
 // tables and (spectra = true) the spectrum pairs of every distinct block row.
 template <typename T>
 static int build_plan(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, const TileCand &c, bool spectra) {
     using V = typename CT<T>::V;
+    P.split = c.split;
+    P.log_m1 = c.log_m1;
+    P.log_m2 = c.log_m2;
     P.log2_ml = c.log_ml;
     P.cluster = c.C;
     P.threads = c.threads;
-    const int M = c.C << c.log_ml;
+    const int M = (int) (cand_N(c) / 2);
     P.fft_n = 2 * M;
     const int64_t        E = (int64_t) P.fft_n - 2LL * (N->lambda - 1);
     std::vector<int64_t> ts;
@@ -755,7 +1288,7 @@ static int build_plan(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, const Ti
             tb.push_back(b);
         }
     P.n_tiles = (int64_t) ts.size();
-    if (P.n_tiles * P.cluster > 0x7fffffffLL) {
+    if (P.n_tiles * std::max(P.cluster, 1) > 0x7fffffffLL) {
         mdp_set_error("noise operator: %lld tiles exceed one launch", (long long) P.n_tiles);
         return MDP_EUNSUPPORTED;
     }
@@ -764,6 +1297,13 @@ static int build_plan(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, const Ti
     if (!ts.empty()) {
         MDP_CUDA(cudaMemcpy(P.tile_start.p, ts.data(), 8 * ts.size(), cudaMemcpyHostToDevice));
         MDP_CUDA(cudaMemcpy(P.tile_block.p, tb.data(), 4 * tb.size(), cudaMemcpyHostToDevice));
+    }
+    if (c.split) {
+        P.cluster = 0;
+        P.threads = 0;
+        MDP_TRY(build_split_tables<T>(ctx, N, P, spectra));
+        P.ready = 1;
+        return MDP_OK;
     }
     MDP_TRY(build_tile_twiddles<V>(c.log_ml, c.C, P.ltw, P.twm, P.ttw));
     const int64_t npair = (int64_t) M / 2 + 1;
@@ -808,6 +1348,7 @@ static int launch_tiles(mdp_context *ctx, const mdp_noise *N, const mdp_tile_pla
     using V = typename CT<T>::V;
     if (P.n_tiles == 0 || ncols < 1) return MDP_OK;
     if (ncols > 65535) return MDP_EUNSUPPORTED;
+    if (P.split) return launch_split<T>(ctx, N, P, d_in, d_out, d_means, ncols, col_stride, d_active);
     TileArgsT<T> a;
     a.vin = d_in;
     a.vout = d_out;
@@ -1180,7 +1721,7 @@ extern "C" int mdp_noise_tile_fp32(mdp_context *ctx, mdp_noise *N, int *fft_size
 }
 
 extern "C" int mdp_noise_plan(mdp_context *ctx, mdp_noise *N, int fp32, int *log2_cta_points, int *cluster_ctas,
-                              int *threads, int *tuned) {
+                              int *threads, int *tuned, int *split_log_m1, int *split_log_m2) {
     if (!ctx || !N) return MDP_EINVAL;
     MDP_CUDA(cudaSetDevice(ctx->device));
     if (fp32) MDP_TRY(mdp_noise_prepare_fp32(ctx, N));
@@ -1189,6 +1730,8 @@ extern "C" int mdp_noise_plan(mdp_context *ctx, mdp_noise *N, int fp32, int *log
     if (cluster_ctas) *cluster_ctas = P.cluster;
     if (threads) *threads = P.threads;
     if (tuned) *tuned = P.tuned;
+    if (split_log_m1) *split_log_m1 = P.split ? P.log_m1 : 0;
+    if (split_log_m2) *split_log_m2 = P.split ? P.log_m2 : 0;
     return MDP_OK;
 }
 

@@ -107,3 +107,45 @@ def test_stbmm_rejects_band_wider_than_block(gpu_ctx):
     import midapack_b200 as mb
     with pytest.raises(mb.MidapackError):
         mb.Noise(gpu_ctx, [10], 64, np.ones(64))
+
+
+@pytest.mark.parametrize("lam,sizes,plan", [
+    (16, [1000, 333], "s,4,5"),              # smallest split tile: 16 x 32 points
+    (64, [4096, 777, 130], "s,5,5"),          # ragged blocks, one shorter than a tile
+    (300, [5000, 600], "s,5,6"),              # lambda not a power of two
+    (2048, [20000, 4100], "s,6,8"),
+    (4096, [40000, 9000], "s,7,8"),
+    (8192, [70000], "s,8,8"),
+    (16384, [140000, 3 * 16384], "s,8,9"),    # largest split tile: 256 x 512 points
+])
+def test_stbmm_split_plan_vs_exact(gpu_ctx, lam, sizes, plan):
+    """The three-kernel (four-step FFT) tile plan, FP64 and FP32."""
+    import torch
+    import midapack_b200 as mb
+    rng = np.random.default_rng(lam + 7)
+    t = np.zeros(lam)
+    t[0] = 2.0
+    t[1:] = rng.standard_normal(lam - 1) * np.exp(-np.arange(1, lam) / (0.3 * lam))
+    invtt = np.tile(t, len(sizes))
+    v = rng.standard_normal(int(sum(sizes))) + 3.0
+    os.environ["MDP_TOEPLITZ_PLAN"] = plan
+    os.environ["MDP_TOEPLITZ_PLAN32"] = plan
+    try:
+        N = mb.Noise(gpu_ctx, sizes, lam, invtt)
+        tile, tile32 = N.tile(), N.tile_fp32()
+    finally:
+        del os.environ["MDP_TOEPLITZ_PLAN"]
+        del os.environ["MDP_TOEPLITZ_PLAN32"]
+    m1, m2 = (int(x) for x in plan.split(",")[1:])
+    assert tile["split"] == [1 << m1, 1 << m2] and tile32["split"] == [1 << m1, 1 << m2]
+    vin = torch.from_numpy(v).cuda()
+    vout = torch.empty_like(vin)
+    N.apply(vin, vout)
+    v32 = vin.float()
+    o32 = torch.empty_like(v32)
+    N.apply_fp32(v32, o32)
+    torch.cuda.synchronize()
+    ref = R.stbmm(v, np.array(sizes), lam, invtt, exact=True)
+    assert _rel(vout.cpu().numpy(), ref) < TOL
+    ref32 = R.stbmm(v32.double().cpu().numpy(), np.array(sizes), lam, invtt, exact=True)
+    assert _rel(o32.double().cpu().numpy(), ref32) < 1e-5
