@@ -1,12 +1,19 @@
-"""Time-to-map benchmark: the FP64 GLS map-making solve on one B200.
+"""Time-to-map benchmark of the GLS map-making solve on one B200: mixed
+precision vs plain FP64, multi-RHS, and served latency.
 
-Workload (synthetic, seeded; no public dataset is involved): 64 detectors x
-2^24 samples (1.07e9 samples) on a 2048x1536 flat grid (3.1M pixels, 9.4M
-I/Q/U unknowns), 2^20-sample stationary intervals (1024 Toeplitz blocks,
-lambda = 2^14), 1% flagged samples, int32 pointing, FP64 weights and TOD.
-One step = one complete map-making solve from device-resident inputs:
-pointing compression (MatInit), inverse-noise spectra, block-Jacobi build with
-the rcond cut, PCG to relative residual 1e-8 (the reference's criterion).
+Headline (value): the at-scale workload, synthetic and seeded (no public
+dataset is involved): 64 detectors x 2^24 samples (1.07e9 samples) on a
+2048x1536 flat grid (3.1M pixels, 9.4M I/Q/U unknowns), 2^20-sample stationary
+intervals (1024 Toeplitz blocks, lambda = 2^14), 1% flagged samples, int32
+pointing, FP64 weights and TOD.  One step = one complete map-making solve from
+device-resident inputs: pointing compression (MatInit), inverse-noise spectra
+and tile plans, block-Jacobi build with the rcond cut, PCG to relative
+residual 1e-8 (the reference's criterion); value = mixed precision,
+config.fp64 = the plain FP64 path.  Further keys on the same line: e2e (the
+MLmap solve from host buffers), cpu_baseline (the reference's C operator on
+the host cores, extrapolated), mixed_fknee_sweep (CPU-runnable workload,
+f_knee 0.1/1/5 Hz), multi_rhs (128 right-hand sides sharing one pointing),
+serving (Poisson stream of independent solves, p50/p99 latency).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -52,8 +59,9 @@ def parse():
     ap.add_argument("--no-compare", action="store_true", help="skip timing the other precision")
     ap.add_argument("--no-multi", action="store_true", help="skip the multi-RHS part")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving part")
-    ap.add_argument("--only", default="", choices=["", "multi", "serve"],
-                    help="run only the multi-RHS or only the serving part (prints their JSON)")
+    ap.add_argument("--no-fknee", action="store_true", help="skip the f_knee sweep part")
+    ap.add_argument("--only", default="", choices=["", "multi", "serve", "fknee"],
+                    help="run only the multi-RHS, serving or f_knee part (prints their JSON)")
     ap.add_argument("--multi-rhs", type=int, default=128, help="right-hand sides of the multi-RHS part")
     ap.add_argument("--multi-fp64-cols", type=int, default=2, help="columns timed with the plain FP64 path")
     ap.add_argument("--serve-requests", type=int, default=256)
@@ -231,6 +239,53 @@ def bench_multi(args, device):
     return out
 
 
+def bench_fknee(args, device):
+    """Mixed-precision configuration on the CPU-runnable workload (4 det x 2^20
+    samples, 256x192 px, lambda 2^12) with f_knee in {0.1, 1, 5} Hz: mixed and
+    plain FP64 time-to-map at 1e-8 and each map's I/Q/U error against the FP64
+    oracle (plain FP64 path at tol 1e-12).  1% flagged samples: without them the
+    operator of this workload is singular (constant offset) and neither path
+    reaches 1e-8."""
+    import torch
+    import midapack_b200 as mb
+    from midapack_b200 import synth
+    base = dict(synth.CONFIGS["c1_4det_2p20_256x192_lam4096"])
+    ctx = mb.Context(device)
+    out = {"workload": "c1_4det_2p20_256x192_lam4096 + 1% flagged samples", "tol": TOL}
+    for fk in (0.1, 1.0, 5.0):
+        cfg = dict(base, fknee=fk, gap_frac=0.01)
+        wl = synth.make_workload_torch("c3", **cfg)
+        m = wl.n_samples
+        res = {}
+        for prec, fn, tol in (("oracle", mb.gls_solve, 1e-12), ("fp64", mb.gls_solve, TOL),
+                              ("mixed", mb.gls_solve_mixed, TOL)):
+            ts = []
+            for rep in range(1 if prec == "oracle" else 3):
+                P = mb.Pointing(ctx, wl.pix, wl.weights, m, 3)
+                N = mb.Noise(ctx, wl.block_sizes, wl.lam, wl.invtt)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                o = fn(ctx, P, N, wl.signal, wl.noise, tol=tol, maxiter=4 * MAXITER)
+                torch.cuda.synchronize()
+                ts.append(time.perf_counter() - t0)
+            res[prec] = (o[0].cpu().numpy(), o[5], min(ts))
+        xo = res["oracle"][0]
+        entry = {}
+        for prec in ("fp64", "mixed"):
+            x, info, t = res[prec]
+            entry[prec] = {"time_to_map_s": round(t, 4), "iterations": info.iterations,
+                           "converged": bool(info.converged),
+                           "map_rel_err_vs_fp64_oracle": {
+                               name: float(np.linalg.norm(x[k::3] - xo[k::3]) / np.linalg.norm(xo[k::3]))
+                               for k, name in enumerate("IQU")}}
+        entry["oracle_iterations"] = res["oracle"][1].iterations
+        out[f"fknee_{fk:g}"] = entry
+        del wl, res
+    ctx.close()
+    torch.cuda.empty_cache()
+    return out
+
+
 def bench_serving(args, device):
     """Serving configuration: Poisson arrivals (args.serve_rate per second) of
     independent solves on args.serve_datasets resident datasets drawn
@@ -300,7 +355,7 @@ def main():
         return 0
     torch.cuda.set_device(local)
     if args.only:
-        r = bench_multi(args, local) if args.only == "multi" else bench_serving(args, local)
+        r = {"multi": bench_multi, "serve": bench_serving, "fknee": bench_fknee}[args.only](args, local)
         print(json.dumps({args.only: r}), flush=True)
         return 0
     if world > 1:
@@ -434,7 +489,10 @@ def main():
     pinned = None
 
     # multi-RHS and serving configurations (one GPU: rank 0 of a single-process run)
-    multi = serve_out = None
+    multi = serve_out = fknee = None
+    ctx.trim()
+    if world == 1 and not args.no_fknee:
+        fknee = bench_fknee(args, local)
     if world == 1 and not args.no_multi:
         multi = bench_multi(args, local)
     if world == 1 and not args.no_serve:
@@ -463,6 +521,8 @@ def main():
             line["e2e"] = e2e
         if cpu:
             line["cpu_baseline"] = cpu
+        if fknee:
+            line["mixed_fknee_sweep"] = fknee
         if multi:
             line["multi_rhs"] = multi
         if serve_out:
