@@ -137,6 +137,20 @@ def algorithmic_bytes32(ns: int, n_map: int, t32):
     }
 
 
+# DRAM bytes per tile of one N^-1 application, measured with ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum of the three split kernels over
+# 704 tiles, lambda 2^14, 2^20-sample blocks; see profiles/), keyed by
+# (precision, M1, M2); scaled to a launch by the tile count
+NINV_TRAFFIC_PER_TILE = {("f32", 256, 256): 1857072128 / 704}
+
+
+def ninv_kernel(t: dict, prec: str) -> str:
+    if t.get("split"):
+        m1, m2 = t["split"]
+        return f"split_cols_kernel + split_rows_kernel + split_cols_kernel<{prec}> ({m1}x{m2} four-step tiles)"
+    return f"toeplitz_tile_kernel<{prec}, {int(np.log2(t['cta_points']))}, {t['cluster']}>"
+
+
 def cpu_reference(wl_host, iterations: int, sample_dets: int, full_samples: int, cores: int):
     """Reference C operator (oracle/_ref) on host cores: one P^T N^-1 P application
     over `sample_dets` detectors (one per forked rank, in a fresh process that
@@ -452,19 +466,26 @@ def main():
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     achieved = ab[dom] / (per[dom] * 1e-3) / 1e9
-    kname = {"P": "matvec_chunk_sums_kernel", "Ninv": "toeplitz_tile_kernel<double,13,8>",
+    kname = {"P": "matvec_chunk_sums_kernel", "Ninv": ninv_kernel(tile, "double"),
              "Pt": "trmatvec_binned_kernel"}
+    ninv_tile, ninv_prec = tile, "f64"
     if args.precision == "mixed":
         t32 = N.tile_fp32()
         ab = algorithmic_bytes32(ns, n_map, (t32["n_tiles"], t32["fft_n"] // 2))
         tile = {"fp64": tile, "fp32": t32}
-        kname = {"P": "matvec32_chunk_sums_kernel", "Ninv": "toeplitz_tile_kernel<float,...> (FP32)",
+        kname = {"P": "matvec32_chunk_sums_kernel", "Ninv": ninv_kernel(t32, "float"),
                  "Pt": "trmatvec32_binned_kernel"}
+        ninv_tile, ninv_prec = t32, "f32"
         dom = max(("P", "Ninv", "Pt"), key=lambda k: per[k])
         achieved = ab[dom] / (per[dom] * 1e-3) / 1e9
+    traffic = None
+    if dom == "Ninv" and ninv_tile.get("split"):
+        tpt = NINV_TRAFFIC_PER_TILE.get((ninv_prec, *ninv_tile["split"]))
+        if tpt:
+            traffic = int(tpt * ninv_tile["n_tiles"])
     roofline = {"bound": "hbm", "kernel": kname[dom],
                 "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
-                "traffic": None, "peak_source": "measured" if peaks else "fallback",
+                "traffic": traffic, "peak_source": "measured" if peaks else "fallback",
                 "per_application_ms": {k: round(v, 4) for k, v in per.items()},
                 "algorithmic_bytes": ab}
 
