@@ -455,6 +455,38 @@ __device__ __forceinline__ void seq_fft(V *s, int nseq, const V *stw) {
     }
 }
 
+// the passes of seq_fft but the innermost one (group size 2^(LOG_L - 4(NP-1)),
+// sets of consecutive positions): DIF passes 0..NP-2, or the DIT passes
+// NP-2..0 that follow an innermost pass done by the caller
+template <typename V, int LOG_L, bool INVERSE>
+__device__ __forceinline__ void seq_fft_outer(V *s, int nseq, const V *stw) {
+    constexpr int NP = ltw_passes(LOG_L);
+    constexpr int L = 1 << LOG_L;
+#pragma unroll
+    for (int pi = 0; pi < NP - 1; pi++) {
+        const int p = INVERSE ? (NP - 2 - pi) : pi;
+        const int logG = LOG_L - 4 * p;  // >= 5: radix-16 passes only
+        const int G = 1 << logG;
+        seq_pass<V, 16, L, INVERSE>(s, nseq, G, stw + ltw_offset(LOG_L, p));
+    }
+}
+
+// real-FFT untangle, product with the real even spectrum, re-tangle of one
+// pair (Z1 = Z[k], Z2 = Z[M-k]); hc = ((H[k]+H[M-k])/2, (H[k]-H[M-k])/2), wk = W_N^k
+template <typename V, typename T>
+__device__ __forceinline__ void twist_pair(V &Z1, V &Z2, V hc, V wk) {
+    const T half = (T) 0.5;
+    const V E0 = mkv(Z1, half * (Z1.x + Z2.x), half * (Z1.y - Z2.y));
+    const V O0 = mkv(Z1, half * (Z1.y + Z2.y), -half * (Z1.x - Z2.x));
+    const T ca = hc.x, cb = hc.y;
+    const V wO = cmul(wk, O0);
+    const V Ep = mkv(Z1, ca * E0.x + cb * wO.x, ca * E0.y + cb * wO.y);
+    const V cE = cmulc(E0, wk);
+    const V Op = mkv(Z1, cb * cE.x + ca * O0.x, cb * cE.y + ca * O0.y);
+    Z1 = mkv(Z1, Ep.x - Op.y, Ep.y + Op.x);
+    Z2 = mkv(Z1, Ep.x + Op.y, -Ep.y + Op.x);
+}
+
 template <typename T>
 struct SplitArgsT {
     using V = typename CT<T>::V;
@@ -476,6 +508,8 @@ struct SplitArgsT {
     int64_t        col_stride;
     const int     *active;
     int            log_m1, log_m2;
+    int            E;           // outputs per tile
+    int            vec2;        // vin aligned to two samples: pair loads
 };
 
 template <typename V>
@@ -520,11 +554,14 @@ __global__ void __launch_bounds__(split_nt(CW << LOG_M1)) split_cols_kernel(Spli
     const int64_t bs = a.blk_start[blk];
     const int64_t be = bs + a.blk_len[blk];
     const int64_t t0 = a.tile_start[tile];
-    const int64_t ws = t0 - (a.lambda - 1);
+    // the window starts on an even row (split tiles keep one output fewer
+    // than the band allows, so the window can move down by one)
+    const int64_t ws = (t0 - (a.lambda - 1)) & ~(int64_t) 1;
     // all loads of a thread are issued before its shared-memory stores
     if (!INV) {
         const T mu = a.means ? (T) a.means[blk] : (T) 0;
-        // element (j1, c): samples ws + 2(M2 j1 + c0 + c) + {0, 1}
+        // element (j1, c): samples ws + 2(M2 j1 + c0 + c) + {0, 1}, one aligned
+        // pair load where both lie in the block
         T x0[EPT], x1[EPT];
 #pragma unroll
         for (int u = 0; u < EPT; u++) {
@@ -532,8 +569,14 @@ __global__ void __launch_bounds__(split_nt(CW << LOG_M1)) split_cols_kernel(Spli
             const int     c = e % CW, j1 = e / CW;
             const int64_t row = ws + 2 * ((int64_t) M2 * j1 + c0 + c);
             const bool    ok = e < CW * M1;
-            x0[u] = (ok && row >= bs && row < be) ? __ldg(a.vin + row) - mu : (T) 0;
-            x1[u] = (ok && row + 1 >= bs && row + 1 < be) ? __ldg(a.vin + row + 1) - mu : (T) 0;
+            if (a.vec2 && ok && row >= bs && row + 1 < be) {
+                const V z = __ldg(reinterpret_cast<const V *>(a.vin + row));
+                x0[u] = z.x - mu;
+                x1[u] = z.y - mu;
+            } else {
+                x0[u] = (ok && row >= bs && row < be) ? __ldg(a.vin + row) - mu : (T) 0;
+                x1[u] = (ok && row + 1 >= bs && row + 1 < be) ? __ldg(a.vin + row + 1) - mu : (T) 0;
+            }
         }
 #pragma unroll
         for (int u = 0; u < EPT; u++) {
@@ -567,8 +610,7 @@ __global__ void __launch_bounds__(split_nt(CW << LOG_M1)) split_cols_kernel(Spli
         }
     } else {
         // position p holds j1 = rev(p): z'[M2 j1 + j2] = conj(value) / M, samples 2(M2 j1 + j2) + {0, 1}
-        const int     E = 2 * M - 2 * (a.lambda - 1);
-        const int64_t out_end = min(t0 + (int64_t) E, be);
+        const int64_t out_end = min(t0 + (int64_t) a.E, be);
         const T       scale = (T) 1 / (T) M;
         for (int e = threadIdx.x; e < CW * M1; e += blockDim.x) {
             const int     c = e % CW, p = e / CW;
@@ -626,6 +668,53 @@ __global__ void __launch_bounds__(split_nt(2 * RP << LOG_M2)) split_rows_kernel(
         }
     }
     __syncthreads();
+    constexpr int RL_ = 1 << (LOG_M2 - 4 * (ltw_passes(LOG_M2) - 1));
+    if (RL_ <= 4 && rp0 > 0) {
+        // Rows k1 and M1-k1: the innermost forward pass works on sets of RL
+        // consecutive positions, and position p of row A pairs with position
+        // M2-1-p of row B, so set g of row A pairs element i <-> RL-1-i with
+        // set NSET-1-g of row B.  That pass, the spectrum product of the pairs
+        // and the first inverse pass run on the two sets in registers: one
+        // shared-memory round trip instead of three (for small innermost
+        // passes; with radix-16 sets the per-thread work is too long and the
+        // three separate passes are faster).
+        constexpr int NP = ltw_passes(LOG_M2);
+        constexpr int RL = 1 << (LOG_M2 - 4 * (NP - 1));
+        constexpr int NSET = M2 / RL;
+        seq_fft_outer<V, LOG_M2, false>(s, 2 * RP, stw);
+        const V one = mkv(V{}, (T) 1, (T) 0);
+        for (int it = threadIdx.x; it < RP * NSET; it += blockDim.x) {
+            const int rl = it / NSET, g = it - rl * NSET, gb = NSET - 1 - g;
+            V         va[RL], vb[RL];
+#pragma unroll
+            for (int i = 0; i < RL; i++) {
+                va[i] = s[sq_idx<M2>(2 * rl, g * RL + i)];
+                vb[i] = s[sq_idx<M2>(2 * rl + 1, gb * RL + i)];
+            }
+            dif_set<V, RL>(va, one);
+            dif_set<V, RL>(vb, one);
+            const int pr0 = (M2 + 1) + (rp0 + rl - 1) * M2 + g * RL;
+#pragma unroll
+            for (int i = 0; i < RL; i++)
+                twist_pair<V, T>(va[i], vb[RL - 1 - i], __ldg(HP + pr0 + i), __ldg(a.ttw + pr0 + i));
+            dit_set<V, RL>(va, one);
+            dit_set<V, RL>(vb, one);
+#pragma unroll
+            for (int i = 0; i < RL; i++) {
+                s[sq_idx<M2>(2 * rl, g * RL + i)] = va[i];
+                s[sq_idx<M2>(2 * rl + 1, gb * RL + i)] = vb[i];
+            }
+        }
+        __syncthreads();
+        seq_fft_outer<V, LOG_M2, true>(s, 2 * RP, stw);
+        for (int e = threadIdx.x; e < 2 * RP * M2; e += blockDim.x) {
+            const int r = e / M2, j2 = e % M2;
+            const int k1 = row_of(r);
+            const V   v = s[sq_idx<M2>(r, j2)];
+            Y[(int64_t) k1 * M2 + j2] = cmulc(v, split_tw(swa, swb, (int) (((int64_t) j2 * k1) & (M - 1))));
+        }
+        return;
+    }
     seq_fft<V, LOG_M2, false>(s, 2 * RP, stw);
     // pairs (k, M-k): position p of row A with position M2-1-p of row B, or
     // inside rows 0 and M1/2 for rp = 0 (table entries in the same order)
@@ -910,7 +999,7 @@ static std::vector<TileCand> tile_candidates(int lambda) {
     for (int logM = 9; logM <= 17; logM++)
         for (auto ab : split_shapes(logM, SplitShape<T>::M1MAX)) {
             TileCand c{0, 0, 0, 1, ab.first, ab.second};
-            if (cand_N(c) - 2LL * (lambda - 1) < 1) continue;
+            if (cand_N(c) - 2LL * (lambda - 1) - 1 < 1) continue;
             out.push_back(c);
         }
     return out;
@@ -1262,6 +1351,8 @@ static int launch_split(mdp_context *ctx, const mdp_noise *N, const mdp_tile_pla
         a.active = d_active ? d_active + c : nullptr;
         a.log_m1 = P.log_m1;
         a.log_m2 = P.log_m2;
+        a.E = P.fft_n - 2 * (N->lambda - 1) - 1;
+        a.vec2 = reinterpret_cast<uintptr_t>(a.vin) % (2 * sizeof(T)) == 0;
         void *args[] = {&a};
         MDP_CUDA(cudaLaunchKernel(pick_cols<T, false>(P.log_m1), dim3((unsigned) gc), dim3(tc), args, sc, ctx->stream));
         MDP_CHECK_LAUNCH(ctx);
@@ -1286,7 +1377,9 @@ static int build_plan(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, const Ti
     P.threads = c.threads;
     const int M = (int) (cand_N(c) / 2);
     P.fft_n = 2 * M;
-    const int64_t        E = (int64_t) P.fft_n - 2LL * (N->lambda - 1);
+    // split tiles: one output fewer, so that every window can start on an even row
+    const int64_t        E = (int64_t) P.fft_n - 2LL * (N->lambda - 1) - (c.split ? 1 : 0);
+    if (E < 1) return MDP_EUNSUPPORTED;
     std::vector<int64_t> ts;
     std::vector<int32_t> tb;
     for (int b = 0; b < N->nb; b++)
