@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=50.0, help="mean Poisson arrival rate, solves/s")
     ap.add_argument("--serve-datasets", type=int, default=16)
     ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--replicas", action="store_true",
+                    help="with N > 1 ranks: N independent solves instead of one solve sharded over the ranks")
     return ap.parse_args()
 
 
@@ -367,6 +369,7 @@ def main():
     import torch
     if args.impl == "reference" and rank != 0:
         return 0
+    local = local % max(torch.cuda.device_count(), 1)
     torch.cuda.set_device(local)
     if args.only:
         r = {"multi": bench_multi, "serve": bench_serving, "fknee": bench_fknee}[args.only](args, local)
@@ -375,7 +378,9 @@ def main():
     if world > 1:
         import torch.distributed as dist
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        # MDP_BENCH_BACKEND=gloo runs the ranks' exchanges through host memory
+        # (a functional check of the sharded path with several ranks on one GPU)
+        dist.init_process_group(os.environ.get("MDP_BENCH_BACKEND", "nccl"), timeout=timedelta(seconds=600))
 
     import midapack_b200 as mb
     from midapack_b200 import synth
@@ -400,6 +405,8 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args, wl, ctx, one_solve)
+    if world > 1 and not args.replicas:
+        return run_sharded(args, wl, ctx, rank, world, local, idv)
 
     for _ in range(args.warmup):
         one_solve()
@@ -611,6 +618,108 @@ def run_cpu_baseline(wl, sample, iterations, ns):
                        f"as {sample_dets} forked ranks: {r['op_seconds_sample']:.2f} s per application; "
                        f"extrapolated x{ns // (per_det * sample_dets)} samples x {iterations + 1} applications on "
                        f"{sample_dets} cores")}
+
+
+def run_sharded(args, wl, ctx, rank, world, local, idv):
+    """One solve sharded over the ranks (midapack_b200.dist): each rank holds
+    64 detectors x 2^24 samples (its own seeded scan of the same 2048x1536
+    sky), one map-sized all-reduce per operator application; weak scaling (the
+    job grows with the ranks).  Time per step = max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from midapack_b200.dist import GpuShard, ShardedGLS
+    ns = wl.n_samples
+
+    def one(precision):
+        shard = GpuShard(ctx, wl.pix, wl.weights, wl.signal, wl.noise, wl.block_sizes, wl.lam, wl.invtt, idv=idv)
+        out = ShardedGLS(shard).solve(tol=TOL, maxiter=MAXITER, precision=precision, inner_tol=args.inner_tol)
+        return shard, out
+
+    def timed(precision, steps):
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stream = torch.cuda.current_stream()
+        e0.record(stream)
+        last = None
+        for _ in range(steps):
+            shard, out = one(precision)
+            shard.close()
+            last = out
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1) / steps], dtype=torch.float64,
+                         device="cuda" if dist.get_backend() == "nccl" else "cpu")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t), last
+
+    for _ in range(args.warmup):
+        shard, _ = one(args.precision)
+        shard.close()
+    launches0 = ctx.launches
+    clocks = Clocks(local)
+    ms, out = timed(args.precision, args.steps)
+    clk = clocks.stop()
+    launches = ctx.launches - launches0
+    info = out[4]
+    other = None
+    if not args.no_compare:
+        oprec = "fp64" if args.precision == "mixed" else "mixed"
+        oms, oout = timed(oprec, args.steps)
+        other = {"precision": oprec, "time_to_map_s": round(oms / 1e3, 4), "iterations": oout[4].iterations,
+                 "outer_iterations": oout[4].outer_iterations, "converged": bool(oout[4].converged)}
+    # roofline: this rank's share of one operator application (P, N^-1, P^T), timed alone
+    shard = GpuShard(ctx, wl.pix, wl.weights, wl.signal, wl.noise, wl.block_sizes, wl.lam, wl.invtt, idv=idv)
+    n_loc = shard.P.shape()["n_map"]
+    h = torch.randn(n_loc, dtype=torch.float64, device="cuda")
+    fp32 = args.precision == "mixed"
+    for _ in range(2):
+        shard.apply(h, fp32)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        shard.apply(h, fp32)
+    e1.record()
+    torch.cuda.synchronize()
+    op_ms = e0.elapsed_time(e1) / 3
+    t = shard.N.tile_fp32() if fp32 else shard.N.tile()
+    ab = (algorithmic_bytes32(ns, n_loc, (t["n_tiles"], t["fft_n"] // 2)) if fp32
+          else algorithmic_bytes(ns, n_loc, t["n_tiles"], t["fft_n"] // 2))
+    shard.close()
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = sum(ab.values()) / (op_ms * 1e-3) / 1e9
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(ms / 1e3, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 2), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 operator + f64 refinement" if fp32 else "f64",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": f"{args.config} per rank, sharded over {world} ranks", "samples": ns * world,
+                       "detectors": wl.n_det * world, "pixels": wl.npix, "unknowns": int(info.n_map),
+                       "lambda": wl.lam, "tol": TOL, "precision": args.precision, "iterations": info.iterations,
+                       "outer_iterations": info.outer_iterations, "converged": bool(info.converged),
+                       "l2": "inputs (tens of GB per rank) far larger than L2",
+                       "parallelism": f"one solve sharded over {world} ranks (detectors per rank), one map "
+                                      f"all-reduce per operator application ({dist.get_backend()})"},
+            "roofline": {"bound": "hbm", "kernel": "P^T N^-1 P, one rank's application "
+                                                  f"({'FP32' if fp32 else 'FP64'} operator)",
+                         "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                         "frac": round(achieved / hbm, 4), "traffic": None,
+                         "peak_source": "measured" if peaks else "fallback", "per_application_ms": round(op_ms, 4)},
+            "clocks": clk, "gpu_launches": int(launches),
+        }
+        if other:
+            line["config"]["fp64" if other["precision"] == "fp64" else "mixed"] = other
+        print(json.dumps(line), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+    return 0
 
 
 def run_reference(args, wl, ctx, one_solve):

@@ -220,6 +220,31 @@ int mdp_gls_solve_multi(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, i
                         const mdp_multi_params *params, double *d_x, int32_t *d_lstid, double *d_cond,
                         int32_t *d_hits, mdp_multi_col_info *col_info, mdp_multi_info *info);
 
+/* ---- Pieces of a solve sharded over ranks (no counterpart in the reference,
+ * whose ranks exchange through MPI inside precondblockjacobilike and
+ * PCG_GLS_true).  Each rank holds the samples of some detectors/intervals;
+ * the caller sums the blocks and the maps over ranks.  npix below is the
+ * pointing's current pixel count, n_map/3 of mdp_pointing_shape. */
+/* getlocalW (precond.c:42-161) on this rank's samples: d_W [npix][9]
+ * (upper triangle and diagonal filled) and d_hits [npix], zeroed first. */
+int  mdp_local_blocks(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, double *d_W, int32_t *d_hits);
+/* Per 3x3 block (summed over ranks): rcond (LAPACK dgecon 1-norm estimate), the
+ * inverse when rcond > 0.1, otherwise a zero block and d_cut[q] = 1
+ * (precond.c:456-702).  d_W is symmetrised in place. */
+int  mdp_block_inverse(mdp_context *ctx, int64_t npix, double *d_W, double *d_inv, double *d_rcond, int32_t *d_cut,
+                       int64_t *n_cut);
+/* The samples of every pixel q with d_target[q] != 0 become cut rows (weights
+ * ignored, signal zeroed in residuals); the other pixels keep their order and
+ * are renumbered; *kept_pixels gets their count. */
+int  mdp_pointing_cut(mdp_context *ctx, mdp_pointing *A, const int32_t *d_target, int64_t *kept_pixels);
+/* d_r = P^T N^-1 (d - P x), d = signal (zero on cut rows) + noise; d_x may be
+ * NULL for x = 0.  FP64. */
+int  mdp_gls_residual(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *d_signal,
+                      const double *d_noise, const double *d_x, double *d_r);
+/* d_q = P^T N^-1 P d_h (maps FP64); fp32 = 1 runs the FP32 operator of the
+ * mixed-precision solver. */
+int  mdp_apply_op(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *d_h, double *d_q, int fp32);
+
 #ifdef __cplusplus
 }
 #endif

@@ -88,6 +88,13 @@ _SIGS = {
     "mdp_gls_solve_multi": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int,
                                        ct.c_int64, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                        ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mdp_local_blocks": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mdp_block_inverse": (ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                     ct.POINTER(ct.c_int64)]),
+    "mdp_pointing_cut": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.POINTER(ct.c_int64)]),
+    "mdp_gls_residual": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                    ct.c_void_p]),
+    "mdp_apply_op": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int]),
     "mdp_noise_plan": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_int, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int),
                                   ct.POINTER(ct.c_int), ct.POINTER(ct.c_int), ct.POINTER(ct.c_int),
                                   ct.POINTER(ct.c_int)]),

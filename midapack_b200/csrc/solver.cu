@@ -918,3 +918,145 @@ extern "C" int mdp_gls_solve_mixed(mdp_context *ctx, mdp_pointing *A, const mdp_
     }
     return MDP_OK;
 }
+
+// ================================================================= pieces of a sharded solve
+// A solve split over ranks (each rank holding the samples of some detectors
+// and stationary intervals) needs the per-rank parts of the steps above with
+// the exchanges between them done by the caller: the rank's 3x3 blocks (summed
+// over ranks), their inversion and rcond cut, the cut applied to the rank's
+// samples, the FP64 residual and one operator application per PCG iteration.
+
+extern "C" int mdp_local_blocks(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, double *d_W,
+                                int32_t *d_hits) {
+    if (!ctx || !A || !N || !d_W || !d_hits) return MDP_EINVAL;
+    if (!A->triplet) {
+        mdp_set_error("mdp_local_blocks: the (I,Q,U) triplet pointing layout is needed");
+        return MDP_EUNSUPPORTED;
+    }
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    const int64_t npix = A->n_map() / 3;
+    cudaStream_t  st = ctx->stream;
+    MDP_CUDA(cudaMemsetAsync(d_W, 0, 72 * npix, st));
+    MDP_CUDA(cudaMemsetAsync(d_hits, 0, 4 * npix, st));
+    localW_kernel<<<grid_for(A->m, 256, ctx->sm_count * 16), 256, 0, st>>>(
+            A->off.as<int32_t>(), A->values, A->m, N->blk_start.as<int64_t>(), N->blk_len.as<int32_t>(),
+            N->blk_t0.as<double>(), N->nb, d_W, d_hits);
+    MDP_CHECK_LAUNCH(ctx);
+    return MDP_OK;
+}
+
+extern "C" int mdp_block_inverse(mdp_context *ctx, int64_t npix, double *d_W, double *d_inv, double *d_rcond,
+                                 int32_t *d_cut, int64_t *n_cut) {
+    if (!ctx || npix < 0 || (npix > 0 && (!d_W || !d_inv || !d_rcond || !d_cut))) return MDP_EINVAL;
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    MDP_TRY(ctx->scratch2.alloc(sizeof(int)));
+    MDP_CUDA(cudaMemsetAsync(ctx->scratch2.p, 0, sizeof(int), st));
+    if (npix > 0) {
+        bj_pixel_kernel<<<grid_for(npix, 128, ctx->sm_count * 8), 128, 0, st>>>(d_W, npix, d_inv, d_rcond, d_cut,
+                                                                               ctx->scratch2.as<int>());
+        MDP_CHECK_LAUNCH(ctx);
+    }
+    int h = 0;
+    MDP_CUDA(cudaMemcpyAsync(&h, ctx->scratch2.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MDP_CUDA(cudaStreamSynchronize(st));
+    if (n_cut) *n_cut = h;
+    return MDP_OK;
+}
+
+extern "C" int mdp_pointing_cut(mdp_context *ctx, mdp_pointing *A, const int32_t *d_target, int64_t *kept_pixels) {
+    if (!ctx || !A || !d_target) return MDP_EINVAL;
+    if (!A->triplet) {
+        mdp_set_error("mdp_pointing_cut: the (I,Q,U) triplet pointing layout is needed");
+        return MDP_EUNSUPPORTED;
+    }
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t  st = ctx->stream;
+    const int64_t npix0 = A->n_map() / 3;
+    if (npix0 == 0) {
+        if (kept_pixels) *kept_pixels = 0;
+        return MDP_OK;
+    }
+    const uint32_t *target = reinterpret_cast<const uint32_t *>(d_target);  // 0 / 1 flags
+    DevBuf          remap, keep, lind2;
+    MDP_TRY(remap.alloc(4 * npix0));
+    MDP_TRY(keep.alloc(4 * npix0));
+    MDP_TRY(lind2.alloc(4 * (3 * npix0 + 3)));
+    const int gb = grid_for(npix0, 256, ctx->sm_count * 8);
+    invert_flags_kernel<<<gb, 256, 0, st>>>(target, keep.as<uint32_t>(), npix0);
+    MDP_CHECK_LAUNCH(ctx);
+    uint32_t kept = 0;
+    MDP_TRY(mdp_exclusive_scan_u32(ctx, keep.as<uint32_t>(), remap.as<uint32_t>(), npix0, &kept));
+    if (kept_pixels) *kept_pixels = kept;
+    if ((int64_t) kept == npix0) return MDP_OK;  // nothing to cut
+    rewrite_off_kernel<<<grid_for(A->m, 256, ctx->sm_count * 16), 256, 0, st>>>(A->off.as<int32_t>(), A->m, target,
+                                                                               remap.as<uint32_t>());
+    MDP_CHECK_LAUNCH(ctx);
+    new_lindices_kernel<<<gb, 256, 0, st>>>(A->lindices.as<int32_t>(), A->trash_pix, npix0, target,
+                                            remap.as<uint32_t>(), lind2.as<int32_t>());
+    MDP_CHECK_LAUNCH(ctx);
+    MDP_CUDA(cudaStreamSynchronize(st));
+    std::swap(A->lindices.p, lind2.p);
+    std::swap(A->lindices.bytes, lind2.bytes);
+    A->bins.valid = 0;
+    A->mbins.valid = 0;
+    A->trash_pix = 1;
+    A->lcount = 3 * (int64_t) kept + 3;
+    delete A->bj_cache;  // built for the old numbering
+    A->bj_cache = nullptr;
+    return MDP_OK;
+}
+
+extern "C" int mdp_gls_residual(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *d_signal,
+                                const double *d_noise, const double *d_x, double *d_r) {
+    if (!ctx || !A || !N || !d_signal || !d_noise || !d_r) return MDP_EINVAL;
+    if (!A->triplet || N->nrow_end > A->m) {
+        mdp_set_error("mdp_gls_residual: triplet pointing and noise blocks within its rows are needed");
+        return MDP_EUNSUPPORTED;
+    }
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const int64_t m = A->m;
+    MDP_TRY(ctx->ws[0].alloc(8 * m));
+    MDP_TRY(ctx->ws[1].alloc(8 * m));
+    double *ta = ctx->ws[0].as<double>(), *tb = ctx->ws[1].as<double>();
+    const int gm = grid_for(m, 256, ctx->sm_count * 16);
+    if (d_x) MDP_TRY(mdp_matvec_launch(ctx, A, d_x, ta));
+    else MDP_CUDA(cudaMemsetAsync(ta, 0, 8 * m, st));
+    tod_residual_kernel<<<gm, 256, 0, st>>>(A->off.as<int32_t>(), d_signal, d_noise, ta, m);
+    MDP_CHECK_LAUNCH(ctx);
+    MDP_TRY(mdp_stbmm_impl(ctx, N, ta, tb, nullptr));
+    return mdp_trmatvec_launch(ctx, A, tb, d_r);
+}
+
+extern "C" int mdp_apply_op(mdp_context *ctx, mdp_pointing *A, const mdp_noise *Nc, const double *d_h, double *d_q,
+                            int fp32) {
+    if (!ctx || !A || !Nc || !d_h || !d_q) return MDP_EINVAL;
+    mdp_noise *N = const_cast<mdp_noise *>(Nc);  // the FP32 plan is a cache of the operator
+    if (N->nrow_end > A->m) {
+        mdp_set_error("mdp_apply_op: noise blocks extend past the pointing rows");
+        return MDP_EINVAL;
+    }
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    const int64_t m = A->m;
+    if (!fp32) {
+        MDP_TRY(ctx->ws[0].alloc(8 * m));
+        MDP_TRY(ctx->ws[1].alloc(8 * m));
+        double   *ta = ctx->ws[0].as<double>(), *tb = ctx->ws[1].as<double>();
+        const int fused = mdp_matvec_blockmeans(ctx, A, N, d_h, ta);
+        if (fused != MDP_OK && fused != MDP_EUNSUPPORTED) return fused;
+        if (fused == MDP_EUNSUPPORTED) MDP_TRY(mdp_matvec_launch(ctx, A, d_h, ta));
+        MDP_TRY(mdp_stbmm_impl(ctx, N, ta, tb, fused == MDP_OK ? N->means.as<double>() : nullptr));
+        return mdp_trmatvec_launch(ctx, A, tb, d_q);
+    }
+    MDP_TRY(mdp_pointing_prepare_fp32(ctx, A));
+    MDP_TRY(mdp_noise_prepare_fp32(ctx, N));
+    MDP_TRY(ctx->ws[8].alloc(4 * m));
+    MDP_TRY(ctx->ws[9].alloc(4 * m));
+    float    *fa = ctx->ws[8].as<float>(), *fb = ctx->ws[9].as<float>();
+    const int fused = mdp_matvec32_blockmeans(ctx, A, N, d_h, fa);
+    if (fused != MDP_OK && fused != MDP_EUNSUPPORTED) return fused;
+    if (fused == MDP_EUNSUPPORTED) MDP_TRY(mdp_matvec32_launch(ctx, A, d_h, fa));
+    MDP_TRY(mdp_stbmm_impl32(ctx, N, fa, fb, fused == MDP_OK ? N->means.as<double>() : nullptr));
+    return mdp_trmatvec32_launch(ctx, A, fb, d_q);
+}
