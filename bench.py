@@ -339,6 +339,8 @@ def bench_serving(args, device):
         st = serve.latency_stats(r)
         st["max_concurrent"] = srv.max_running
         st["errors"] = sum(1 for x in r if x.error)
+        if st["errors"]:
+            st["error_samples"] = sorted({x.error for x in r if x.error})[:4]
         out[prec] = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in st.items()}
         res[prec] = r
     # FP64 oracle (tol 1e-12) for the requests whose maps were kept: the error

@@ -124,11 +124,16 @@ int  mdp_noise_plan(mdp_context *ctx, mdp_noise *N, int fp32, int *log2_cta_poin
  * on the same device) race on it and must be serialised by the caller. */
 int  mdp_stbmm_noalloc(mdp_context *ctx, const mdp_noise *N, const double *d_in, double *d_out);
 
-/* ---- GLS solve (reference PCG_GLS_true with block-Jacobi, pcg_true.c:20-241) ---- */
+/* ---- GLS solve (reference PCG_GLS_true, pcg_true.c:20-241) ---- */
 typedef struct {
     double tol;      /* relative residual: stop when sum(g^2) <= tol^2 sum(g0^2) */
     int    maxiter;  /* K: at most K-1 iterations, as the reference */
     int    verbose;  /* 1: print the reference's per-iteration line on stdout */
+    int    precond;  /* 0: block Jacobi; 1: two-level a priori (build_Z); 2: two-level
+                        a posteriori (Lanczos Ritz vectors); precond.c:1310-1423.
+                        Two-level: mdp_gls_solve only (FP64) */
+    int    z_2lvl;   /* deflation columns of the two-level preconditioners, 1..128
+                        (0: one, the reference's default of one per rank) */
 } mdp_solve_params;
 
 typedef struct {

@@ -28,7 +28,8 @@ class MidapackError(RuntimeError):
 
 
 class SolveParams(ct.Structure):
-    _fields_ = [("tol", ct.c_double), ("maxiter", ct.c_int), ("verbose", ct.c_int)]
+    _fields_ = [("tol", ct.c_double), ("maxiter", ct.c_int), ("verbose", ct.c_int), ("precond", ct.c_int),
+                ("z_2lvl", ct.c_int)]
 
 
 class SolveInfo(ct.Structure):
@@ -321,8 +322,12 @@ class Noise:
             pass
 
 
-def gls_solve(ctx: Context, A: Pointing, N: Noise, signal, noise, tol=1e-8, maxiter=500, verbose=False):
-    """PCG_GLS_true on device tensors.  Returns (x, lstid, cond, hits, res_rel, info) as torch tensors."""
+def gls_solve(ctx: Context, A: Pointing, N: Noise, signal, noise, tol=1e-8, maxiter=500, verbose=False, precond=0,
+              z_2lvl=0):
+    """PCG_GLS_true on device tensors.  Returns (x, lstid, cond, hits, res_rel, info) as torch tensors.
+
+    precond 0: block Jacobi; 1: two-level a priori; 2: two-level a posteriori (Lanczos), with z_2lvl
+    deflation columns (0: one)."""
     import torch
     n0 = A.shape()["n_map"]
     x = torch.empty(max(n0, 1), dtype=torch.float64, device="cuda")
@@ -330,7 +335,7 @@ def gls_solve(ctx: Context, A: Pointing, N: Noise, signal, noise, tol=1e-8, maxi
     cond = torch.empty(max(n0 // 3, 1), dtype=torch.float64, device="cuda")
     hits = torch.empty(max(n0 // 3, 1), dtype=torch.int32, device="cuda")
     res = np.zeros(maxiter + 1)
-    prm = SolveParams(tol, maxiter, 1 if verbose else 0)
+    prm = SolveParams(tol, maxiter, 1 if verbose else 0, precond, z_2lvl)
     info = SolveInfo()
     check(lib().mdp_gls_solve(ctx.h, A.h, N.h, ct.c_void_p(_ptr(signal)), ct.c_void_p(_ptr(noise)), ct.byref(prm),
                               ct.c_void_p(x.data_ptr()), ct.c_void_p(lst.data_ptr()), ct.c_void_p(cond.data_ptr()),

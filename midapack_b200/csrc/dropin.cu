@@ -475,41 +475,120 @@ extern "C" int precondblockjacobilike(Mat *A, Tpltz *Nm1, Mat *BJ_inv, Mat *BJ, 
     return 0;
 }
 
+// Two-level state of the device pointing/noise after the block-Jacobi cut;
+// precond 2 starts its Lanczos run from the first residual P^T N^-1 (b + noise)
+// with b the (cut) host signal.
+static int twolevel_for(mdp_context *ctx, MatDev *D, mdp_noise *N, int precond, int zn, const double *b,
+                        const double *noise, mdp_twolevel *tl) {
+    DevBuf g0;
+    if (precond == 2) {
+        const int64_t m = D->P->m;
+        DevBuf        db, dn;
+        MDP_TRY(db.alloc(8 * m));
+        MDP_TRY(dn.alloc(8 * m));
+        MDP_TRY(g0.alloc(8 * std::max<int64_t>(D->P->n_map(), 1)));
+        MDP_CUDA(cudaMemcpyAsync(db.p, b, 8 * m, cudaMemcpyHostToDevice, ctx->stream));
+        MDP_CUDA(cudaMemcpyAsync(dn.p, noise, 8 * m, cudaMemcpyHostToDevice, ctx->stream));
+        MDP_TRY(mdp_gls_rhs(ctx, D->P, N, db.as<double>(), dn.as<double>(), g0.as<double>()));
+        MDP_CUDA(cudaStreamSynchronize(ctx->stream));  // db, dn are released on return
+    }
+    return mdp_twolevel_build(ctx, D->P, N, precond, zn, g0.as<double>(), tl);
+}
+
 extern "C" void build_precond(Precond **out_p, double **out_pixpond, int *out_n, Mat *A, Tpltz *Nm1, double **in_out_x,
                               double *b, double *noise, double *cond, int *lhits, double tol, int Zn, int precond) {
-    (void) noise;
     (void) tol;
-    if (precond != 0) {
-        fprintf(stderr, "midapack_b200 build_precond: only precond = 0 (block Jacobi) is available\n");
-        *out_p = nullptr;
+    *out_p = nullptr;
+    if (precond < 0 || precond > 2) {
+        fprintf(stderr, "midapack_b200 build_precond: precond must be 0 (block Jacobi), 1 or 2 (two-level), got %d\n",
+                precond);
         return;
     }
     Precond *p = (Precond *) calloc(1, sizeof(Precond));
-    p->precond = 0;
+    p->precond = precond;
     p->Zn = Zn;
     if (precondblockjacobilike(A, Nm1, &p->BJ_inv, &p->BJ, b, cond, lhits) != 0) {
         free(p);
-        *out_p = nullptr;
         return;
     }
     p->n = A->lcount - A->nnz * A->trash_pix;
     p->pixpond = (double *) malloc(sizeof(double) * std::max(p->n, 1));
     get_pixshare_pond(A, p->pixpond);
+    if (precond != 0) {
+        // Z, AZ (Zn columns of n) and Em1 (Zn x Zn) built on the device and
+        // kept in the reference's host fields (precond.c:1341-1394)
+        std::lock_guard<std::mutex> lk(g_mu);
+        mdp_context                *ctx = default_ctx();
+        MatDev                     *D = mat_dev(A);
+        mdp_noise                  *N = nullptr;
+        mdp_twolevel                tl;
+        int                         rc = D ? noise_for(Nm1, &N) : MDP_EINVAL;
+        if (!rc) rc = twolevel_for(ctx, D, N, precond, Zn, b, noise, &tl);
+        if (rc) {
+            fail("build_precond", rc);
+            free(p->pixpond);
+            free(p);
+            return;
+        }
+        const int zn = tl.zn, n = p->n;
+        p->Zn = zn;
+        p->Z = (double **) calloc(zn, sizeof(double *));
+        p->AZ = (double **) calloc(zn, sizeof(double *));
+        for (int j = 0; j < zn; j++) {
+            p->Z[j] = (double *) malloc(sizeof(double) * std::max(n, 1));
+            p->AZ[j] = (double *) malloc(sizeof(double) * std::max(n, 1));
+            cudaMemcpy(p->Z[j], tl.Z.as<double>() + (int64_t) j * n, 8 * (size_t) n, cudaMemcpyDeviceToHost);
+            cudaMemcpy(p->AZ[j], tl.AZ.as<double>() + (int64_t) j * n, 8 * (size_t) n, cudaMemcpyDeviceToHost);
+        }
+        p->Em1 = (double *) malloc(sizeof(double) * (size_t) zn * zn);
+        memcpy(p->Em1, tl.h_Em1.data(), sizeof(double) * (size_t) zn * zn);
+        p->Qg = (double *) calloc(std::max(n, 1), sizeof(double));
+        p->AQg = (double *) calloc(std::max(n, 1), sizeof(double));
+        p->w = (double *) calloc(zn, sizeof(double));
+        p->Qtx = (double *) calloc(zn, sizeof(double));
+    }
     *out_p = p;
     *out_pixpond = p->pixpond;
     *out_n = p->n;
     (void) in_out_x;  // x keeps its allocation (it is at least n long)
 }
 
+// Host arrays in and out, as the reference's apply_precond: block Jacobi, or
+// the two-level product Cg = BJ_inv (g - AZ Qtx) + Z Qtx with Qtx = Em1 Z^T g
+// (precond.c:1403-1423)
 extern "C" void apply_precond(Precond *p, const Mat *A, Tpltz *Nm1, double *g, double *Cg) {
     (void) A;
     (void) Nm1;
     const int n = p->BJ_inv.m;
+    const double *src = g;
+    if (p->precond != 0) {
+        const int zn = p->Zn;
+        for (int j = 0; j < zn; j++) {
+            double s = 0.0;
+            for (int k = 0; k < n; k++) s += p->Z[j][k] * g[k] * p->pixpond[k];
+            p->w[j] = s;
+        }
+        for (int i = 0; i < zn; i++) {
+            double s = 0.0;
+            for (int j = 0; j < zn; j++) s += p->Em1[i * zn + j] * p->w[j];
+            p->Qtx[i] = s;
+        }
+        for (int k = 0; k < n; k++) p->Qg[k] = p->AQg[k] = 0.0;
+        for (int j = 0; j < zn; j++)
+            for (int k = 0; k < n; k++) {
+                p->Qg[k] += p->Z[j][k] * p->Qtx[j];
+                p->AQg[k] += p->AZ[j][k] * p->Qtx[j];
+            }
+        for (int k = 0; k < n; k++) p->AQg[k] = g[k] - p->AQg[k];
+        src = p->AQg;
+    }
     for (int i = 0; i < n; i++) {
         const double *r = p->BJ_inv.values + 3 * i;
         const int     q = 3 * (i / 3);
-        Cg[i] = r[0] * g[q] + r[1] * g[q + 1] + r[2] * g[q + 2];
+        Cg[i] = r[0] * src[q] + r[1] * src[q + 1] + r[2] * src[q + 2];
     }
+    if (p->precond != 0)
+        for (int i = 0; i < n; i++) Cg[i] += p->Qg[i];
 }
 
 extern "C" void free_precond(Precond **in_out_p) {
@@ -521,6 +600,19 @@ extern "C" void free_precond(Precond **in_out_p) {
     free(p->BJ_inv.lindices);
     free(p->BJ.values);
     free(p->BJ.lindices);
+    if (p->precond != 0) {
+        for (int j = 0; j < p->Zn; j++) {
+            if (p->Z) free(p->Z[j]);
+            if (p->AZ) free(p->AZ[j]);
+        }
+        free(p->Z);
+        free(p->AZ);
+        free(p->Em1);
+        free(p->Qg);
+        free(p->AQg);
+        free(p->w);
+        free(p->Qtx);
+    }
     free(p);
     *in_out_p = nullptr;
 }
@@ -537,9 +629,8 @@ static void write_residuals(const char *outpath, const char *ref, const std::vec
 
 extern "C" int PCG_GLS_true(char *outpath, char *ref, Mat *A, Tpltz *Nm1, double *x, double *b, double *noise,
                             double *cond, int *lhits, double tol, int K, int precond, int Z_2lvl) {
-    (void) Z_2lvl;
-    if (precond != 0) {
-        fprintf(stderr, "midapack_b200 PCG_GLS_true: only precond = 0 (block Jacobi) is available\n");
+    if (precond < 0 || precond > 2) {
+        fprintf(stderr, "midapack_b200 PCG_GLS_true: precond must be 0 (block Jacobi), 1 or 2 (two-level)\n");
         return 1;
     }
     std::lock_guard<std::mutex> lk(g_mu);
@@ -563,11 +654,13 @@ extern "C" int PCG_GLS_true(char *outpath, char *ref, Mat *A, Tpltz *Nm1, double
         return fail("PCG_GLS_true", rc);
     cudaMemcpyAsync(db.p, b, 8 * m, cudaMemcpyHostToDevice, ctx->stream);
     cudaMemcpyAsync(dn.p, noise, 8 * m, cudaMemcpyHostToDevice, ctx->stream);
-    mdp_solve_params prm = {tol, K, 1};
+    mdp_twolevel tl;
+    if (precond != 0 && (rc = twolevel_for(ctx, D, N, precond, Z_2lvl, b, noise, &tl))) return fail("PCG_GLS_true", rc);
+    mdp_solve_params prm = {tol, K, 1, precond, Z_2lvl};
     mdp_solve_info   info = {};
     std::vector<double> res(std::max(K, 1) + 1, 0.0);
     rc = mdp_pcg_run(ctx, D->P, N, bj.inv.as<double>(), bj.npix, db.as<double>(), dn.as<double>(), &prm, dx.as<double>(),
-                     res.data(), &info);
+                     res.data(), &info, precond != 0 ? &tl : nullptr);
     if (rc) return fail("PCG_GLS_true", rc);
     cudaMemcpy(x, dx.p, 8 * 3 * bj.npix, cudaMemcpyDeviceToHost);
     cudaMemcpy(cond, bj.rcond.p, 8 * bj.npix, cudaMemcpyDeviceToHost);
@@ -602,7 +695,7 @@ static void x2map(double *mapI, double *mapQ, double *mapU, double *Cond, int *H
 
 static int mlmap_device(int m, int nb, const int *blocks, const int *pix, const double *w, const double *sig,
                         const double *noi, int lambda, const double *invtt, double tol, int maxiter, int verbose,
-                        std::vector<double> &x, std::vector<int> &lstid, std::vector<double> &cond,
+                        int precond, int z_2lvl, std::vector<double> &x, std::vector<int> &lstid, std::vector<double> &cond,
                         std::vector<int> &hits, int *iters, double *res_rel) {
     mdp_context *ctx = default_ctx();
     if (!ctx) return MDP_ECUDA;
@@ -638,7 +731,7 @@ static int mlmap_device(int m, int nb, const int *blocks, const int *pix, const 
         mdp_noise_destroy(N);
         return rc;
     }
-    mdp_solve_params    prm = {tol, maxiter, verbose};
+    mdp_solve_params    prm = {tol, maxiter, verbose, precond, z_2lvl};
     mdp_solve_info      info = {};
     std::vector<double> res(std::max(maxiter, 1) + 1, 0.0);
     rc = mdp_gls_solve(ctx, P, N, ds.as<double>(), dn.as<double>(), &prm, dx.as<double>(), dl.as<int32_t>(),
@@ -728,9 +821,9 @@ extern "C" void MLmap(MPI_Comm comm, char *outpath, char *ref, int solver, int p
                       int pointing_commflag, double tol, int maxiter, int enlFac, int ortho_alg, int bs_red, int nside,
                       void *data_size_proc, int nb_blocks_loc, void *local_blocks_sizes, int Nnz, void *pix,
                       void *pixweights, void *signal, double *noise, int lambda, double *invtt) {
-    (void) comm, (void) Z_2lvl, (void) pointing_commflag, (void) enlFac, (void) ortho_alg, (void) bs_red;
-    if (solver != 0 || precond != 0 || Nnz != 3) {
-        fprintf(stderr, "midapack_b200 MLmap: only solver 0 (PCG), precond 0 (block Jacobi) and Nnz 3 are available\n");
+    (void) comm, (void) pointing_commflag, (void) enlFac, (void) ortho_alg, (void) bs_red;
+    if (solver != 0 || precond < 0 || precond > 2 || Nnz != 3) {
+        fprintf(stderr, "midapack_b200 MLmap: only solver 0 (PCG), precond 0, 1, 2 and Nnz 3 are available\n");
         return;
     }
     const int m = ((int *) data_size_proc)[0];
@@ -743,8 +836,8 @@ extern "C" void MLmap(MPI_Comm comm, char *outpath, char *ref, int solver, int p
     {
         std::lock_guard<std::mutex> lk(g_mu);
         rc = mlmap_device(m, nb_blocks_loc, (const int *) local_blocks_sizes, (const int *) pix,
-                          (const double *) pixweights, (const double *) signal, noise, lambda, invtt, tol, maxiter, 1, x,
-                          lstid, cond, hits, &it, &rr);
+                          (const double *) pixweights, (const double *) signal, noise, lambda, invtt, tol, maxiter, 1,
+                          precond, Z_2lvl, x, lstid, cond, hits, &it, &rr);
     }
     if (rc) {
         fail("MLmap", rc);
@@ -769,8 +862,8 @@ extern "C" int MLmap_b200(int solver, int precond, double tol, int maxiter, int 
                           const int *local_blocks_sizes, int Nnz, const int *pix, const double *pixweights,
                           const double *signal, const double *noise, int lambda, const double *invtt, double *mapI,
                           double *mapQ, double *mapU, double *Cond, int *Hits, int *iterations, double *res_rel) {
-    if (solver != 0 || precond != 0 || Nnz != 3) {
-        mdp_set_error("MLmap_b200: only solver 0, precond 0 and Nnz 3 are available");
+    if (solver != 0 || precond < 0 || precond > 2 || Nnz != 3) {
+        mdp_set_error("MLmap_b200: only solver 0, precond 0, 1, 2 and Nnz 3 are available");
         return MDP_EUNSUPPORTED;
     }
     std::vector<double> x, cond;
@@ -779,7 +872,7 @@ extern "C" int MLmap_b200(int solver, int precond, double tol, int maxiter, int 
     {
         std::lock_guard<std::mutex> lk(g_mu);
         rc = mlmap_device(m, nb_blocks_loc, local_blocks_sizes, pix, pixweights, signal, noise, lambda, invtt, tol,
-                          maxiter, 0, x, lstid, cond, hits, iterations, res_rel);
+                          maxiter, 0, precond, 0, x, lstid, cond, hits, iterations, res_rel);
     }
     if (rc) return rc;
     const int64_t npix = 12LL * nside * nside;

@@ -189,11 +189,32 @@ struct mdp_noise {
     DevBuf               partial;        // double [n_chunks] chunk sums
 };
 
+// ---------------------------------------------------------------- two-level preconditioner (twolevel.cu)
+// M g = BJ_inv (g - AZ qtx) + Z qtx with qtx = Em1 Z^T g, Em1 the pseudo-inverse
+// of E = Z^T AZ and AZ = P^T N^-1 P Z.
+#define MDP_TL_MAX_ZN 128
+#define MDP_TL_BLOCKS 296
+struct mdp_twolevel {
+    int     precond = 0;   // 1: a priori columns (build_Z), 2: Ritz vectors (Lanczos)
+    int     zn = 0;        // deflation columns
+    int64_t n = 0;         // map unknowns
+    DevBuf  Z, AZ;         // double [zn][n]
+    DevBuf  Em1;           // double [zn][zn] row-major
+    DevBuf  qtx;           // double [zn]
+    DevBuf  part;          // double [zn][MDP_TL_BLOCKS] partial dot products
+    std::vector<double> h_Em1;
+};
+int mdp_twolevel_build(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, int precond, int zn,
+                       const double *d_g0, mdp_twolevel *tl);
+int mdp_twolevel_qtx(mdp_context *ctx, const mdp_twolevel *tl, const double *d_g);
+int mdp_apply_op_impl(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *d_h, double *d_q);
+int mdp_gls_rhs(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *d_signal, const double *d_noise,
+                double *d_g);
 int mdp_bj_build(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, BJState *bj);
 int mdp_bj_cached(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const BJState **bj);
 int mdp_pcg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *inv, int64_t npix,
                 const double *d_signal, const double *d_noise, const mdp_solve_params *params, double *d_x,
-                double *h_res_rel, mdp_solve_info *info);
+                double *h_res_rel, mdp_solve_info *info, const mdp_twolevel *tl = nullptr);
 int mdp_pointing_create_ex(mdp_context *ctx, int64_t m, int nnz, const int32_t *d_g, const double *d_values,
                            int32_t *d_local_out, mdp_pointing **out);
 int mdp_matvec_launch(mdp_context *ctx, const mdp_pointing *A, const double *d_x, double *d_y);

@@ -479,6 +479,111 @@ __global__ void __launch_bounds__(RED_THREADS) pcg_update_kernel(const double *_
     }
 }
 
+// ---------------------------------------------------------------- two-level preconditioner
+// c = M g for pixel q: BJ_inv (g - AZ qtx) + Z qtx, sums over the columns in
+// column order (apply_precond, precond.c:1412-1423; mul_ZQtx :1053-1069)
+__device__ __forceinline__ void tl_apply3(const double *__restrict__ inv, const double *__restrict__ Z,
+                                          const double *__restrict__ AZ, const double *qtx, int zn, int64_t n,
+                                          int64_t q, const double (&gq)[3], double (&c)[3]) {
+    double qg[3] = {0.0, 0.0, 0.0}, aq[3] = {0.0, 0.0, 0.0};
+    for (int j = 0; j < zn; j++) {
+        const double  t = qtx[j];
+        const double *z = Z + (int64_t) j * n + 3 * q, *az = AZ + (int64_t) j * n + 3 * q;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            qg[k] += z[k] * t;
+            aq[k] += az[k] * t;
+        }
+    }
+    double r[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) r[k] = gq[k] - aq[k];
+    const double *I = inv + 9 * q;
+    c[0] = I[0] * r[0] + I[1] * r[1] + I[2] * r[2];
+    c[1] = I[3] * r[0] + I[4] * r[1] + I[5] * r[2];
+    c[2] = I[6] * r[0] + I[7] * r[1] + I[8] * r[2];
+#pragma unroll
+    for (int k = 0; k < 3; k++) c[k] += qg[k];
+}
+
+// init with the two-level preconditioner: Cg = M g, h = Cg, g2pix = (Cg, g), res = (g, g)
+__global__ void __launch_bounds__(RED_THREADS) pcg_init_tl_kernel(const double *__restrict__ inv,
+                                                                  const double *__restrict__ g, double *__restrict__ Cg,
+                                                                  double *__restrict__ h, int64_t npix,
+                                                                  const double *__restrict__ Z,
+                                                                  const double *__restrict__ AZ,
+                                                                  const double *__restrict__ qtx_g, int zn, Scal *S) {
+    __shared__ double qtx[MDP_TL_MAX_ZN];
+    for (int j = threadIdx.x; j < zn; j += blockDim.x) qtx[j] = qtx_g[j];
+    __syncthreads();
+    const int64_t n = 3 * npix;
+    double        v[2] = {0.0, 0.0};
+    for (int64_t q = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; q < npix; q += (int64_t) gridDim.x * blockDim.x) {
+        const double gq[3] = {g[3 * q], g[3 * q + 1], g[3 * q + 2]};
+        double       c[3];
+        tl_apply3(inv, Z, AZ, qtx, zn, n, q, gq, c);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            Cg[3 * q + k] = c[k];
+            h[3 * q + k] = c[k];
+            v[0] += c[k] * gq[k];
+            v[1] += gq[k] * gq[k];
+        }
+    }
+    block_reduce_store<2>(v, S, 0);
+    if (last_block(S, 0) && threadIdx.x == 0) {
+        S->g2pix = sum_partials(S, 0);
+        S->res = sum_partials(S, 1);
+        S->count[0] = 0;
+    }
+}
+
+// x += ro h; g = gp - ro AtNm1Ah (the preconditioner follows once Z^T g is known)
+__global__ void pcg_step_kernel(double *__restrict__ x, const double *__restrict__ h, const double *__restrict__ q_,
+                                const double *__restrict__ gp, double *__restrict__ g, int64_t n, const Scal *S) {
+    const double ro = S->ro;
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+        x[i] = x[i] + ro * h[i];
+        g[i] = gp[i] - ro * q_[i];
+    }
+}
+
+// Cg = M g with the two-level preconditioner; dots (Cg,g), (Cg,g-gp), (g,g)
+__global__ void __launch_bounds__(RED_THREADS) pcg_precond_tl_kernel(const double *__restrict__ inv,
+                                                                     const double *__restrict__ g,
+                                                                     const double *__restrict__ gp,
+                                                                     double *__restrict__ Cg, int64_t npix,
+                                                                     const double *__restrict__ Z,
+                                                                     const double *__restrict__ AZ,
+                                                                     const double *__restrict__ qtx_g, int zn, Scal *S) {
+    __shared__ double qtx[MDP_TL_MAX_ZN];
+    for (int j = threadIdx.x; j < zn; j += blockDim.x) qtx[j] = qtx_g[j];
+    __syncthreads();
+    const int64_t n = 3 * npix;
+    double        v[3] = {0.0, 0.0, 0.0};
+    for (int64_t q = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; q < npix; q += (int64_t) gridDim.x * blockDim.x) {
+        const double gq[3] = {g[3 * q], g[3 * q + 1], g[3 * q + 2]};
+        double       c[3];
+        tl_apply3(inv, Z, AZ, qtx, zn, n, q, gq, c);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            Cg[3 * q + k] = c[k];
+            v[0] += c[k] * gq[k];
+            v[1] += c[k] * (gq[k] - gp[3 * q + k]);
+            v[2] += gq[k] * gq[k];
+        }
+    }
+    block_reduce_store<3>(v, S, 0);
+    if (last_block(S, 2) && threadIdx.x == 0) {
+        S->g2pixp = S->g2pix;
+        S->g2pix = sum_partials(S, 0);
+        S->g2pix_polak = sum_partials(S, 1);
+        S->res = sum_partials(S, 2);
+        S->gamma = S->g2pix_polak / S->g2pixp;
+        S->count[2] = 0;
+    }
+}
+
 // out = d' - out where d' = b (0 on cut rows) + noise: the TOD residual d' - P x
 __global__ void tod_residual_kernel(const int32_t *__restrict__ off, const double *__restrict__ b,
                                     const double *__restrict__ noise, double *__restrict__ out, int64_t m) {
@@ -602,7 +707,7 @@ int mdp_bj_build(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, BJState 
 
 int mdp_pcg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *inv, int64_t npix,
                 const double *d_signal, const double *d_noise, const mdp_solve_params *params, double *d_x,
-                double *h_res_rel, mdp_solve_info *info) {
+                double *h_res_rel, mdp_solve_info *info, const mdp_twolevel *tl) {
     cudaStream_t  st = ctx->stream;
     const int64_t m = A->m;
     const int64_t n = 3 * npix;
@@ -627,7 +732,13 @@ int mdp_pcg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const dou
     MDP_CHECK_LAUNCH(ctx);
     MDP_TRY(mdp_stbmm_impl(ctx, N, ta, tb, nullptr));
     MDP_TRY(mdp_trmatvec_launch(ctx, A, tb, g));
-    pcg_init_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(inv, g, Cg, h, npix, S);
+    if (tl) {
+        MDP_TRY(mdp_twolevel_qtx(ctx, tl, g));
+        pcg_init_tl_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(inv, g, Cg, h, npix, tl->Z.as<double>(),
+                                                               tl->AZ.as<double>(), tl->qtx.as<double>(), tl->zn, S);
+    } else {
+        pcg_init_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(inv, g, Cg, h, npix, S);
+    }
     MDP_CHECK_LAUNCH(ctx);
     Scal *hs = reinterpret_cast<Scal *>(ctx->h_pinned);
     MDP_CUDA(cudaMemcpyAsync(hs, S, 8 * 8, cudaMemcpyDeviceToHost, st));
@@ -661,7 +772,16 @@ int mdp_pcg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const dou
         if (prof) cudaEventRecord(ctx->ev[3], st);
         pcg_coeff_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(h, q, n, S);
         MDP_CHECK_LAUNCH(ctx);
-        pcg_update_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(inv, x, h, q, gp, g, Cg, npix, S);
+        if (tl) {
+            pcg_step_kernel<<<grid_for(n, 256, ctx->sm_count * 8), 256, 0, st>>>(x, h, q, gp, g, n, S);
+            MDP_CHECK_LAUNCH(ctx);
+            MDP_TRY(mdp_twolevel_qtx(ctx, tl, g));
+            pcg_precond_tl_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(inv, g, gp, Cg, npix, tl->Z.as<double>(),
+                                                                      tl->AZ.as<double>(), tl->qtx.as<double>(),
+                                                                      tl->zn, S);
+        } else {
+            pcg_update_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(inv, x, h, q, gp, g, Cg, npix, S);
+        }
         MDP_CHECK_LAUNCH(ctx);
         if (prof) cudaEventRecord(ctx->ev[4], st);
         MDP_CUDA(cudaMemcpyAsync(hs, S, 8 * 8, cudaMemcpyDeviceToHost, st));
@@ -723,8 +843,22 @@ extern "C" int mdp_gls_solve(mdp_context *ctx, mdp_pointing *A, const mdp_noise 
     if (d_cond) MDP_CUDA(cudaMemcpyAsync(d_cond, bj.rcond.p, 8 * bj.npix, cudaMemcpyDeviceToDevice, st));
     if (d_hits) MDP_CUDA(cudaMemcpyAsync(d_hits, bj.hits.p, 4 * bj.npix, cudaMemcpyDeviceToDevice, st));
     MDP_CUDA(cudaStreamSynchronize(st));
+    // two-level preconditioners: Z, AZ and E^+ on the post-cut pointing; the
+    // a-posteriori columns start from the first residual (precond.c:1341-1360)
+    mdp_twolevel  tl;
+    mdp_twolevel *tlp = nullptr;
+    if (params->precond != 0) {
+        DevBuf g0;
+        if (params->precond == 2) {
+            MDP_TRY(g0.alloc(8 * (size_t) A->n_map()));
+            MDP_TRY(mdp_gls_rhs(ctx, A, N, d_signal, d_noise, g0.as<double>()));
+        }
+        MDP_TRY(mdp_twolevel_build(ctx, A, N, params->precond, params->z_2lvl, g0.as<double>(), &tl));
+        tlp = &tl;
+    }
     auto tp1 = std::chrono::steady_clock::now();
-    MDP_TRY(mdp_pcg_run(ctx, A, N, bj.inv.as<double>(), bj.npix, d_signal, d_noise, params, d_x, h_res_rel, info));
+    MDP_TRY(mdp_pcg_run(ctx, A, N, bj.inv.as<double>(), bj.npix, d_signal, d_noise, params, d_x, h_res_rel, info,
+                        tlp));
     auto tp2 = std::chrono::steady_clock::now();
     if (info) {
         info->n_cut = bj.ncut;
@@ -773,6 +907,10 @@ extern "C" int mdp_gls_solve_mixed(mdp_context *ctx, mdp_pointing *A, const mdp_
     if (N->nrow_end > A->m) {
         mdp_set_error("mdp_gls_solve_mixed: noise blocks extend past the pointing rows");
         return MDP_EINVAL;
+    }
+    if (params->precond != 0) {
+        mdp_set_error("mdp_gls_solve_mixed: the two-level preconditioners run on the FP64 path (mdp_gls_solve)");
+        return MDP_EUNSUPPORTED;
     }
     MDP_CUDA(cudaSetDevice(ctx->device));
     auto           tp0 = std::chrono::steady_clock::now();
@@ -1007,6 +1145,33 @@ extern "C" int mdp_pointing_cut(mdp_context *ctx, mdp_pointing *A, const int32_t
     return MDP_OK;
 }
 
+// g = P^T N^-1 d' with d' = b (0 on cut rows) + noise: the PCG's first residual for x0 = 0
+int mdp_gls_rhs(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *d_signal, const double *d_noise,
+                double *d_g) {
+    const int64_t m = A->m;
+    MDP_TRY(ctx->ws[0].alloc(8 * m));
+    MDP_TRY(ctx->ws[1].alloc(8 * m));
+    double *ta = ctx->ws[0].as<double>(), *tb = ctx->ws[1].as<double>();
+    rhs_kernel<<<grid_for(m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(A->off.as<int32_t>(), d_signal,
+                                                                               d_noise, ta, m);
+    MDP_CHECK_LAUNCH(ctx);
+    MDP_TRY(mdp_stbmm_impl(ctx, N, ta, tb, nullptr));
+    return mdp_trmatvec_launch(ctx, A, tb, d_g);
+}
+
+// q = P^T N^-1 P h in FP64, the block means of P h fused into P when the blocks tile the rows
+int mdp_apply_op_impl(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *d_h, double *d_q) {
+    const int64_t m = A->m;
+    MDP_TRY(ctx->ws[0].alloc(8 * m));
+    MDP_TRY(ctx->ws[1].alloc(8 * m));
+    double   *ta = ctx->ws[0].as<double>(), *tb = ctx->ws[1].as<double>();
+    const int fused = mdp_matvec_blockmeans(ctx, A, N, d_h, ta);
+    if (fused != MDP_OK && fused != MDP_EUNSUPPORTED) return fused;
+    if (fused == MDP_EUNSUPPORTED) MDP_TRY(mdp_matvec_launch(ctx, A, d_h, ta));
+    MDP_TRY(mdp_stbmm_impl(ctx, N, ta, tb, fused == MDP_OK ? N->means.as<double>() : nullptr));
+    return mdp_trmatvec_launch(ctx, A, tb, d_q);
+}
+
 extern "C" int mdp_gls_residual(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *d_signal,
                                 const double *d_noise, const double *d_x, double *d_r) {
     if (!ctx || !A || !N || !d_signal || !d_noise || !d_r) return MDP_EINVAL;
@@ -1039,16 +1204,7 @@ extern "C" int mdp_apply_op(mdp_context *ctx, mdp_pointing *A, const mdp_noise *
     }
     MDP_CUDA(cudaSetDevice(ctx->device));
     const int64_t m = A->m;
-    if (!fp32) {
-        MDP_TRY(ctx->ws[0].alloc(8 * m));
-        MDP_TRY(ctx->ws[1].alloc(8 * m));
-        double   *ta = ctx->ws[0].as<double>(), *tb = ctx->ws[1].as<double>();
-        const int fused = mdp_matvec_blockmeans(ctx, A, N, d_h, ta);
-        if (fused != MDP_OK && fused != MDP_EUNSUPPORTED) return fused;
-        if (fused == MDP_EUNSUPPORTED) MDP_TRY(mdp_matvec_launch(ctx, A, d_h, ta));
-        MDP_TRY(mdp_stbmm_impl(ctx, N, ta, tb, fused == MDP_OK ? N->means.as<double>() : nullptr));
-        return mdp_trmatvec_launch(ctx, A, tb, d_q);
-    }
+    if (!fp32) return mdp_apply_op_impl(ctx, A, N, d_h, d_q);
     MDP_TRY(mdp_pointing_prepare_fp32(ctx, A));
     MDP_TRY(mdp_noise_prepare_fp32(ctx, N));
     MDP_TRY(ctx->ws[8].alloc(4 * m));

@@ -1307,13 +1307,21 @@ static int build_split_tables(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, 
     }
     constexpr int CW = SplitShape<T>::CW, RP = SplitShape<T>::RP;
     const size_t  sc = split_cols_smem<V>(P.log_m1, P.log_m2, CW), sr = split_rows_smem<V>(P.log_m1, P.log_m2, RP);
+    // A split kernel's shared memory depends on both factors while the kernel
+    // only fixes one of them: plans of other operators launch the same kernel
+    // with other sizes.  The per-kernel limit is therefore raised to the
+    // device's opt-in maximum once, never lowered to this plan's need (which
+    // would make the launches of a larger plan built earlier fail).
+    int optin = 0;
+    MDP_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    if (sc > (size_t) optin || sr > (size_t) optin) return MDP_EUNSUPPORTED;
     for (const void *fn : {pick_cols<T, false>(P.log_m1), pick_cols<T, true>(P.log_m1)}) {
         if (!fn) return MDP_EUNSUPPORTED;
-        MDP_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sc));
+        MDP_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     }
     const void *fr = pick_rows<T>(P.log_m2);
     if (!fr) return MDP_EUNSUPPORTED;
-    MDP_CUDA(cudaFuncSetAttribute(fr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sr));
+    MDP_CUDA(cudaFuncSetAttribute(fr, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     return MDP_OK;
 }
 

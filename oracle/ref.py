@@ -74,8 +74,10 @@ def stbmm(V, block_sizes, lam, invtt):
     return out
 
 
-def pcg(gindices, values, signal, noise, block_sizes, lam, invtt, tol=1e-8, maxiter=500, nnz=3):
-    """Single-rank MLmap set-up + PCG_GLS_true. Returns (x, lstid, cond, hits, res_rel)."""
+def pcg(gindices, values, signal, noise, block_sizes, lam, invtt, tol=1e-8, maxiter=500, nnz=3, precond=0,
+        z_2lvl=0):
+    """Single-rank MLmap set-up + PCG_GLS_true (precond 0: block Jacobi, 1/2: the
+    two-level preconditioners with z_2lvl columns). Returns (x, lstid, cond, hits, res_rel)."""
     m = len(signal)
     idx = np.ascontiguousarray(gindices, dtype=np.int32).copy()
     v = np.ascontiguousarray(values, dtype=np.float64).copy()
@@ -89,9 +91,9 @@ def pcg(gindices, values, signal, noise, block_sizes, lam, invtt, tol=1e-8, maxi
     cond = np.zeros(cap // 3 + 1)
     hits = np.zeros(cap // 3 + 1, dtype=np.int32)
     with tempfile.TemporaryDirectory() as td:
-        n = lib().ref_pcg(m, nnz, _p(idx, I32), _p(v, F64), _p(sig, F64), _p(noi, F64), len(bs), _p(bs, I32), lam,
-                          _p(tt, F64), F64(tol), maxiter, td.encode(), b"oracle", _p(x, F64), _p(lstid, I32),
-                          _p(cond, F64), _p(hits, I32), cap)
+        n = lib().ref_pcg_precond(m, nnz, _p(idx, I32), _p(v, F64), _p(sig, F64), _p(noi, F64), len(bs),
+                                  _p(bs, I32), lam, _p(tt, F64), F64(tol), maxiter, precond, z_2lvl, td.encode(),
+                                  b"oracle", _p(x, F64), _p(lstid, I32), _p(cond, F64), _p(hits, I32), cap)
         res = np.fromfile(os.path.join(td, "pcg_residuals_oracle.dat"), dtype=np.float64)
     return x[:n].copy(), lstid[:n].copy(), cond[:n // 3].copy(), hits[:n // 3].copy(), res
 

@@ -108,14 +108,17 @@ static void build_ll(Mat *A, int m) {
 }
 
 /*
- * Single-rank GLS solve exactly as MLmap drives it (solver 0, BJ precond).
+ * Single-rank GLS solve exactly as MLmap drives it (solver 0); precond 0 is
+ * block Jacobi, 1 and 2 the two-level preconditioners with z_2lvl columns
+ * (0: one per rank).
  * gindices/values/signal are modified in place like the reference does.
  * Outputs: x_out (capacity 3*npix_cap unknowns), lstid_out (global ids of x),
  * cond_out, hits_out; returns the number of unknowns n.
  */
-int ref_pcg(int m, int nnz, int *gindices, double *values, double *signal, double *noise, int nb_blocks,
-            int *block_sizes, int lambda, double *invtt, double tol, int maxiter, const char *outpath,
-            const char *ref, double *x_out, int *lstid_out, double *cond_out, int *hits_out, int cap) {
+int ref_pcg_precond(int m, int nnz, int *gindices, double *values, double *signal, double *noise, int nb_blocks,
+                    int *block_sizes, int lambda, double *invtt, double tol, int maxiter, int precond, int z_2lvl,
+                    const char *outpath, const char *ref, double *x_out, int *lstid_out, double *cond_out,
+                    int *hits_out, int cap) {
     Mat A;
     build_mat(&A, m, nnz, gindices, values);
     build_ll(&A, m);
@@ -126,7 +129,8 @@ int ref_pcg(int m, int nnz, int *gindices, double *values, double *signal, doubl
     Tpltz   Nm1;
     Block  *blocks;
     build_tpltz(&Nm1, &blocks, nb_blocks, block_sizes, lambda, invtt, (int64_t) m);
-    PCG_GLS_true((char *) outpath, (char *) ref, &A, &Nm1, x, signal, noise, cond, lhits, tol, maxiter, 0, 0);
+    PCG_GLS_true((char *) outpath, (char *) ref, &A, &Nm1, x, signal, noise, cond, lhits, tol, maxiter, precond,
+                 z_2lvl);
     int n = A.lcount - A.nnz * A.trash_pix;
     if (n > cap) n = cap;
     memcpy(x_out, x, sizeof(double) * (size_t) n);
@@ -139,6 +143,13 @@ int ref_pcg(int m, int nnz, int *gindices, double *values, double *signal, doubl
     free(lhits);
     free(blocks);
     return n;
+}
+
+int ref_pcg(int m, int nnz, int *gindices, double *values, double *signal, double *noise, int nb_blocks,
+            int *block_sizes, int lambda, double *invtt, double tol, int maxiter, const char *outpath,
+            const char *ref, double *x_out, int *lstid_out, double *cond_out, int *hits_out, int cap) {
+    return ref_pcg_precond(m, nnz, gindices, values, signal, noise, nb_blocks, block_sizes, lambda, invtt, tol,
+                           maxiter, 0, 0, outpath, ref, x_out, lstid_out, cond_out, hits_out, cap);
 }
 
 /* ---- MLmap over forked ranks ---- */

@@ -263,6 +263,111 @@ def apply_bj(inv: np.ndarray, g: np.ndarray) -> np.ndarray:
     return out.reshape(-1)
 
 
+# --------------------------------------------------------------------------- two-level preconditioners
+EPS_2LVL = 1.0e-15  # precond.c:25
+
+
+def build_Z(A: Pointing, Zn: int) -> np.ndarray:
+    """build_Z (precond.c:791-938), one rank: the a-priori deflation columns.
+
+    The rows are split into Zn equal groups (m // Zn rows each, the rest left
+    out); count[g][i] counts local index i in group g and tcount[i] sums the
+    groups.  Column g holds, at the I entry i = 3q of every local pixel,
+    count_flat[g * group + i] / tcount[i] with count_flat the [group][lcount]
+    array flattened -- the reference's index (precond.c:878), kept as it is --
+    and zero at the Q and U entries; the trash entries are then dropped.
+    Returns Z as [Zn][n]."""
+    size = 1
+    group = Zn // size if Zn > size else 1
+    lc, nnz = A.lcount, A.nnz
+    per = (A.m // group) * nnz
+    count = np.zeros(group * lc, dtype=np.int64)
+    for g in range(group):
+        count[g * lc:(g + 1) * lc] = np.bincount(A.local[g * per:(g + 1) * per].astype(np.int64), minlength=lc)
+    tcount = count.reshape(group, lc).sum(axis=0)
+    Z = np.zeros((group * size, lc))
+    i = np.arange(0, lc, nnz)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        for g in range(group):
+            Z[g, i] = count[g * group + i].astype(np.float64) / tcount[i].astype(np.float64)
+    return Z[:, nnz * A.trash_pix:].copy()
+
+
+def build_AZ(op, Z: np.ndarray) -> np.ndarray:
+    """build_AZ (precond.c:1003-1024): AZ[i] = P^T N^-1 P Z[i]."""
+    return np.stack([op(z) for z in Z])
+
+
+def pinv_gelss(E: np.ndarray, rcond: float = EPS_2LVL) -> np.ndarray:
+    """inverse_svd_bis (precond.c:772-788): LAPACKE_dgelss(E, I) with rcond = eps,
+    the minimum-norm least-squares inverse; singular values <= rcond * s_max
+    count as zero."""
+    U, sv, Vt = np.linalg.svd(E)
+    keep = sv > rcond * sv[0] if sv.size else sv.astype(bool)
+    return (Vt[keep].T / sv[keep]) @ U[:, keep].T
+
+
+def build_Em1(Z: np.ndarray, AZ: np.ndarray) -> np.ndarray:
+    """build_Em1 (precond.c:951-1000), pixpond = 1: E[i][j] = sum_k Z[j][k] AZ[i][k],
+    then its dgelss pseudo-inverse."""
+    return pinv_gelss(AZ @ Z.T)
+
+
+def lanczos_eig(op, w0: np.ndarray, K: int):
+    """Lanczos_eig (precond.c:1028-1252), pixpond = 1: K Lanczos steps from
+    w0 = P^T N^-1 (b + noise - P x0), the K x K tridiagonal T, its eigenvectors Y
+    (dsyev) and the Ritz vectors Z = V Y, AZ = (A V) Y.
+
+    Kept as the reference does: the first three-term update subtracts
+    beta * vold with vold still zero (precond.c:1161,1196-1200), and a step
+    with beta <= eps leaves its Lanczos vector column zero and v unchanged.
+    The reference's last operator application (step K) only feeds entries
+    that its K x K truncation drops, so it is not made here."""
+    n = w0.size
+    beta = float(np.sqrt(np.dot(w0, w0)))
+    v = w0 / beta if beta > EPS_2LVL else np.zeros(n)
+    V = np.zeros((K + 1, n))
+    AV = np.zeros((K + 1, n))
+    V[0] = v
+    Av = op(v)
+    alpha = float(np.dot(v, Av))
+    AV[0] = Av
+    w = Av - alpha * v
+    vold = np.zeros(n)
+    T = np.zeros((K + 1, K + 1))
+    for i in range(K):
+        beta = float(np.sqrt(np.dot(w, w)))
+        if beta > EPS_2LVL:
+            v = w / beta
+            V[i + 1] = v
+        T[i, i], T[i, i + 1], T[i + 1, i] = alpha, beta, beta
+        if i == K - 1:
+            break
+        Av = op(v)
+        alpha = float(np.dot(v, Av))
+        AV[i + 1] = Av
+        w = Av - alpha * v - beta * vold
+        vold = v
+    _, Y = np.linalg.eigh(T[:K, :K])
+    return Y.T @ V[:K], Y.T @ AV[:K]
+
+
+@dataclass
+class TwoLevel:
+    Z: np.ndarray     # [Zn][n]
+    AZ: np.ndarray    # [Zn][n]
+    Em1: np.ndarray   # [Zn][Zn]
+
+
+def apply_2lvl(p: TwoLevel, inv: np.ndarray, g: np.ndarray) -> np.ndarray:
+    """apply_precond, precond 1/2 (precond.c:1412-1423; build_Qtx, mul_ZQtx at
+    :1026-1069): Qtx = Em1 Z^T g; Cg = BJ_inv (g - AZ Qtx) + Z Qtx."""
+    Qtx = p.Em1 @ (p.Z @ g)
+    Qg = p.Z.T @ Qtx
+    AQg = g - p.AZ.T @ Qtx
+    return apply_bj(inv, AQg) + Qg
+
+
 # --------------------------------------------------------------------------- PCG
 @dataclass
 class PCGResult:
@@ -273,10 +378,12 @@ class PCGResult:
 
 
 def pcg(gindices, values, signal, noise, block_sizes, lam, invtt, tol=1e-8, maxiter=500,
-        nnz: int = 3, exact_toeplitz: bool = False) -> PCGResult:
+        nnz: int = 3, exact_toeplitz: bool = False, precond: int = 0, z_2lvl: int = 0) -> PCGResult:
     """PCG_GLS_true (mappraiser/src/pcg_true.c:20-241), single rank (pixpond = 1):
-    Polak-Ribiere PCG on (P^T N^-1 P) x = P^T N^-1 (b + noise), block-Jacobi
-    preconditioner, stop when sum(g^2) <= tol^2 * sum(g0^2)."""
+    Polak-Ribiere PCG on (P^T N^-1 P) x = P^T N^-1 (b + noise), stop when
+    sum(g^2) <= tol^2 * sum(g0^2).  precond 0: block Jacobi; 1: two-level a
+    priori (build_Z); 2: two-level a posteriori (Lanczos_eig), with z_2lvl
+    deflation columns (0: one per rank, pcg_true.c:52)."""
     m = len(signal)
     A = local_shape(gindices, values, m, nnz)
     bj = precond_blockjacobi(A, signal, block_sizes, lam, invtt)
@@ -284,9 +391,23 @@ def pcg(gindices, values, signal, noise, block_sizes, lam, invtt, tol=1e-8, maxi
     n = A.n
     x = np.zeros(n)
     N = lambda v: stbmm(v, block_sizes, lam, invtt, exact=exact_toeplitz)  # noqa: E731
+    op = lambda v: trmatvec(A, N(matvec(A, v)))  # noqa: E731
     _g = bj.signal + noise - matvec(A, x)
     g = trmatvec(A, N(_g))
-    Cg = apply_bj(bj.inv, g)
+    Zn = z_2lvl if z_2lvl else 1
+    if precond == 0:
+        M = lambda r: apply_bj(bj.inv, r)  # noqa: E731
+    elif precond in (1, 2):
+        if precond == 1:
+            Z = build_Z(A, Zn)
+            AZ = build_AZ(op, Z)
+        else:
+            Z, AZ = lanczos_eig(op, g, Zn)
+        tl = TwoLevel(Z, AZ, build_Em1(Z, AZ))
+        M = lambda r: apply_2lvl(tl, bj.inv, r)  # noqa: E731
+    else:
+        raise ValueError(f"precond {precond}")
+    Cg = M(g)
     h = Cg.copy()
     g2pix = float(np.dot(Cg, g))
     res = float(np.dot(g, g))
@@ -304,7 +425,7 @@ def pcg(gindices, values, signal, noise, block_sizes, lam, invtt, tol=1e-8, maxi
         ro = g2pix / coeff
         x = x + ro * h
         g = gp - ro * AtNm1Ah
-        Cg = apply_bj(bj.inv, g)
+        Cg = M(g)
         g2pixp = g2pix
         g2pix = float(np.dot(Cg, g))
         g2pix_polak = float(np.dot(Cg, g - gp))

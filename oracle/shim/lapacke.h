@@ -7,8 +7,9 @@
  * are implemented in shim_lapacke.c as restatements of reference LAPACK's
  * unblocked algorithms (DGETF2, DGECON with DLACN2 / Higham 1988, DTRTI2 +
  * DGETRI) and are checked against scipy.linalg.lapack in the CPU tests.
- * dsyev/dgelss/dgesdd/dgesvd are only reached by the out-of-scope two-level
- * preconditioners and templates; they return an error.
+ * dsyev and dgelss (the two-level preconditioners, precond.c:770-1307) are
+ * restated with Jacobi methods in shim_lapacke.c; dgesdd/dgesvd are only
+ * reached by the out-of-scope templates and return an error.
  */
 #ifndef ORACLE_SHIM_LAPACKE_H
 #define ORACLE_SHIM_LAPACKE_H

@@ -1,6 +1,6 @@
 /*
- * Test-oracle restatement of the four LAPACK routines the block-Jacobi
- * preconditioner uses (see lapacke.h).  NOT product code.
+ * Test-oracle restatement of the LAPACK routines the block-Jacobi and the
+ * two-level preconditioners use (see lapacke.h).  NOT product code.
  *
  * Row-major calls are handled the way LAPACKE does: the logical matrix is
  * copied to column-major, the column-major algorithm runs, and the result is
@@ -295,21 +295,161 @@ lapack_int LAPACKE_dgetri(int layout, lapack_int n, double *a, lapack_int lda, c
 }
 
 static lapack_int unavailable(const char *name) {
-    fprintf(stderr, "shim %s: not available in the test oracle (two-level preconditioner / templates only)\n",
+    fprintf(stderr, "shim %s: not available in the test oracle (templates only)\n",
             name);
     return -1;
 }
 
-lapack_int LAPACKE_dsyev(int layout, char jobz, char uplo, lapack_int n, double *a, lapack_int lda, double *w) {
-    (void) layout, (void) jobz, (void) uplo, (void) n, (void) a, (void) lda, (void) w;
-    return unavailable("LAPACKE_dsyev");
+/*
+ * The two-level preconditioners (precond.c:791-1307) call dsyev('V','U') on
+ * the Lanczos tridiagonal matrix and dgelss on E = Z^T A Z (pseudo-inverse).
+ * Both are restated with Jacobi methods, which give the same eigen/singular
+ * decompositions as LAPACK's QR-based drivers up to rounding and the signs of
+ * the vectors (the preconditioners only depend on the spanned subspace):
+ *   dsyev  -> cyclic two-sided Jacobi (Golub & Van Loan, Matrix Computations,
+ *             4th ed., section 8.5), eigenvalues sorted ascending
+ *   dgelss -> one-sided Jacobi SVD (Hestenes 1958; Demmel & Veselic 1992),
+ *             minimum-norm solution with singular values <= rcond * s_max
+ *             treated as zero (rcond < 0: machine epsilon), as DGELSS
+ */
+static void jacobi_eig_cm(int n, double *a, double *v) {
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) CM(v, n, i, j) = (i == j) ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 100; sweep++) {
+        double off = 0.0, tot = 0.0;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                tot += CM(a, n, i, j) * CM(a, n, i, j);
+                if (i != j) off += CM(a, n, i, j) * CM(a, n, i, j);
+            }
+        if (off <= DBL_EPSILON * DBL_EPSILON * tot || off == 0.0) break;
+        for (int p = 0; p < n - 1; p++)
+            for (int q = p + 1; q < n; q++) {
+                double apq = CM(a, n, p, q);
+                if (apq == 0.0) continue;
+                double theta = (CM(a, n, q, q) - CM(a, n, p, p)) / (2.0 * apq);
+                double t     = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                for (int k = 0; k < n; k++) { /* A <- A J (columns p, q) */
+                    double akp = CM(a, n, k, p), akq = CM(a, n, k, q);
+                    CM(a, n, k, p) = c * akp - s * akq;
+                    CM(a, n, k, q) = s * akp + c * akq;
+                }
+                for (int k = 0; k < n; k++) { /* A <- J^T A (rows p, q) */
+                    double apk = CM(a, n, p, k), aqk = CM(a, n, q, k);
+                    CM(a, n, p, k) = c * apk - s * aqk;
+                    CM(a, n, q, k) = s * apk + c * aqk;
+                }
+                for (int k = 0; k < n; k++) {
+                    double vkp = CM(v, n, k, p), vkq = CM(v, n, k, q);
+                    CM(v, n, k, p) = c * vkp - s * vkq;
+                    CM(v, n, k, q) = s * vkp + c * vkq;
+                }
+            }
+    }
 }
+
+lapack_int LAPACKE_dsyev(int layout, char jobz, char uplo, lapack_int n, double *a, lapack_int lda, double *w) {
+    if (n <= 0) return 0;
+    double *c = malloc(sizeof(double) * (size_t) n * n), *v = malloc(sizeof(double) * (size_t) n * n);
+    int    *ord = malloc(sizeof(int) * (size_t) n);
+    to_cm(layout, n, n, a, lda, c);
+    const int up = (uplo == 'U' || uplo == 'u');
+    for (int j = 0; j < n; j++) /* symmetric from the referenced triangle */
+        for (int i = 0; i < n; i++)
+            if ((up && i > j) || (!up && i < j)) CM(c, n, i, j) = CM(c, n, j, i);
+    jacobi_eig_cm(n, c, v);
+    for (int i = 0; i < n; i++) ord[i] = i;
+    for (int i = 1; i < n; i++) /* insertion sort, ascending eigenvalues */
+        for (int k = i; k > 0 && CM(c, n, ord[k], ord[k]) < CM(c, n, ord[k - 1], ord[k - 1]); k--) {
+            int t = ord[k]; ord[k] = ord[k - 1]; ord[k - 1] = t;
+        }
+    double *out = malloc(sizeof(double) * (size_t) n * n);
+    for (int j = 0; j < n; j++) {
+        w[j] = CM(c, n, ord[j], ord[j]);
+        for (int i = 0; i < n; i++) CM(out, n, i, j) = (jobz == 'V' || jobz == 'v') ? CM(v, n, i, ord[j]) : 0.0;
+    }
+    if (jobz == 'V' || jobz == 'v') from_cm(layout, n, n, out, a, lda);
+    free(c), free(v), free(ord), free(out);
+    return 0;
+}
+
 lapack_int LAPACKE_dgelss(int layout, lapack_int m, lapack_int n, lapack_int nrhs, double *a, lapack_int lda,
                           double *b, lapack_int ldb, double *s, double rcond, lapack_int *rank) {
-    (void) layout, (void) m, (void) n, (void) nrhs, (void) a, (void) lda, (void) b, (void) ldb, (void) s,
-            (void) rcond, (void) rank;
-    return unavailable("LAPACKE_dgelss");
+    const int mb = m > n ? m : n;                       /* rows of b */
+    double   *u = malloc(sizeof(double) * (size_t) m * n), *v = malloc(sizeof(double) * (size_t) n * n);
+    double   *bc = calloc((size_t) mb * nrhs, sizeof(double)), *sv = malloc(sizeof(double) * (size_t) n);
+    double   *x = calloc((size_t) n * nrhs, sizeof(double));
+    int      *ord = malloc(sizeof(int) * (size_t) n);
+    to_cm(layout, m, n, a, lda, u);
+    for (int i = 0; i < m; i++)
+        for (int r = 0; r < nrhs; r++)
+            CM(bc, mb, i, r) = (layout == LAPACK_ROW_MAJOR) ? b[(size_t) i * ldb + r] : b[(size_t) r * ldb + i];
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) CM(v, n, i, j) = (i == j) ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 100; sweep++) {
+        int rotated = 0;
+        for (int p = 0; p < n - 1; p++)
+            for (int q = p + 1; q < n; q++) {
+                double al = 0.0, be = 0.0, ga = 0.0;
+                for (int k = 0; k < m; k++) {
+                    al += CM(u, m, k, p) * CM(u, m, k, p);
+                    be += CM(u, m, k, q) * CM(u, m, k, q);
+                    ga += CM(u, m, k, p) * CM(u, m, k, q);
+                }
+                if (ga == 0.0 || fabs(ga) <= DBL_EPSILON * sqrt(al * be)) continue;
+                rotated = 1;
+                double zeta = (be - al) / (2.0 * ga);
+                double t    = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                double c = 1.0 / sqrt(1.0 + t * t), sn = c * t;
+                for (int k = 0; k < m; k++) {
+                    double up = CM(u, m, k, p), uq = CM(u, m, k, q);
+                    CM(u, m, k, p) = c * up - sn * uq;
+                    CM(u, m, k, q) = sn * up + c * uq;
+                }
+                for (int k = 0; k < n; k++) {
+                    double vp = CM(v, n, k, p), vq = CM(v, n, k, q);
+                    CM(v, n, k, p) = c * vp - sn * vq;
+                    CM(v, n, k, q) = sn * vp + c * vq;
+                }
+            }
+        if (!rotated) break;
+    }
+    double smax = 0.0;
+    for (int j = 0; j < n; j++) {
+        double nn = 0.0;
+        for (int k = 0; k < m; k++) nn += CM(u, m, k, j) * CM(u, m, k, j);
+        sv[j] = sqrt(nn);
+        if (sv[j] > smax) smax = sv[j];
+    }
+    const double thr = (rcond < 0 ? DBL_EPSILON : rcond) * smax;
+    int          kept = 0;
+    for (int j = 0; j < n; j++) {
+        if (!(sv[j] > thr)) continue;
+        kept++;
+        for (int r = 0; r < nrhs; r++) { /* x += v_j (u_j^T b_r) / s_j^2 (u_j unnormalised) */
+            double d = 0.0;
+            for (int k = 0; k < m; k++) d += CM(u, m, k, j) * CM(bc, mb, k, r);
+            d /= sv[j] * sv[j];
+            for (int i = 0; i < n; i++) CM(x, n, i, r) += CM(v, n, i, j) * d;
+        }
+    }
+    for (int i = 0; i < n; i++) ord[i] = i;
+    for (int i = 1; i < n; i++) /* singular values in decreasing order */
+        for (int k = i; k > 0 && sv[ord[k]] > sv[ord[k - 1]]; k--) {
+            int t = ord[k]; ord[k] = ord[k - 1]; ord[k - 1] = t;
+        }
+    for (int j = 0; j < (m < n ? m : n); j++) s[j] = sv[ord[j]];
+    for (int i = 0; i < n; i++)
+        for (int r = 0; r < nrhs; r++) {
+            if (layout == LAPACK_ROW_MAJOR) b[(size_t) i * ldb + r] = CM(x, n, i, r);
+            else b[(size_t) r * ldb + i] = CM(x, n, i, r);
+        }
+    if (rank) *rank = kept;
+    free(u), free(v), free(bc), free(sv), free(x), free(ord);
+    return 0;
 }
+
 lapack_int LAPACKE_dgesdd(int layout, char jobz, lapack_int m, lapack_int n, double *a, lapack_int lda, double *s,
                           double *u, lapack_int ldu, double *vt, lapack_int ldvt) {
     (void) layout, (void) jobz, (void) m, (void) n, (void) a, (void) lda, (void) s, (void) u, (void) ldu,

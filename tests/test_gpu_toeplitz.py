@@ -149,3 +149,37 @@ def test_stbmm_split_plan_vs_exact(gpu_ctx, lam, sizes, plan):
     assert _rel(vout.cpu().numpy(), ref) < TOL
     ref32 = R.stbmm(v32.double().cpu().numpy(), np.array(sizes), lam, invtt, exact=True)
     assert _rel(o32.double().cpu().numpy(), ref32) < 1e-5
+
+
+def test_split_plans_of_two_operators_share_kernels(gpu_ctx):
+    """Two operators whose split plans launch the same column kernel with
+    different shared-memory sizes (256 x 512 and 256 x 256 points): the plan
+    built second must not break the launches of the first."""
+    import torch
+    import midapack_b200 as mb
+    ops = []
+    for lam, sizes, plan in [(16384, [140000], "s,8,9"), (8192, [70000], "s,8,8")]:
+        rng = np.random.default_rng(lam)
+        t = np.zeros(lam)
+        t[0] = 2.0
+        t[1:] = rng.standard_normal(lam - 1) * np.exp(-np.arange(1, lam) / (0.3 * lam))
+        os.environ["MDP_TOEPLITZ_PLAN"] = plan
+        os.environ["MDP_TOEPLITZ_PLAN32"] = plan
+        try:
+            N = mb.Noise(gpu_ctx, sizes, lam, np.tile(t, len(sizes)))
+            N.tile_fp32()
+        finally:
+            del os.environ["MDP_TOEPLITZ_PLAN"]
+            del os.environ["MDP_TOEPLITZ_PLAN32"]
+        ops.append((N, sizes, lam, np.tile(t, len(sizes))))
+    for N, sizes, lam, invtt in ops:
+        v = np.random.default_rng(lam + 1).standard_normal(int(sum(sizes)))
+        vin = torch.from_numpy(v).cuda()
+        vout = torch.empty_like(vin)
+        N.apply(vin, vout)
+        o32 = torch.empty(vin.shape, dtype=torch.float32, device="cuda")
+        N.apply_fp32(vin.float(), o32)
+        torch.cuda.synchronize()
+        ref = R.stbmm(v, np.array(sizes), lam, invtt, exact=True)
+        assert _rel(vout.cpu().numpy(), ref) < TOL
+        assert _rel(o32.double().cpu().numpy(), ref) < 1e-5

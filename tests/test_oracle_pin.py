@@ -96,3 +96,60 @@ def test_shim_lapack_vs_scipy(ref_lib):
                              ipiv.ctypes.data_as(ct.POINTER(ct.c_int)))
             inv, _ = lapack.dgetri(lu, piv)
             assert np.allclose(m, inv, rtol=1e-12, atol=1e-12 * np.abs(inv).max())
+
+
+def test_shim_dsyev_dgelss_vs_numpy(ref_lib):
+    """The shim's Jacobi dsyev / dgelss (two-level preconditioners) against
+    numpy's LAPACK: eigenvalues, eigenvectors up to sign, pseudo-inverse with
+    the rcond cut, rank."""
+    L = ct.CDLL(os.path.join(os.path.dirname(ref_lib.LIB_PATH), "libmidapack_ref_shims.so"))
+    dp = ct.POINTER(ct.c_double)
+    L.LAPACKE_dsyev.argtypes = [ct.c_int, ct.c_char, ct.c_char, ct.c_int, dp, ct.c_int, dp]
+    L.LAPACKE_dgelss.argtypes = [ct.c_int, ct.c_int, ct.c_int, ct.c_int, dp, ct.c_int, dp, ct.c_int, dp, ct.c_double,
+                                 ct.POINTER(ct.c_int)]
+    rng = np.random.default_rng(11)
+    for n in (1, 2, 5, 16, 40):
+        off = rng.standard_normal(n - 1)
+        t = np.diag(rng.uniform(1, 10, n)) + np.diag(off, 1) + np.diag(off, -1)  # a Lanczos-like tridiagonal matrix
+        a = np.ascontiguousarray(t.copy())
+        w = np.zeros(n)
+        assert L.LAPACKE_dsyev(101, b"V", b"U", n, a.ctypes.data_as(dp), n, w.ctypes.data_as(dp)) == 0
+        ev, ey = np.linalg.eigh(t)
+        assert np.allclose(w, ev, rtol=1e-12, atol=1e-12 * np.abs(ev).max())
+        assert np.allclose(np.abs(a.T @ ey), np.eye(n), atol=1e-10)  # same eigenvectors up to sign
+        # dgelss(E, I): full rank and rank deficient (one exact null direction)
+        for deficient in (False, True):
+            z = rng.standard_normal((n, n + 3))
+            e = z @ z.T
+            if deficient and n > 1:
+                v = rng.standard_normal(n)
+                e = e - np.outer(e @ v, e @ v) / (v @ e @ v)  # e v = 0
+            ea = np.ascontiguousarray(e.copy())
+            b = np.ascontiguousarray(np.eye(n))
+            s = np.zeros(n)
+            rank = ct.c_int()
+            assert L.LAPACKE_dgelss(101, n, n, n, ea.ctypes.data_as(dp), n, b.ctypes.data_as(dp), n,
+                                    s.ctypes.data_as(dp), 1e-10, ct.byref(rank)) == 0
+            sv = np.linalg.svd(e, compute_uv=False)
+            assert np.allclose(s, sv, rtol=1e-10, atol=1e-10 * sv[0])
+            assert rank.value == int((sv > 1e-10 * sv[0]).sum())
+            assert np.allclose(b, np.linalg.pinv(e, rcond=1e-10), rtol=1e-8, atol=1e-8 * np.abs(b).max())
+
+
+@pytest.mark.parametrize("case", ["gaps", "cut_gaps"])
+@pytest.mark.parametrize("precond,zn", [(1, 0), (1, 4), (1, 6), (2, 0), (2, 4), (2, 8)])
+def test_pcg_two_level(ref_lib, case, precond, zn):
+    """The two-level preconditioners: build_Z (with the reference's column
+    index), build_AZ, the dgelss pseudo-inverse of E, Lanczos_eig (with its
+    first three-term update), apply_precond; same iterations and residual
+    history as the compiled reference, maps within 1e-11."""
+    wl = solver_cases()[case]()
+    o = R.pcg(wl.pix, wl.weights, wl.signal, wl.noise, wl.block_sizes, wl.lam, wl.invtt, tol=1e-10, maxiter=400,
+              precond=precond, z_2lvl=zn)
+    xr, lst, cond, hits, res = ref_lib.pcg(wl.pix, wl.weights, wl.signal, wl.noise, wl.block_sizes, wl.lam, wl.invtt,
+                                           tol=1e-10, maxiter=400, precond=precond, z_2lvl=zn)
+    assert np.array_equal(o.bj.A.lindices[3 * o.bj.A.trash_pix:], lst)
+    assert o.iters == len(res) - 1
+    k = min(8, len(res))
+    assert np.allclose(o.res_rel[:k], res[:k], rtol=1e-8, atol=0)
+    assert _rel(o.x, xr) < 1e-11
