@@ -6,8 +6,10 @@
  *   mappraiser/include/mappraiser/precond.h:6-35       Precond, build_precond, apply_precond, free_precond,
  *                                                      precondblockjacobilike
  *   mappraiser/include/mappraiser/create_toeplitz.h    defineTpltz_avg, defineBlocks_avg
- * Scope: solver 0 (PCG) with precond 0 (block Jacobi) on one GPU.  Other
- * solver/precond values return an error (MLmap prints it and returns).
+ *   mappraiser/include/mappraiser/ecg.h:6-7            ECG_GLS
+ * Scope: solver 0 (PCG) with precond 0 (block Jacobi), 1 and 2 (two-level),
+ * solver 1 (ECG, block Jacobi), on one GPU.  Other solver/precond values
+ * return an error (MLmap prints it and returns).
  */
 #ifndef MDP_DROPIN_MAPPRAISER_H
 #define MDP_DROPIN_MAPPRAISER_H
@@ -57,11 +59,15 @@ void get_pixshare_pond(Mat *A, double *pixpond);
 /* pcg_true.c:578-600 */
 int  apply_weights(Tpltz *Nm1, double *tod);
 
-/* pcg_true.h:11-12 -> pcg_true.c:20-241 (precond 0) */
+/* pcg_true.h:11-12 -> pcg_true.c:20-241 (precond 0, 1, 2) */
 int PCG_GLS_true(char *outpath, char *ref, Mat *A, Tpltz *Nm1, double *x, double *b, double *noise, double *cond,
                  int *lhits, double tol, int K, int precond, int Z_2lvl);
 
-/* map.h:10-13 -> mappraiser.c:34-385 (solver 0, precond 0).  Writes the
+/* ecg.h:6-7 -> ecg.c:44-175 (enlarged CG; the preAlps iteration restated) */
+int ECG_GLS(char *outpath, char *ref, Mat *A, Tpltz *Nm1, double *x, double *b, double *noise, double *cond,
+            int *lhits, double tol, int maxIter, int enlFac, int ortho_alg, int bs_red);
+
+/* map.h:10-13 -> mappraiser.c:34-385 (solver 0 with precond 0, 1, 2; solver 1).  Writes the
  * I, Q, U, Cond and Hits maps (12*nside^2 entries each) to
  * outpath/{mapI,mapQ,mapU,Cond,Hits}_<ref>.fits as HEALPix binary tables. */
 void MLmap(MPI_Comm comm, char *outpath, char *ref, int solver, int precond, int Z_2lvl, int pointing_commflag,

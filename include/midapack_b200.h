@@ -160,6 +160,27 @@ int mdp_gls_solve(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const d
                   const double *d_noise, const mdp_solve_params *params, double *d_x, int32_t *d_lstid,
                   double *d_cond, int32_t *d_hits, double *h_res_rel, mdp_solve_info *info);
 
+/* ---- ECG solve (reference ECG_GLS, mappraiser/src/ecg.c:44-175, solver 1) ----
+ * Enlarged conjugate gradient with enl_fac search directions per iteration
+ * (the residual split over enl_fac contiguous ranges of the map's pixels),
+ * block-Jacobi preconditioner and rcond cut as mdp_gls_solve, Orthomin
+ * (ortho_alg 1) or Orthodir (ortho_alg 0) block recurrences, A-orthonormal
+ * blocks by Cholesky or, with bs_red = 1, by eigenvectors with the block
+ * shrinking when it loses rank; stops when ||r|| < tol ||r0||.  FP64.
+ * Outputs as mdp_gls_solve; h_res_rel (maxiter+1 entries) receives ||r||/||r0||. */
+#define MDP_ECG_MAX_ENL 64
+typedef struct {
+    double tol;
+    int    maxiter;
+    int    enl_fac;    /* 1..MDP_ECG_MAX_ENL */
+    int    ortho_alg;  /* 0: Orthodir, 1: Orthomin */
+    int    bs_red;     /* 1: adaptive block size */
+    int    verbose;
+} mdp_ecg_params;
+int mdp_ecg_solve(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *d_signal,
+                  const double *d_noise, const mdp_ecg_params *params, double *d_x, int32_t *d_lstid,
+                  double *d_cond, int32_t *d_hits, double *h_res_rel, mdp_solve_info *info);
+
 /* Mixed precision: the same solve as mdp_gls_solve (same preconditioner, cut
  * and stop test on the FP64 residual sum(g^2) <= tol^2 sum(g0^2)), computed as
  * FP64 iterative refinement.  Each step recomputes g = P^T N^-1 (d - P x) in

@@ -38,6 +38,11 @@ class SolveInfo(ct.Structure):
                 ("solve_seconds", ct.c_double), ("outer_iterations", ct.c_int), ("fp64_applications", ct.c_int)]
 
 
+class ECGParams(ct.Structure):
+    _fields_ = [("tol", ct.c_double), ("maxiter", ct.c_int), ("enl_fac", ct.c_int), ("ortho_alg", ct.c_int),
+                ("bs_red", ct.c_int), ("verbose", ct.c_int)]
+
+
 class MultiParams(ct.Structure):
     _fields_ = [("tol", ct.c_double), ("maxiter", ct.c_int), ("inner_tol", ct.c_double), ("inner_maxiter", ct.c_int),
                 ("slots", ct.c_int), ("use_graph", ct.c_int), ("verbose", ct.c_int)]
@@ -105,6 +110,9 @@ _SIGS = {
     "mdp_gls_solve_mixed": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                        ct.POINTER(SolveParams), ct.c_double, ct.c_int, ct.c_void_p, ct.c_void_p,
                                        ct.c_void_p, ct.c_void_p, c_f64p, ct.POINTER(SolveInfo)]),
+    "mdp_ecg_solve": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                 ct.POINTER(ECGParams), ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                 c_f64p, ct.POINTER(SolveInfo)]),
     # reference-compatible host API (include/mapmat.h, toeplitz.h, mappraiser.h)
     "MatInit": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, c_i32p, c_f64p, ct.c_int, ct.c_int]),
     "MatSetIndices": (None, [ct.c_void_p, ct.c_int, ct.c_int, c_i32p]),
@@ -131,6 +139,8 @@ _SIGS = {
     "get_pixshare_pond": (None, [ct.c_void_p, c_f64p]),
     "PCG_GLS_true": (ct.c_int, [ct.c_char_p, ct.c_char_p, ct.c_void_p, ct.c_void_p, c_f64p, c_f64p, c_f64p, c_f64p,
                                 c_i32p, ct.c_double, ct.c_int, ct.c_int, ct.c_int]),
+    "ECG_GLS": (ct.c_int, [ct.c_char_p, ct.c_char_p, ct.c_void_p, ct.c_void_p, c_f64p, c_f64p, c_f64p, c_f64p,
+                           c_i32p, ct.c_double, ct.c_int, ct.c_int, ct.c_int, ct.c_int]),
     "MLmap": (None, [ct.c_int, ct.c_char_p, ct.c_char_p, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_double,
                      ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int, c_i32p, ct.c_int, c_i32p, ct.c_int, c_i32p,
                      c_f64p, c_f64p, c_f64p, ct.c_int, c_f64p]),
@@ -364,6 +374,27 @@ def gls_solve_mixed(ctx: Context, A: Pointing, N: Noise, signal, noise, tol=1e-8
           "mdp_gls_solve_mixed")
     n = info.n_map
     return x[:n], lst[:n], cond[:n // 3], hits[:n // 3], res[:info.outer_iterations + 1], info
+
+
+def gls_solve_ecg(ctx: Context, A: Pointing, N: Noise, signal, noise, tol=1e-8, maxiter=500, enl_fac=4,
+                  ortho_alg=1, bs_red=0, verbose=False):
+    """ECG_GLS on device tensors: enlarged CG with enl_fac search directions (ortho_alg 1: Orthomin,
+    0: Orthodir; bs_red 1: adaptive block size).  Returns (x, lstid, cond, hits, res_rel, info)."""
+    import torch
+    n0 = A.shape()["n_map"]
+    x = torch.empty(max(n0, 1), dtype=torch.float64, device="cuda")
+    lst = torch.empty(max(n0, 1), dtype=torch.int32, device="cuda")
+    cond = torch.empty(max(n0 // 3, 1), dtype=torch.float64, device="cuda")
+    hits = torch.empty(max(n0 // 3, 1), dtype=torch.int32, device="cuda")
+    res = np.zeros(maxiter + 1)
+    prm = ECGParams(tol, maxiter, enl_fac, ortho_alg, bs_red, 1 if verbose else 0)
+    info = SolveInfo()
+    check(lib().mdp_ecg_solve(ctx.h, A.h, N.h, ct.c_void_p(_ptr(signal)), ct.c_void_p(_ptr(noise)), ct.byref(prm),
+                              ct.c_void_p(x.data_ptr()), ct.c_void_p(lst.data_ptr()), ct.c_void_p(cond.data_ptr()),
+                              ct.c_void_p(hits.data_ptr()), res.ctypes.data_as(c_f64p), ct.byref(info)),
+          "mdp_ecg_solve")
+    n = info.n_map
+    return x[:n], lst[:n], cond[:n // 3], hits[:n // 3], res[:info.iterations + 1], info
 
 
 def gls_solve_multi(ctx: Context, A: Pointing, N: Noise, noise, signal=None, signal_col=-1, tol=1e-8, maxiter=500,

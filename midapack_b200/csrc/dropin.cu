@@ -674,6 +674,60 @@ extern "C" int PCG_GLS_true(char *outpath, char *ref, Mat *A, Tpltz *Nm1, double
     return 0;
 }
 
+// ECG_GLS (ecg.c:44-175): block-Jacobi preconditioner with the cut mirrored on
+// the host Mat and b, then the enlarged CG on the device; x receives the
+// solution, cond/lhits the kept pixels' rcond and hits, and
+// <outpath>/rel_res_<ref>_enlfac_<t>_o=<ortho_alg>.txt the relative residuals.
+extern "C" int ECG_GLS(char *outpath, char *ref, Mat *A, Tpltz *Nm1, double *x, double *b, double *noise,
+                       double *cond, int *lhits, double tol, int maxIter, int enlFac, int ortho_alg, int bs_red) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    mdp_context                *ctx = default_ctx();
+    MatDev                     *D = mat_dev(A);
+    mdp_noise                  *N;
+    int                         rc;
+    if (!D || !ctx) return fail("ECG_GLS", MDP_EINVAL);
+    if (enlFac < 1 || enlFac > MDP_ECG_MAX_ENL) {
+        mdp_set_error("ECG_GLS: enlFac must be in 1..%d", MDP_ECG_MAX_ENL);
+        return fail("ECG_GLS", MDP_EINVAL);
+    }
+    if ((rc = noise_for(Nm1, &N))) return fail("ECG_GLS", rc);
+    const int64_t m = A->m;
+    BJState       bj;
+    if ((rc = mdp_bj_build(ctx, D->P, N, &bj))) return fail("ECG_GLS", rc);
+    if (bj.ncut > 0 && (rc = mirror_cut_to_host(ctx, A, D, b))) return fail("ECG_GLS", rc);
+    if (A->id_last_pix) free(A->id_last_pix);
+    if (A->ll) free(A->ll);
+    A->id_last_pix = nullptr;
+    A->ll = nullptr;
+    DevBuf        db, dn, dx;
+    const int64_t nmap = D->P->n_map();
+    if ((rc = db.alloc(8 * m)) || (rc = dn.alloc(8 * m)) || (rc = dx.alloc(8 * std::max<int64_t>(nmap, 1))))
+        return fail("ECG_GLS", rc);
+    cudaMemcpyAsync(db.p, b, 8 * m, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(dn.p, noise, 8 * m, cudaMemcpyHostToDevice, ctx->stream);
+    mdp_ecg_params      prm = {tol, maxIter, enlFac, ortho_alg, bs_red, 0};
+    mdp_solve_info      info = {};
+    std::vector<double> res(std::max(maxIter, 1) + 1, 0.0);
+    rc = mdp_ecg_run(ctx, D->P, N, bj.inv.as<double>(), bj.npix, db.as<double>(), dn.as<double>(), &prm,
+                     dx.as<double>(), res.data(), &info);
+    if (rc) return fail("ECG_GLS", rc);
+    cudaMemcpy(x, dx.p, 8 * 3 * bj.npix, cudaMemcpyDeviceToHost);
+    cudaMemcpy(cond, bj.rcond.p, 8 * bj.npix, cudaMemcpyDeviceToHost);
+    cudaMemcpy(lhits, bj.hits.p, 4 * bj.npix, cudaMemcpyDeviceToHost);
+    printf("*** ECG: %d iterations, relative residual %e (%s)\n", info.iterations, std::sqrt(info.res / info.res0),
+           info.converged ? "converged" : "not converged");
+    if (outpath && ref) {
+        char fn[4096];
+        snprintf(fn, sizeof(fn), "%s/rel_res_%s_enlfac_%d_o=%d.txt", outpath, ref, enlFac, ortho_alg);
+        FILE *f = fopen(fn, "w");
+        if (f) {
+            for (int i = 0; i <= info.iterations; i++) fprintf(f, "%.15e\n", res[i]);
+            fclose(f);
+        }
+    }
+    return 0;
+}
+
 // ------------------------------------------------------------------ MLmap
 // x2map_pol (mappraiser.c:836-853)
 static void x2map(double *mapI, double *mapQ, double *mapU, double *Cond, int *Hits, const double *x, const int *lstid,
@@ -695,7 +749,8 @@ static void x2map(double *mapI, double *mapQ, double *mapU, double *Cond, int *H
 
 static int mlmap_device(int m, int nb, const int *blocks, const int *pix, const double *w, const double *sig,
                         const double *noi, int lambda, const double *invtt, double tol, int maxiter, int verbose,
-                        int precond, int z_2lvl, std::vector<double> &x, std::vector<int> &lstid, std::vector<double> &cond,
+                        int precond, int z_2lvl, int solver, int enl_fac, int ortho_alg, int bs_red,
+                        std::vector<double> &x, std::vector<int> &lstid, std::vector<double> &cond,
                         std::vector<int> &hits, int *iters, double *res_rel) {
     mdp_context *ctx = default_ctx();
     if (!ctx) return MDP_ECUDA;
@@ -734,8 +789,14 @@ static int mlmap_device(int m, int nb, const int *blocks, const int *pix, const 
     mdp_solve_params    prm = {tol, maxiter, verbose, precond, z_2lvl};
     mdp_solve_info      info = {};
     std::vector<double> res(std::max(maxiter, 1) + 1, 0.0);
-    rc = mdp_gls_solve(ctx, P, N, ds.as<double>(), dn.as<double>(), &prm, dx.as<double>(), dl.as<int32_t>(),
-                       dc.as<double>(), dh.as<int32_t>(), res.data(), &info);
+    if (solver == 1) {
+        mdp_ecg_params eprm = {tol, maxiter, enl_fac, ortho_alg, bs_red, verbose};
+        rc = mdp_ecg_solve(ctx, P, N, ds.as<double>(), dn.as<double>(), &eprm, dx.as<double>(), dl.as<int32_t>(),
+                           dc.as<double>(), dh.as<int32_t>(), res.data(), &info);
+    } else {
+        rc = mdp_gls_solve(ctx, P, N, ds.as<double>(), dn.as<double>(), &prm, dx.as<double>(), dl.as<int32_t>(),
+                           dc.as<double>(), dh.as<int32_t>(), res.data(), &info);
+    }
     if (!rc) {
         const int64_t n = info.n_map;
         x.resize(n);
@@ -821,9 +882,9 @@ extern "C" void MLmap(MPI_Comm comm, char *outpath, char *ref, int solver, int p
                       int pointing_commflag, double tol, int maxiter, int enlFac, int ortho_alg, int bs_red, int nside,
                       void *data_size_proc, int nb_blocks_loc, void *local_blocks_sizes, int Nnz, void *pix,
                       void *pixweights, void *signal, double *noise, int lambda, double *invtt) {
-    (void) comm, (void) pointing_commflag, (void) enlFac, (void) ortho_alg, (void) bs_red;
-    if (solver != 0 || precond < 0 || precond > 2 || Nnz != 3) {
-        fprintf(stderr, "midapack_b200 MLmap: only solver 0 (PCG), precond 0, 1, 2 and Nnz 3 are available\n");
+    (void) comm, (void) pointing_commflag;
+    if (solver < 0 || solver > 1 || precond < 0 || precond > 2 || Nnz != 3 || (solver == 1 && precond != 0)) {
+        fprintf(stderr, "midapack_b200 MLmap: solver 0 (PCG, precond 0, 1, 2) or 1 (ECG, block Jacobi) with Nnz 3\n");
         return;
     }
     const int m = ((int *) data_size_proc)[0];
@@ -837,7 +898,7 @@ extern "C" void MLmap(MPI_Comm comm, char *outpath, char *ref, int solver, int p
         std::lock_guard<std::mutex> lk(g_mu);
         rc = mlmap_device(m, nb_blocks_loc, (const int *) local_blocks_sizes, (const int *) pix,
                           (const double *) pixweights, (const double *) signal, noise, lambda, invtt, tol, maxiter, 1,
-                          precond, Z_2lvl, x, lstid, cond, hits, &it, &rr);
+                          precond, Z_2lvl, solver, enlFac, ortho_alg, bs_red, x, lstid, cond, hits, &it, &rr);
     }
     if (rc) {
         fail("MLmap", rc);
@@ -862,8 +923,8 @@ extern "C" int MLmap_b200(int solver, int precond, double tol, int maxiter, int 
                           const int *local_blocks_sizes, int Nnz, const int *pix, const double *pixweights,
                           const double *signal, const double *noise, int lambda, const double *invtt, double *mapI,
                           double *mapQ, double *mapU, double *Cond, int *Hits, int *iterations, double *res_rel) {
-    if (solver != 0 || precond < 0 || precond > 2 || Nnz != 3) {
-        mdp_set_error("MLmap_b200: only solver 0, precond 0, 1, 2 and Nnz 3 are available");
+    if (solver < 0 || solver > 1 || precond < 0 || precond > 2 || Nnz != 3 || (solver == 1 && precond != 0)) {
+        mdp_set_error("MLmap_b200: solver 0 (PCG, precond 0, 1, 2) or 1 (ECG with enlFac 1, block Jacobi), Nnz 3");
         return MDP_EUNSUPPORTED;
     }
     std::vector<double> x, cond;
@@ -872,7 +933,7 @@ extern "C" int MLmap_b200(int solver, int precond, double tol, int maxiter, int 
     {
         std::lock_guard<std::mutex> lk(g_mu);
         rc = mlmap_device(m, nb_blocks_loc, local_blocks_sizes, pix, pixweights, signal, noise, lambda, invtt, tol,
-                          maxiter, 0, precond, 0, x, lstid, cond, hits, iterations, res_rel);
+                          maxiter, 0, precond, 0, solver, 1, 1, 0, x, lstid, cond, hits, iterations, res_rel);
     }
     if (rc) return rc;
     const int64_t npix = 12LL * nside * nside;

@@ -211,6 +211,9 @@ int mdp_apply_op_impl(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, con
 int mdp_gls_rhs(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *d_signal, const double *d_noise,
                 double *d_g);
 int mdp_bj_build(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, BJState *bj);
+int mdp_ecg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *inv, int64_t npix,
+                const double *d_signal, const double *d_noise, const mdp_ecg_params *prm, double *d_x,
+                double *h_res_rel, mdp_solve_info *info);
 int mdp_bj_cached(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const BJState **bj);
 int mdp_pcg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *inv, int64_t npix,
                 const double *d_signal, const double *d_noise, const mdp_solve_params *params, double *d_x,

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "mdp_internal.cuh"
+#include "smalldense.h"
 
 namespace {
 
@@ -182,111 +183,6 @@ __global__ void ritz_kernel(const double *__restrict__ V, const double *__restri
     }
 }
 
-// ------------------------------------------------------------ host dense algebra
-// Cyclic two-sided Jacobi eigen-decomposition of the symmetric K x K matrix a
-// (row-major, destroyed): eigenvalues ascending in w, eigenvectors as the
-// columns of y (row-major).  Golub & Van Loan, Matrix Computations 4th ed., 8.5.
-void jacobi_eigh(int K, std::vector<double> &a, std::vector<double> &w, std::vector<double> &y) {
-    std::vector<double> v((size_t) K * K, 0.0);
-    for (int i = 0; i < K; i++) v[(size_t) i * K + i] = 1.0;
-    auto A = [&](int i, int j) -> double & { return a[(size_t) i * K + j]; };
-    for (int sweep = 0; sweep < 100; sweep++) {
-        double off = 0.0, tot = 0.0;
-        for (int i = 0; i < K; i++)
-            for (int j = 0; j < K; j++) {
-                tot += A(i, j) * A(i, j);
-                if (i != j) off += A(i, j) * A(i, j);
-            }
-        if (off == 0.0 || off <= DBL_EPSILON * DBL_EPSILON * tot) break;
-        for (int p = 0; p < K - 1; p++)
-            for (int q = p + 1; q < K; q++) {
-                const double apq = A(p, q);
-                if (apq == 0.0) continue;
-                const double theta = (A(q, q) - A(p, p)) / (2.0 * apq);
-                const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-                const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
-                for (int k = 0; k < K; k++) {
-                    const double akp = A(k, p), akq = A(k, q);
-                    A(k, p) = c * akp - s * akq;
-                    A(k, q) = s * akp + c * akq;
-                }
-                for (int k = 0; k < K; k++) {
-                    const double apk = A(p, k), aqk = A(q, k);
-                    A(p, k) = c * apk - s * aqk;
-                    A(q, k) = s * apk + c * aqk;
-                }
-                for (int k = 0; k < K; k++) {
-                    const double vkp = v[(size_t) k * K + p], vkq = v[(size_t) k * K + q];
-                    v[(size_t) k * K + p] = c * vkp - s * vkq;
-                    v[(size_t) k * K + q] = s * vkp + c * vkq;
-                }
-            }
-    }
-    std::vector<int> ord(K);
-    for (int i = 0; i < K; i++) ord[i] = i;
-    std::stable_sort(ord.begin(), ord.end(), [&](int x, int z) { return A(x, x) < A(z, z); });
-    w.assign(K, 0.0);
-    y.assign((size_t) K * K, 0.0);
-    for (int j = 0; j < K; j++) {
-        w[j] = A(ord[j], ord[j]);
-        for (int i = 0; i < K; i++) y[(size_t) i * K + j] = v[(size_t) i * K + ord[j]];
-    }
-}
-
-// Pseudo-inverse of the n x n matrix e (row-major) as DGELSS(e, I) computes
-// it: the minimum-norm least-squares solution, singular values <= rcond *
-// s_max treated as zero.  One-sided Jacobi SVD (Hestenes 1958; Demmel &
-// Veselic, SIAM J. Matrix Anal. Appl. 13:1204, 1992) on the columns of e.
-std::vector<double> pinv_gelss(int n, const std::vector<double> &e, double rcond) {
-    std::vector<double> u(e), v((size_t) n * n, 0.0), out((size_t) n * n, 0.0), sv(n);
-    auto U = [&](int i, int j) -> double & { return u[(size_t) i * n + j]; };
-    auto Vm = [&](int i, int j) -> double & { return v[(size_t) i * n + j]; };
-    for (int i = 0; i < n; i++) Vm(i, i) = 1.0;
-    for (int sweep = 0; sweep < 100; sweep++) {
-        bool rotated = false;
-        for (int p = 0; p < n - 1; p++)
-            for (int q = p + 1; q < n; q++) {
-                double al = 0.0, be = 0.0, ga = 0.0;
-                for (int k = 0; k < n; k++) {
-                    al += U(k, p) * U(k, p);
-                    be += U(k, q) * U(k, q);
-                    ga += U(k, p) * U(k, q);
-                }
-                if (ga == 0.0 || std::fabs(ga) <= DBL_EPSILON * std::sqrt(al * be)) continue;
-                rotated = true;
-                const double zeta = (be - al) / (2.0 * ga);
-                const double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
-                const double c = 1.0 / std::sqrt(1.0 + t * t), s = c * t;
-                for (int k = 0; k < n; k++) {
-                    const double up = U(k, p), uq = U(k, q);
-                    U(k, p) = c * up - s * uq;
-                    U(k, q) = s * up + c * uq;
-                }
-                for (int k = 0; k < n; k++) {
-                    const double vp = Vm(k, p), vq = Vm(k, q);
-                    Vm(k, p) = c * vp - s * vq;
-                    Vm(k, q) = s * vp + c * vq;
-                }
-            }
-        if (!rotated) break;
-    }
-    double smax = 0.0;
-    for (int j = 0; j < n; j++) {
-        double nn = 0.0;
-        for (int k = 0; k < n; k++) nn += U(k, j) * U(k, j);
-        sv[j] = std::sqrt(nn);
-        smax = std::max(smax, sv[j]);
-    }
-    // e = sum_j (u_j / s_j) s_j v_j^T  =>  e^+ = sum_j v_j u_j^T / s_j^2 over the kept j
-    for (int j = 0; j < n; j++) {
-        if (!(sv[j] > rcond * smax)) continue;
-        const double s2 = sv[j] * sv[j];
-        for (int r = 0; r < n; r++)
-            for (int c = 0; c < n; c++) out[(size_t) r * n + c] += Vm(r, j) * U(c, j) / s2;
-    }
-    return out;
-}
-
 // deterministic dot product on the device, read back to the host
 int dot_host(mdp_context *ctx, const double *a, const double *b, int64_t n, DevBuf &part, double *out) {
     MDP_TRY(part.alloc(8 * (MDP_TL_BLOCKS + 1)));
@@ -422,7 +318,7 @@ int mdp_twolevel_build(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, in
         }
         T[(size_t) (K - 1) * K + K - 1] = alpha;
         std::vector<double> ev, Y;
-        jacobi_eigh(K, T, ev, Y);
+        mdp_dense::jacobi_eigh(K, T, ev, Y);
         MDP_TRY(ritz(ctx, V, Y, K, n, Z));
         MDP_TRY(ritz(ctx, AV, Y, K, n, AZ));
     }
@@ -444,7 +340,7 @@ int mdp_twolevel_build(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, in
             mdp_set_error("two-level preconditioner: E = Z^T A Z is not finite");
             return MDP_ENAN;
         }
-    tl->h_Em1 = pinv_gelss(zn, E, EPS_2LVL);
+    tl->h_Em1 = mdp_dense::pinv_gelss(zn, E, EPS_2LVL);
     MDP_CUDA(cudaMemcpyAsync(tl->Em1.p, tl->h_Em1.data(), 8 * (size_t) zn * zn, cudaMemcpyHostToDevice, st));
     MDP_CUDA(cudaStreamSynchronize(st));
     return MDP_OK;

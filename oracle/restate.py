@@ -439,6 +439,106 @@ def pcg(gindices, values, signal, noise, block_sizes, lam, invtt, tol=1e-8, maxi
     return PCGResult(x, k, res_rel, bj)
 
 
+# --------------------------------------------------------------------------- ECG
+def ecg_split(r: np.ndarray, t: int) -> np.ndarray:
+    """The enlarged residual T(r): column j keeps the entries of the j-th of t
+    contiguous ranges of the map's pixels (unknowns sorted by global index,
+    pixel triples kept together), zero elsewhere.  Returns [t][n]."""
+    n = r.size
+    npix = n // 3
+    col = (np.arange(n) // 3) * t // max(npix, 1)
+    R = np.zeros((t, n))
+    R[col, np.arange(n)] = r
+    return R
+
+
+def a_orthonormalize(P: np.ndarray, AP: np.ndarray, bs_red: bool, tol: float = 1e-12):
+    """P <- P G^{-1/2}-like factor with G = P^T A P: the Cholesky factor
+    G = L L^T gives P L^-T (bs unchanged); with bs_red a rank-revealing
+    eigen-decomposition G = V diag(l) V^T keeps the directions with
+    l > tol * max(l) and scales them to l^-1/2 (the block size may shrink).
+    Returns (P, AP) with P^T A P = I."""
+    G = P @ AP.T
+    G = 0.5 * (G + G.T)
+    if not bs_red:
+        L = np.linalg.cholesky(G)
+        Li = np.linalg.inv(L)
+        return Li @ P, Li @ AP
+    lam, V = np.linalg.eigh(G)
+    keep = lam > tol * lam.max()
+    F = V[:, keep] / np.sqrt(lam[keep])
+    return F.T @ P, F.T @ AP
+
+
+@dataclass
+class ECGResult:
+    x: np.ndarray
+    iters: int
+    res_rel: list
+    bs: list
+    bj: BJResult
+
+
+def ecg(gindices, values, signal, noise, block_sizes, lam, invtt, tol=1e-8, maxiter=500, enl=4, ortho_alg=1,
+        bs_red=0, nnz: int = 3) -> ECGResult:
+    """ECG_GLS (mappraiser/src/ecg.c:44-175) with the enlarged conjugate
+    gradient of preAlps (absent here; restated from Grigori, Moufawad & Nataf,
+    SIAM J. Matrix Anal. Appl. 37:744, 2016, and Grigori & Tissot, "Reducing
+    the communication and computational costs of enlarged Krylov subspaces
+    conjugate gradient", Numer. Algorithms 80:1333, 2019), one rank:
+
+      R_0 = T(r_0), P_1 = M^-1 R_0, A-orthonormalised
+      k = 1, 2, ...: alpha = P^T R; X += P alpha; R -= AP alpha;
+        stop when ||sum_j R_j|| < tol ||r_0|| (ecg.c:131-136);
+        Orthomin (ortho_alg 1): Z = M^-1 R, P <- Z - P (AP^T Z);
+        Orthodir (ortho_alg 0): Z = M^-1 AP, P <- Z - P (AP^T Z) - P_prev (AP_prev^T Z);
+        AP = A P, A-orthonormalise (bs_red: rank-revealing, the block may shrink)
+      x = sum_j X_j.
+    M is the block-Jacobi preconditioner with the rcond cut (ecg.c:67)."""
+    m = len(signal)
+    A = local_shape(gindices, values, m, nnz)
+    bj = precond_blockjacobi(A, signal, block_sizes, lam, invtt)
+    A = bj.A
+    n = A.n
+    N = lambda v: stbmm(v, block_sizes, lam, invtt)  # noqa: E731
+    op = lambda v: trmatvec(A, N(matvec(A, v)))  # noqa: E731
+    Mi = lambda V: np.stack([apply_bj(bj.inv, v) for v in V])  # noqa: E731
+    opb = lambda V: np.stack([op(v) for v in V])  # noqa: E731
+    r0 = trmatvec(A, N(bj.signal + noise))
+    normb = float(np.sqrt(np.dot(r0, r0)))
+    R = ecg_split(r0, enl)
+    X = np.zeros((enl, n))
+    P = Mi(R)
+    AP = opb(P)
+    P, AP = a_orthonormalize(P, AP, bool(bs_red))
+    Pp = APp = None
+    res_rel = [1.0]
+    bs = [P.shape[0]]
+    it = 0
+    while it < maxiter:
+        alpha = P @ R.T                      # [bs][t]
+        X = X + alpha.T @ P
+        R = R - alpha.T @ AP
+        it += 1
+        r = R.sum(axis=0)
+        res = float(np.sqrt(np.dot(r, r)))
+        res_rel.append(res / normb)
+        if res < tol * normb:
+            break
+        if ortho_alg == 1:
+            Z = Mi(R)
+            Pn = Z - (AP @ Z.T).T @ P
+        else:
+            Z = Mi(AP)
+            Pn = Z - (AP @ Z.T).T @ P
+            if Pp is not None:
+                Pn = Pn - (APp @ Z.T).T @ Pp
+            Pp, APp = P, AP
+        P, AP = a_orthonormalize(Pn, opb(Pn), bool(bs_red))
+        bs.append(P.shape[0])
+    return ECGResult(X.sum(axis=0), it, res_rel, bs, bj)
+
+
 def x2map_pol(x, lstid, cond, hits, npix):
     """x2map_pol (mappraiser/src/mappraiser.c:836-853)."""
     mapI = np.zeros(npix)

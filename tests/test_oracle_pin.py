@@ -153,3 +153,27 @@ def test_pcg_two_level(ref_lib, case, precond, zn):
     k = min(8, len(res))
     assert np.allclose(o.res_rel[:k], res[:k], rtol=1e-8, atol=0)
     assert _rel(o.x, xr) < 1e-11
+
+
+@pytest.mark.parametrize("case", ["gaps", "cut_gaps"])
+@pytest.mark.parametrize("enl,ortho,bs_red", [(1, 1, 0), (4, 1, 0), (8, 1, 1), (16, 1, 1)])
+def test_ecg_restatement_solves_the_reference_system(ref_lib, case, enl, ortho, bs_red):
+    """ECG's iteration comes from preAlps, which the reference does not ship:
+    the restated enlarged CG is pinned through the solution, which is unique
+    on the determined pixels -- it must equal the compiled reference's PCG
+    map (tol 1e-12) within 1e-8, with the same pixels."""
+    wl = solver_cases()[case]()
+    e = R.ecg(wl.pix, wl.weights, wl.signal, wl.noise, wl.block_sizes, wl.lam, wl.invtt, tol=1e-10, maxiter=800,
+              enl=enl, ortho_alg=ortho, bs_red=bs_red)
+    xr, lst, cond, hits, res = ref_lib.pcg(wl.pix, wl.weights, wl.signal, wl.noise, wl.block_sizes, wl.lam,
+                                           wl.invtt, tol=1e-12, maxiter=800)
+    assert e.res_rel[-1] < 1e-10
+    assert np.array_equal(e.bj.A.lindices[3 * e.bj.A.trash_pix:], lst)
+    det = np.ones(len(xr), dtype=bool)
+    if case == "cut_gaps":  # the rewritten pixel of the cut is an exact null direction
+        W, _ = R.local_W(e.bj.A, wl.block_sizes, wl.lam, wl.invtt)
+        ev = np.linalg.eigvalsh(W)
+        det = np.repeat(ev[:, 0] > 1e-6 * ev[:, 2], 3)
+    for k in range(3):
+        s = det[k::3]
+        assert _rel(e.x[k::3][s], xr[k::3][s]) < 1e-8
