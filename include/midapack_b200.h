@@ -99,6 +99,10 @@ int  mdp_noise_tile(const mdp_noise *N, int *fft_size, int *cluster_ctas, int64_
 int  mdp_stbmm_fp32(mdp_context *ctx, mdp_noise *N, const float *d_in, float *d_out);
 /* FP32 tile plan (builds it on first use) */
 int  mdp_noise_tile_fp32(mdp_context *ctx, mdp_noise *N, int *fft_size, int *cluster_ctas, int64_t *n_tiles);
+/* No counterpart in the reference.  Builds the FP32 operator state of the
+ * mixed-precision solves ahead of them (FP32 weights of A, FP32 tile plan and
+ * spectra of N), which they otherwise build on first use. */
+int  mdp_prepare_fp32(mdp_context *ctx, mdp_pointing *A, mdp_noise *N);
 /* Launch shape of a tile plan (fp32 = 0: FP64 tiles, 1: FP32 tiles, built on
  * first use): 2^log2_cta_points complex points per CTA, CTAs per cluster,
  * threads per CTA, and whether the autotuner picked it (1) by timing the

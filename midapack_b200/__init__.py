@@ -88,6 +88,7 @@ _SIGS = {
     "mdp_stbmm": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "mdp_stbmm_noalloc": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "mdp_stbmm_fp32": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mdp_prepare_fp32": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "mdp_noise_tile_fp32": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int),
                                        ct.POINTER(ct.c_int64)]),
     "mdp_noise_tile": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int), ct.POINTER(ct.c_int64)]),
@@ -353,6 +354,12 @@ def gls_solve(ctx: Context, A: Pointing, N: Noise, signal, noise, tol=1e-8, maxi
           "mdp_gls_solve")
     n = info.n_map
     return x[:n], lst[:n], cond[:n // 3], hits[:n // 3], res[:info.iterations + 1], info
+
+
+def prepare_fp32(ctx: Context, A: Pointing, N: Noise):
+    """Builds the FP32 operator state of the mixed-precision solves (FP32 weights, FP32 tile plan and
+    spectra) ahead of the solve."""
+    check(lib().mdp_prepare_fp32(ctx.h, A.h, N.h), "mdp_prepare_fp32")
 
 
 def gls_solve_mixed(ctx: Context, A: Pointing, N: Noise, signal, noise, tol=1e-8, maxiter=500, inner_tol=1e-4,

@@ -85,7 +85,7 @@ struct mdp_context {
     // work buffers of the solves, kept for the context's next solve (a context
     // runs one solve at a time): no cudaMalloc/cudaFree, which would
     // synchronise the device, in the solves of a serving loop
-    DevBuf       ws[12];
+    DevBuf       ws[13];    // [12]: FP32 (x, y, z, 0) copy of the map gathered by the FP32 P
     double      *h_pinned = nullptr;  // pinned host scalars
     // optional per-operator timing inside the solver (CUDA events on the stream)
     int          profile = 0;

@@ -224,8 +224,12 @@ struct TileArgsT {
     const int     *active;      // [ncols] nonzero for the columns to apply, or nullptr (all)
 };
 
+// FP32 tiles of up to 2^13 points per CTA (64 KB of shared memory, two CTAs
+// fit an SM) are held to 64 registers so that two 512-thread CTAs are resident
+// (15-25 % faster despite ~100 bytes of spills); larger FP32 tiles and FP64
+// tiles (one CTA per SM by shared memory) keep 128.
 template <typename T, int LOG_ML, int C>
-__global__ void __launch_bounds__(512) toeplitz_tile_kernel(TileArgsT<T> a) {
+__global__ void __launch_bounds__(512, (sizeof(T) == 4 && LOG_ML <= 13) ? 2 : 1) toeplitz_tile_kernel(TileArgsT<T> a) {
     using V = typename CT<T>::V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V            *smem = reinterpret_cast<V *>(smem_raw);
@@ -519,11 +523,17 @@ __device__ __forceinline__ V split_tw(const V *wa, const V *wb, int e) {  // W_M
 
 // threads of a split kernel working on `work` complex points (one radix-16 set each)
 __host__ __device__ constexpr int split_nt(int work) { return work / 16 < 64 ? 64 : (work / 16 > 512 ? 512 : work / 16); }
+// resident CTAs per SM asked of the compiler for a split kernel of nt threads:
+// FP32 kernels are held to 64 registers (1024 threads per SM; a few bytes of
+// spills, 10-13 % faster than 80-90 registers at a third fewer warps); FP64
+// kernels keep their registers (their 16 complex points take 64 by themselves)
+__host__ __device__ constexpr int split_minb(int nt, int elem) { return elem == 4 ? (1024 / nt > 1 ? 1024 / nt : 1) : 1; }
 
 // forward (INV = false) or inverse (INV = true) column transforms of one tile:
 // CW consecutive columns per CTA
 template <typename T, int LOG_M1, int CW, bool INV>
-__global__ void __launch_bounds__(split_nt(CW << LOG_M1)) split_cols_kernel(SplitArgsT<T> a) {
+__global__ void __launch_bounds__(split_nt(CW << LOG_M1), split_minb(split_nt(CW << LOG_M1), sizeof(T)))
+        split_cols_kernel(SplitArgsT<T> a) {
     using V = typename CT<T>::V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V            *s = reinterpret_cast<V *>(smem_raw);
@@ -626,7 +636,8 @@ __global__ void __launch_bounds__(split_nt(CW << LOG_M1)) split_cols_kernel(Spli
 // row pairs of one tile: pair rp = 0 holds the self-paired rows 0 and M1/2,
 // pair rp > 0 the rows rp and M1 - rp; RP pairs (2 RP rows) per CTA
 template <typename T, int LOG_M2, int RP>
-__global__ void __launch_bounds__(split_nt(2 * RP << LOG_M2)) split_rows_kernel(SplitArgsT<T> a) {
+__global__ void __launch_bounds__(split_nt(2 * RP << LOG_M2), split_minb(split_nt(2 * RP << LOG_M2), sizeof(T)))
+        split_rows_kernel(SplitArgsT<T> a) {
     using V = typename CT<T>::V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V            *s = reinterpret_cast<V *>(smem_raw);
@@ -1771,6 +1782,65 @@ int mdp_noise_chunks(const mdp_noise *N, int *n_chunks, const int64_t **d_chunk_
     return MDP_OK;
 }
 
+// x4[q] = ((float) x[3q], (float) x[3q+1], (float) x[3q+2], 0): one aligned
+// 16-byte gather per sample in the FP32 P instead of three 8-byte ones
+__global__ void map_to_float4_kernel(const double *__restrict__ x, float4 *__restrict__ x4, int64_t npix) {
+    for (int64_t q = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; q < npix; q += (int64_t) gridDim.x * blockDim.x)
+        x4[q] = make_float4((float) x[3 * q], (float) x[3 * q + 1], (float) x[3 * q + 2], 0.0f);
+}
+
+__device__ __forceinline__ float p32_row(int32_t o, float w0, float w1, float w2, const float4 *__restrict__ x4) {
+    if (o < 0) return 0.0f;
+    const float4 m = __ldg(x4 + o / 3);
+    return w0 * m.x + w1 * m.y + w2 * m.z;
+}
+
+// y32 = P x with the map as FP32 quadruples, fused with FP64 block-mean
+// partial sums; four consecutive samples per thread with 16-byte loads of
+// their offsets and weights (the chunk's unaligned head and tail one by one)
+__global__ void __launch_bounds__(512) matvec32_chunk_sums4_kernel(const int32_t *__restrict__ off,
+                                                                   const float *__restrict__ w,
+                                                                   const float4 *__restrict__ x4,
+                                                                   float *__restrict__ y,
+                                                                   const int64_t *__restrict__ chunk_start,
+                                                                   const int32_t *__restrict__ chunk_len,
+                                                                   double *__restrict__ partial) {
+    const int64_t s = chunk_start[blockIdx.x];
+    const int64_t e = s + chunk_len[blockIdx.x];
+    const int64_t a = min((s + 3) & ~(int64_t) 3, e);  // first multiple of 4 in [s, e]
+    const int64_t b = max(e & ~(int64_t) 3, a);         // end of the aligned body
+    double        acc = 0.0;
+    for (int64_t t = a + 4 * (int64_t) threadIdx.x; t < b; t += 4 * (int64_t) blockDim.x) {
+        const int4    o = __ldg(reinterpret_cast<const int4 *>(off + t));
+        const float4 *wv = reinterpret_cast<const float4 *>(w + 3 * t);  // 48-byte aligned
+        const float4  w0 = __ldg(wv), w1 = __ldg(wv + 1), w2 = __ldg(wv + 2);
+        float4        v;
+        v.x = p32_row(o.x, w0.x, w0.y, w0.z, x4);
+        v.y = p32_row(o.y, w0.w, w1.x, w1.y, x4);
+        v.z = p32_row(o.z, w1.z, w1.w, w2.x, x4);
+        v.w = p32_row(o.w, w2.y, w2.z, w2.w, x4);
+        *reinterpret_cast<float4 *>(y + t) = v;
+        acc += (double) v.x + (double) v.y + (double) v.z + (double) v.w;
+    }
+    // head [s, a) and tail [b, e): fewer than 4 rows each
+    const int64_t rest = (a - s) + (e - b);
+    if (threadIdx.x < rest) {
+        const int64_t t = threadIdx.x < a - s ? s + threadIdx.x : b + (threadIdx.x - (a - s));
+        const float   v = p32_row(off[t], w[3 * t], w[3 * t + 1], w[3 * t + 2], x4);
+        y[t] = v;
+        acc += (double) v;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    __shared__ double wsum[16];
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = (threadIdx.x < (blockDim.x >> 5)) ? wsum[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) partial[blockIdx.x] = v;
+    }
+}
+
 // y32 = P x (x FP64, weights FP32) fused with FP64 block-mean partial sums
 __global__ void __launch_bounds__(512) matvec32_chunk_sums_kernel(const int32_t *__restrict__ off,
                                                                   const float *__restrict__ w,
@@ -1806,9 +1876,23 @@ int mdp_matvec32_blockmeans(mdp_context *ctx, const mdp_pointing *A, const mdp_n
                             float *d_y) {
     if (!A->triplet || !A->w32.p || !N->covers_all || N->lambda == 1 || N->nrow_end != A->m || N->n_chunks == 0)
         return MDP_EUNSUPPORTED;
-    matvec32_chunk_sums_kernel<<<N->n_chunks, 512, 0, ctx->stream>>>(A->off.as<int32_t>(), A->w32.as<float>(), d_x, d_y,
-                                                                     N->chunk_start.as<int64_t>(),
-                                                                     N->chunk_len.as<int32_t>(), N->partial.as<double>());
+    const int64_t npix = A->n_map() / 3;
+    // the vector loads need 16-byte aligned offsets, weights and output
+    const bool vec = (reinterpret_cast<uintptr_t>(A->off.p) % 16 == 0) &&
+                     (reinterpret_cast<uintptr_t>(A->w32.p) % 16 == 0) && (reinterpret_cast<uintptr_t>(d_y) % 16 == 0);
+    if (vec) {
+        MDP_TRY(ctx->ws[12].alloc(sizeof(float4) * (size_t) std::max<int64_t>(npix, 1)));
+        float4 *x4 = ctx->ws[12].as<float4>();
+        map_to_float4_kernel<<<grid_for(npix, 256, ctx->sm_count * 8), 256, 0, ctx->stream>>>(d_x, x4, npix);
+        MDP_CHECK_LAUNCH(ctx);
+        matvec32_chunk_sums4_kernel<<<N->n_chunks, 512, 0, ctx->stream>>>(
+                A->off.as<int32_t>(), A->w32.as<float>(), x4, d_y, N->chunk_start.as<int64_t>(),
+                N->chunk_len.as<int32_t>(), N->partial.as<double>());
+    } else {
+        matvec32_chunk_sums_kernel<<<N->n_chunks, 512, 0, ctx->stream>>>(
+                A->off.as<int32_t>(), A->w32.as<float>(), d_x, d_y, N->chunk_start.as<int64_t>(),
+                N->chunk_len.as<int32_t>(), N->partial.as<double>());
+    }
     MDP_CHECK_LAUNCH(ctx);
     block_means_final<<<grid_for(N->nb, 128, 1024), 128, 0, ctx->stream>>>(
             N->partial.as<double>(), N->blk_chunk0.as<int32_t>(), N->blk_nchunk.as<int32_t>(), N->blk_len.as<int32_t>(),
@@ -1825,6 +1909,15 @@ extern "C" int mdp_noise_tile_fp32(mdp_context *ctx, mdp_noise *N, int *fft_size
     if (fft_size) *fft_size = N->p32.fft_n;
     if (cluster_ctas) *cluster_ctas = N->p32.cluster;
     if (n_tiles) *n_tiles = N->p32.n_tiles;
+    return MDP_OK;
+}
+
+extern "C" int mdp_prepare_fp32(mdp_context *ctx, mdp_pointing *A, mdp_noise *N) {
+    if (!ctx || !A || !N) return MDP_EINVAL;
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    MDP_TRY(mdp_pointing_prepare_fp32(ctx, A));
+    MDP_TRY(mdp_noise_prepare_fp32(ctx, N));
+    MDP_CUDA(cudaStreamSynchronize(ctx->stream));
     return MDP_OK;
 }
 
