@@ -11,9 +11,11 @@ and tile plans, block-Jacobi build with the rcond cut, PCG to relative
 residual 1e-8 (the reference's criterion); value = mixed precision,
 config.fp64 = the plain FP64 path.  Further keys on the same line: e2e (the
 MLmap solve from host buffers), cpu_baseline (the reference's C operator on
-the host cores, extrapolated), mixed_fknee_sweep (CPU-runnable workload,
-f_knee 0.1/1/5 Hz), multi_rhs (128 right-hand sides sharing one pointing),
-serving (Poisson stream of independent solves, p50/p99 latency).
+the host cores, extrapolated), c1_reference (the CPU-runnable workload: the
+reference's whole MLmap on 4 host ranks vs the GPU paths), mixed_fknee_sweep
+(CPU-runnable workload, f_knee 0.1/1/5 Hz), multi_rhs (128 right-hand sides
+sharing one pointing), serving (Poisson stream of independent solves, p50/p99
+latency).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -60,7 +62,8 @@ def parse():
     ap.add_argument("--no-multi", action="store_true", help="skip the multi-RHS part")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving part")
     ap.add_argument("--no-fknee", action="store_true", help="skip the f_knee sweep part")
-    ap.add_argument("--only", default="", choices=["", "multi", "serve", "fknee"],
+    ap.add_argument("--no-c1", action="store_true", help="skip the CPU-runnable reference comparison")
+    ap.add_argument("--only", default="", choices=["", "multi", "serve", "fknee", "c1"],
                     help="run only the multi-RHS, serving or f_knee part (prints their JSON)")
     ap.add_argument("--multi-rhs", type=int, default=128, help="right-hand sides of the multi-RHS part")
     ap.add_argument("--multi-fp64-cols", type=int, default=2, help="columns timed with the plain FP64 path")
@@ -306,6 +309,80 @@ def bench_fknee(args, device):
     return out
 
 
+def bench_c1(args, device):
+    """The CPU-runnable configuration (4 detectors x 2^20 samples, 256x192 px,
+    lambda 2^12, one Toeplitz block per detector) with 1% flagged samples (without
+    them the operator is singular and the reference stalls above 1e-8): the
+    reference's whole MLmap (oracle/_ref: set-up, block-Jacobi, PCG to 1e-8) on 4
+    forked host ranks, wall time, against the plain FP64 and mixed GPU paths
+    (time-to-map from device-resident inputs, compression and operator set-up
+    included, best of 3 after a warm-up) and each GPU map's I/Q/U error against
+    the reference's maps on the observed pixels."""
+    import torch
+    import midapack_b200 as mb
+    from midapack_b200 import synth
+    from oracle import ref
+    cfg = dict(synth.CONFIGS["c1_4det_2p20_256x192_lam4096"], gap_frac=0.01)
+    wl = synth.make_workload("c1", **cfg)
+    m, nside = wl.n_samples, wl.nside
+    out = {"workload": "c1_4det_2p20_256x192_lam4096 + 1% flagged samples", "tol": TOL}
+    if not ref.available():
+        out["reference"] = {"unavailable": "oracle/_ref not built"}
+        refmaps = None
+    else:
+        with tempfile.TemporaryDirectory() as td:
+            case, res_path = os.path.join(td, "case.npz"), os.path.join(td, "maps.npz")
+            np.savez(case, pix=wl.pix, weights=wl.weights, signal=wl.signal, noise=wl.noise,
+                     block_sizes=wl.block_sizes, lam=wl.lam, invtt=wl.invtt, nside=nside, tol=TOL,
+                     maxiter=4 * MAXITER)
+            r = subprocess.run([sys.executable, "-m", "oracle.cpu_baseline", "--mlmap", case, "4", res_path],
+                               cwd=ROOT, capture_output=True, text=True, timeout=1200)
+            lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+            if r.returncode != 0 or not lines:
+                raise RuntimeError("reference MLmap failed: " + r.stderr[-500:])
+            rj = json.loads(lines[-1])
+            mz = np.load(res_path)
+            refmaps = (mz["I"], mz["Q"], mz["U"], mz["Hits"])
+        out["reference"] = {"path": "reference MLmap (oracle/_ref, shim FFT/MPI/LAPACK), 4 forked host ranks",
+                            "ranks": rj["ranks"], "time_to_map_s": round(rj["seconds"], 3),
+                            "iterations": rj["iterations"],
+                            "per_iter_ms": round(1e3 * rj["seconds"] / max(rj["iterations"], 1), 3)}
+    ctx = mb.Context(device)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    pix, w, sig, noi = d(wl.pix), d(wl.weights), d(wl.signal), d(wl.noise)
+    npix = 12 * nside * nside
+    for prec, fn in (("fp64", mb.gls_solve), ("mixed", mb.gls_solve_mixed)):
+        ts = []
+        for rep in range(4):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            P = mb.Pointing(ctx, pix, w, m, 3)
+            N = mb.Noise(ctx, wl.block_sizes, wl.lam, wl.invtt)
+            o = fn(ctx, P, N, sig, noi, tol=TOL, maxiter=4 * MAXITER)
+            torch.cuda.synchronize()
+            if rep:
+                ts.append(time.perf_counter() - t0)
+        x, lst, info = o[0].cpu().numpy(), o[1].cpu().numpy(), o[5]
+        entry = {"time_to_map_s": round(min(ts), 4), "iterations": info.iterations, "converged": bool(info.converged),
+                 "per_iter_ms": round(1e3 * min(ts) / max(info.iterations, 1), 3)}
+        if refmaps is not None:
+            p = lst[0::3] // 3
+            hit = refmaps[3][p] > 0
+            errs = {}
+            for k, name in enumerate("IQU"):
+                mine = np.zeros(npix)
+                mine[p] = x[k::3]
+                sel = np.zeros(npix, dtype=bool)
+                sel[p[hit]] = True
+                errs[name] = float(np.linalg.norm(mine[sel] - refmaps[k][sel]) / np.linalg.norm(refmaps[k][sel]))
+            entry["map_rel_err_vs_reference"] = errs
+            entry["speedup_vs_reference"] = round(out["reference"]["time_to_map_s"] / min(ts), 1)
+        out[prec] = entry
+    ctx.close()
+    torch.cuda.empty_cache()
+    return out
+
+
 def bench_serving(args, device):
     """Serving configuration: Poisson arrivals (args.serve_rate per second) of
     independent solves on args.serve_datasets resident datasets drawn
@@ -378,7 +455,7 @@ def main():
     local = local % max(torch.cuda.device_count(), 1)
     torch.cuda.set_device(local)
     if args.only:
-        r = {"multi": bench_multi, "serve": bench_serving, "fknee": bench_fknee}[args.only](args, local)
+        r = {"multi": bench_multi, "serve": bench_serving, "fknee": bench_fknee, "c1": bench_c1}[args.only](args, local)
         print(json.dumps({args.only: r}), flush=True)
         return 0
     if world > 1:
@@ -525,6 +602,9 @@ def main():
     # multi-RHS and serving configurations (one GPU: rank 0 of a single-process run)
     multi = serve_out = fknee = None
     ctx.trim()
+    c1 = None
+    if world == 1 and not args.no_c1:
+        c1 = bench_c1(args, local)
     if world == 1 and not args.no_fknee:
         fknee = bench_fknee(args, local)
     if world == 1 and not args.no_multi:
@@ -555,6 +635,8 @@ def main():
             line["e2e"] = e2e
         if cpu:
             line["cpu_baseline"] = cpu
+        if c1:
+            line["c1_reference"] = c1
         if fknee:
             line["mixed_fknee_sweep"] = fknee
         if multi:

@@ -5,6 +5,9 @@ separate process (a fresh interpreter that never touched CUDA, since the
 oracle forks one process per rank).
 
     python -m oracle.cpu_baseline SAMPLE.npz RANKS   -> prints seconds per application (JSON)
+    python -m oracle.cpu_baseline --mlmap CASE.npz RANKS OUT.npz
+        -> runs the reference's whole MLmap (RANKS forked ranks, detectors split
+           evenly), prints its wall time and iterations (JSON), saves its maps
 """
 import json
 import sys
@@ -24,5 +27,25 @@ def main(path, ranks):
     print(json.dumps({"seconds_per_application": t, "ranks": ranks}))
 
 
+def mlmap(path, ranks, out):
+    import time
+    d = np.load(path)
+    ranks = int(ranks)
+    m = int(d["signal"].size)
+    nb = int(d["block_sizes"].size)
+    if m % ranks or nb % ranks:
+        raise SystemExit("samples and blocks must split evenly over the ranks")
+    t0 = time.perf_counter()
+    maps = ref.mlmap(ranks, [m // ranks] * ranks, [nb // ranks] * ranks, d["block_sizes"], d["pix"], d["weights"],
+                     d["signal"], d["noise"], int(d["lam"]), d["invtt"], int(d["nside"]), tol=float(d["tol"]),
+                     maxiter=int(d["maxiter"]))
+    t = time.perf_counter() - t0
+    np.savez(out, I=maps[0], Q=maps[1], U=maps[2], Cond=maps[3], Hits=maps[4], res=maps[5])
+    print(json.dumps({"seconds": t, "ranks": ranks, "iterations": int(len(maps[5]) - 1)}))
+
+
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if sys.argv[1] == "--mlmap":
+        mlmap(*sys.argv[2:])
+    else:
+        main(*sys.argv[1:])
