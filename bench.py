@@ -146,7 +146,8 @@ def algorithmic_bytes32(ns: int, n_map: int, t32):
 # (dram__bytes_read.sum + dram__bytes_write.sum of the three split kernels over
 # 704 tiles, lambda 2^14, 2^20-sample blocks; see profiles/), keyed by
 # (precision, M1, M2); scaled to a launch by the tile count
-NINV_TRAFFIC_PER_TILE = {("f32", 256, 256): 1857072128 / 704}
+NINV_TRAFFIC_PER_TILE = {("f32", 256, 256): 1857072128 / 704,   # profiles/ninv_split_fp32_256x256_lambda16384.md
+                         ("f32", 256, 512): 1728509184 / 320}   # profiles/op32_split_256x512_lambda16384.md
 
 
 def ninv_kernel(t: dict, prec: str) -> str:

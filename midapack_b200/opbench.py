@@ -64,6 +64,17 @@ def main(argv=None):
             ms = timed(fn)
             out[name] = {"ms": round(ms, 4), "algorithmic_GBps": round((ns * 36 + n * 8) / ms / 1e6, 1)}
             continue
+        if name == "Op32":
+            # the FP32 operator of the mixed-precision solver: P (FP32 weights and TOD), N^-1 (FP32
+            # tiles), P^T (FP64 accumulation), from and to FP64 maps
+            N = mb.Noise(ctx, wl.block_sizes, wl.lam, wl.invtt)
+            mb.prepare_fp32(ctx, P, N)
+            fn = lambda: mb.check(mb.lib().mdp_apply_op(ctx.h, P.h, N.h, x.data_ptr(), xo.data_ptr(), 1),  # noqa: E731
+                                  "mdp_apply_op")
+            ms = timed(fn)
+            out[name] = {"ms": round(ms, 4), "tile": N.tile_fp32(), "plan": N._plan(1)}
+            N.close()
+            continue
         fp32 = name == "Ninv32"
         var = "MDP_TOEPLITZ_PLAN32" if fp32 else "MDP_TOEPLITZ_PLAN"
         res = []
