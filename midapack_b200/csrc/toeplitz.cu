@@ -577,7 +577,7 @@ __global__ void __launch_bounds__(split_nt(CW << LOG_M1), split_minb(split_nt(CW
         for (int u = 0; u < EPT; u++) {
             const int     e = threadIdx.x + u * NT;
             const int     c = e % CW, j1 = e / CW;
-            const int64_t row = ws + 2 * ((int64_t) M2 * j1 + c0 + c);
+            const int64_t row = ws + 2 * (M2 * j1 + c0 + c);  // in-tile offsets fit in 32 bits (M <= 2^18)
             const bool    ok = e < CW * M1;
             if (a.vec2 && ok && row >= bs && row + 1 < be) {
                 const V z = __ldg(reinterpret_cast<const V *>(a.vin + row));
@@ -599,7 +599,7 @@ __global__ void __launch_bounds__(split_nt(CW << LOG_M1), split_minb(split_nt(CW
 #pragma unroll
         for (int u = 0; u < EPT; u++) {
             const int e = threadIdx.x + u * NT;
-            if (e < CW * M1) y[u] = Y[(int64_t) (e / CW) * M2 + c0 + e % CW];
+            if (e < CW * M1) y[u] = Y[(e / CW) * M2 + c0 + e % CW];
         }
 #pragma unroll
         for (int u = 0; u < EPT; u++) {
@@ -616,7 +616,7 @@ __global__ void __launch_bounds__(split_nt(CW << LOG_M1), split_minb(split_nt(CW
             const int k1 = (int) (__brev((unsigned) p) >> (32 - LOG_M1));
             const int j2 = c0 + c;
             const V   v = s[sq_idx<M1>(c, p)];
-            Y[(int64_t) k1 * M2 + j2] = cmul(v, split_tw(swa, swb, (int) (((int64_t) j2 * k1) & (M - 1))));
+            Y[k1 * M2 + j2] = cmul(v, split_tw(swa, swb, (j2 * k1) & (M - 1)));
         }
     } else {
         // position p holds j1 = rev(p): z'[M2 j1 + j2] = conj(value) / M, samples 2(M2 j1 + j2) + {0, 1}
@@ -626,7 +626,7 @@ __global__ void __launch_bounds__(split_nt(CW << LOG_M1), split_minb(split_nt(CW
             const int     c = e % CW, p = e / CW;
             const int     j1 = (int) (__brev((unsigned) p) >> (32 - LOG_M1));
             const V       v = s[sq_idx<M1>(c, p)];
-            const int64_t row = ws + 2 * ((int64_t) M2 * j1 + c0 + c);
+            const int64_t row = ws + 2 * (M2 * j1 + c0 + c);
             if (row >= t0 && row < out_end) a.vout[row] = v.x * scale;
             if (row + 1 >= t0 && row + 1 < out_end) a.vout[row + 1] = -v.y * scale;
         }
@@ -670,7 +670,7 @@ __global__ void __launch_bounds__(split_nt(2 * RP << LOG_M2), split_minb(split_n
 #pragma unroll
         for (int u = 0; u < EPT; u++) {
             const int e = threadIdx.x + u * NT;
-            if (e < 2 * RP * M2) y[u] = Y[(int64_t) row_of(e / M2) * M2 + e % M2];
+            if (e < 2 * RP * M2) y[u] = Y[row_of(e / M2) * M2 + e % M2];
         }
 #pragma unroll
         for (int u = 0; u < EPT; u++) {
@@ -722,7 +722,7 @@ __global__ void __launch_bounds__(split_nt(2 * RP << LOG_M2), split_minb(split_n
             const int r = e / M2, j2 = e % M2;
             const int k1 = row_of(r);
             const V   v = s[sq_idx<M2>(r, j2)];
-            Y[(int64_t) k1 * M2 + j2] = cmulc(v, split_tw(swa, swb, (int) (((int64_t) j2 * k1) & (M - 1))));
+            Y[k1 * M2 + j2] = cmulc(v, split_tw(swa, swb, (j2 * k1) & (M - 1)));
         }
         return;
     }
@@ -775,7 +775,7 @@ __global__ void __launch_bounds__(split_nt(2 * RP << LOG_M2), split_minb(split_n
         const int r = e / M2, j2 = e % M2;
         const int k1 = row_of(r);
         const V   v = s[sq_idx<M2>(r, j2)];
-        Y[(int64_t) k1 * M2 + j2] = cmulc(v, split_tw(swa, swb, (int) (((int64_t) j2 * k1) & (M - 1))));
+        Y[k1 * M2 + j2] = cmulc(v, split_tw(swa, swb, (j2 * k1) & (M - 1)));
     }
 }
 
