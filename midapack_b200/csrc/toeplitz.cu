@@ -57,6 +57,45 @@ template <typename V> __device__ __forceinline__ V csq(V a) {  // a^2
     return mkv(a, a.x * a.x - a.y * a.y, 2 * a.x * a.y);
 }
 
+// Complex FP32 arithmetic on Blackwell's paired FP32 instructions (add / sub /
+// mul / fma .f32x2): one instruction for both components, each lane rounded as
+// the scalar instruction would round it (6-8 % faster FP32 N^-1 than scalar).
+__device__ __forceinline__ unsigned long long f2b(float x, float y) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
+    return r;
+}
+__device__ __forceinline__ float2 b2f(unsigned long long r) {
+    float2 v;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+    return v;
+}
+template <> __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) {
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2b(a.x, a.y)), "l"(f2b(b.x, b.y)));
+    return b2f(r);
+}
+template <> __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) {
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2b(a.x, a.y)), "l"(f2b(b.x, b.y)));
+    return b2f(r);
+}
+// a b = (a.x b.x - a.y b.y, a.x b.y + a.y b.x) = (a.x, a.x) (b.x, b.y) + (a.y, a.y) (-b.y, b.x)
+template <> __device__ __forceinline__ float2 cmul<float2>(float2 a, float2 b) {
+    unsigned long long t, r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(t) : "l"(f2b(a.x, a.x)), "l"(f2b(b.x, b.y)));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(f2b(a.y, a.y)), "l"(f2b(-b.y, b.x)), "l"(t));
+    return b2f(r);
+}
+// a conj(b) = (a.x b.x + a.y b.y, a.y b.x - a.x b.y) = (a.x, a.y) (b.x, b.x) + (a.y, a.x) (b.y, -b.y)
+template <> __device__ __forceinline__ float2 cmulc<float2>(float2 a, float2 b) {
+    unsigned long long t, r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(t) : "l"(f2b(a.x, a.y)), "l"(f2b(b.x, b.x)));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(f2b(a.y, a.x)), "l"(f2b(b.y, -b.y)), "l"(t));
+    return b2f(r);
+}
+
+
 // 16th roots of unity exp(-2 pi i k / 16), k < 8, correctly rounded
 __constant__ double2 c_w16[8] = {
     {0x1.0000000000000p+0, 0.0},
