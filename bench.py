@@ -13,7 +13,8 @@ config.fp64 = the plain FP64 path.  Further keys on the same line: e2e (the
 MLmap solve from host buffers), cpu_baseline (the reference's C operator on
 the host cores, extrapolated), c1_reference (the CPU-runnable workload: the
 reference's whole MLmap on 4 host ranks vs the GPU paths), mixed_fknee_sweep
-(CPU-runnable workload, f_knee 0.1/1/5 Hz), multi_rhs (128 right-hand sides
+(CPU-runnable workload, f_knee 0.1/1/5 Hz), solvers_low_fknee (two-level
+preconditioners and ECG at f_knee 0.1 Hz), multi_rhs (128 right-hand sides
 sharing one pointing), serving (Poisson stream of independent solves, p50/p99
 latency).
 
@@ -63,7 +64,8 @@ def parse():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving part")
     ap.add_argument("--no-fknee", action="store_true", help="skip the f_knee sweep part")
     ap.add_argument("--no-c1", action="store_true", help="skip the CPU-runnable reference comparison")
-    ap.add_argument("--only", default="", choices=["", "multi", "serve", "fknee", "c1"],
+    ap.add_argument("--no-solvers", action="store_true", help="skip the two-level / ECG part")
+    ap.add_argument("--only", default="", choices=["", "multi", "serve", "fknee", "c1", "solvers"],
                     help="run only the multi-RHS, serving or f_knee part (prints their JSON)")
     ap.add_argument("--multi-rhs", type=int, default=128, help="right-hand sides of the multi-RHS part")
     ap.add_argument("--multi-fp64-cols", type=int, default=2, help="columns timed with the plain FP64 path")
@@ -384,6 +386,58 @@ def bench_c1(args, device):
     return out
 
 
+def bench_solvers(args, device):
+    """The reference's other solvers and preconditioners on the CPU-runnable
+    workload at low f_knee (0.1 Hz, the ill-conditioned end of the sweep), 1%
+    flagged samples: block-Jacobi PCG (precond 0), the two-level
+    preconditioners (precond 1 a priori, precond 2 a posteriori, z_2lvl
+    columns) and ECG (solver 1, Orthomin, enlFac search directions), all FP64 to
+    relative residual 1e-8; time-to-map from device-resident inputs with the
+    set-up (compression, spectra, block-Jacobi, deflation columns) included, best
+    of 2 after a warm-up, and each map's I/Q/U error against the FP64 PCG
+    solution at 1e-12."""
+    import torch
+    import midapack_b200 as mb
+    from midapack_b200 import synth
+    cfg = dict(synth.CONFIGS["c1_4det_2p20_256x192_lam4096"], gap_frac=0.01, fknee=0.1)
+    wl = synth.make_workload_torch("solvers", **cfg)
+    m = wl.n_samples
+    ctx = mb.Context(device)
+    out = {"workload": "c1_4det_2p20_256x192_lam4096 + 1% flagged samples, f_knee 0.1 Hz", "tol": TOL}
+    runs = [("pcg_bj", mb.gls_solve, {}),
+            ("pcg_2lvl_apriori_z1", mb.gls_solve, {"precond": 1, "z_2lvl": 1}),
+            ("pcg_2lvl_apriori_z8", mb.gls_solve, {"precond": 1, "z_2lvl": 8}),
+            ("pcg_2lvl_aposteriori_z8", mb.gls_solve, {"precond": 2, "z_2lvl": 8}),
+            ("pcg_2lvl_aposteriori_z16", mb.gls_solve, {"precond": 2, "z_2lvl": 16}),
+            ("ecg_omin_enl4", mb.gls_solve_ecg, {"enl_fac": 4}),
+            ("ecg_omin_enl8", mb.gls_solve_ecg, {"enl_fac": 8})]
+
+    def solve(fn, kw, tol):
+        P = mb.Pointing(ctx, wl.pix, wl.weights, m, 3)
+        N = mb.Noise(ctx, wl.block_sizes, wl.lam, wl.invtt)
+        return fn(ctx, P, N, wl.signal, wl.noise, tol=tol, maxiter=4 * MAXITER, **kw)
+
+    xo = solve(mb.gls_solve, {}, 1e-12)[0].cpu().numpy()
+    for name, fn, kw in runs:
+        ts = []
+        for rep in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            o = solve(fn, kw, TOL)
+            torch.cuda.synchronize()
+            if rep:
+                ts.append(time.perf_counter() - t0)
+        x, info = o[0].cpu().numpy(), o[5]
+        out[name] = {"time_to_map_s": round(min(ts), 4), "iterations": info.iterations,
+                     "converged": bool(info.converged),
+                     "map_rel_err_vs_fp64_oracle": {
+                         nm: float(np.linalg.norm(x[k::3] - xo[k::3]) / np.linalg.norm(xo[k::3]))
+                         for k, nm in enumerate("IQU")}}
+    ctx.close()
+    torch.cuda.empty_cache()
+    return out
+
+
 def bench_serving(args, device):
     """Serving configuration: Poisson arrivals (args.serve_rate per second) of
     independent solves on args.serve_datasets resident datasets drawn
@@ -456,7 +510,8 @@ def main():
     local = local % max(torch.cuda.device_count(), 1)
     torch.cuda.set_device(local)
     if args.only:
-        r = {"multi": bench_multi, "serve": bench_serving, "fknee": bench_fknee, "c1": bench_c1}[args.only](args, local)
+        r = {"multi": bench_multi, "serve": bench_serving, "fknee": bench_fknee, "c1": bench_c1,
+             "solvers": bench_solvers}[args.only](args, local)
         print(json.dumps({args.only: r}), flush=True)
         return 0
     if world > 1:
@@ -608,6 +663,9 @@ def main():
         c1 = bench_c1(args, local)
     if world == 1 and not args.no_fknee:
         fknee = bench_fknee(args, local)
+    solvers = None
+    if world == 1 and not args.no_solvers:
+        solvers = bench_solvers(args, local)
     if world == 1 and not args.no_multi:
         multi = bench_multi(args, local)
     if world == 1 and not args.no_serve:
@@ -640,6 +698,8 @@ def main():
             line["c1_reference"] = c1
         if fknee:
             line["mixed_fknee_sweep"] = fknee
+        if solvers:
+            line["solvers_low_fknee"] = solvers
         if multi:
             line["multi_rhs"] = multi
         if serve_out:
