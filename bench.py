@@ -172,7 +172,8 @@ def cpu_reference(wl_host, iterations: int, sample_dets: int, full_samples: int,
     nb_per_det = int(np.searchsorted(ends, per_det, side="right"))
     if nb_per_det < 1 or ends[nb_per_det - 1] != per_det:
         raise RuntimeError("Toeplitz blocks do not tile the detectors")
-    with tempfile.TemporaryDirectory() as td:
+    # the sample (several GB) goes through host memory when /dev/shm exists
+    with tempfile.TemporaryDirectory(dir="/dev/shm" if os.path.isdir("/dev/shm") else None) as td:
         path = os.path.join(td, "sample.npz")
         np.savez(path, pix=pix, weights=w, block_sizes=bs, lam=lam, invtt=invtt, per_det=per_det,
                  nb_per_det=nb_per_det)
@@ -744,9 +745,16 @@ def run_e2e(args, wl, world, pinned):
             "api": "MLmap_b200 (MLmap solve, host buffers)", "iterations": it.value}
 
 
+def host_cores() -> int:
+    """Host threads this process may use (the reference runs one rank per core)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def cpu_sample(wl):
-    cores = os.cpu_count() or 1
-    sample_dets = max(1, min(cores, 8, wl.n_det))
+    sample_dets = max(1, min(host_cores(), wl.n_det))
     per_det = wl.n_samp
     return (sample_dets, wl.pix[:3 * per_det * sample_dets].cpu().numpy(),
             wl.weights[:3 * per_det * sample_dets].cpu().numpy())
@@ -876,8 +884,7 @@ def run_reference(args, wl, ctx, one_solve):
     # iteration count of the same solve (device run, untimed) to extrapolate the operator cost
     _, _, out = one_solve()
     iters = out[5].iterations
-    cores = os.cpu_count() or 1
-    sample_dets = max(1, min(cores, 8, wl.n_det))
+    sample_dets = max(1, min(host_cores(), wl.n_det))
     per_det = wl.n_samp
     pix = wl.pix[:3 * per_det * sample_dets].cpu().numpy()
     w = wl.weights[:3 * per_det * sample_dets].cpu().numpy()
