@@ -10,7 +10,9 @@ device-resident inputs: pointing compression (MatInit), inverse-noise spectra
 and tile plans, block-Jacobi build with the rcond cut, PCG to relative
 residual 1e-8 (the reference's criterion); value = mixed precision,
 config.fp64 = the plain FP64 path.  Further keys on the same line: e2e (the
-MLmap solve from host buffers), cpu_baseline (the reference's C operator on
+same solve from pinned host inputs through the library's API, copies
+included; e2e.mlmap_fp64 the reference's MLmap entry point, FP64, host maps
+out), cpu_baseline (the reference's C operator on
 the host cores, extrapolated), c1_reference (the CPU-runnable workload: the
 reference's whole MLmap on 4 host ranks vs the GPU paths), mixed_fknee_sweep
 (CPU-runnable workload, f_knee 0.1/1/5 Hz), solvers_low_fknee (two-level
@@ -653,7 +655,11 @@ def main():
     torch.cuda.empty_cache()
 
     # end to end through the reference-facing API with host buffers
-    e2e = run_e2e(args, wl, world, pinned) if pinned else None
+    e2e = None
+    if pinned:
+        e2e = run_e2e_device_api(args, wl, world, pinned)
+        # the reference's own entry point (MLmap: FP64, host maps out) on the same inputs
+        e2e["mlmap_fp64"] = run_e2e(args, wl, world, pinned)
     pinned = None
 
     # multi-RHS and serving configurations (one GPU: rank 0 of a single-process run)
@@ -709,6 +715,47 @@ def main():
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def run_e2e_device_api(args, wl, world, pinned):
+    """The headline solve end to end through the library's Python/C device API
+    (midapack_b200.Pointing, Noise, gls_solve_mixed or gls_solve by --precision):
+    each step copies the inputs from pinned host memory to the device, builds
+    the operators, solves and reads the map back; max over ranks."""
+    import torch
+    import midapack_b200 as mb
+    ctx = mb.Context(torch.cuda.current_device())
+    nb = len(wl.block_sizes)
+    idv = np.arange(nb, dtype=np.int64) * wl.block_len
+    times, it = [], 0
+    for _ in range(args.e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dev = {k: v.to("cuda", non_blocking=True) for k, v in pinned.items()}
+        P = mb.Pointing(ctx, dev["pix"], dev["weights"], wl.n_samples, 3)
+        N = mb.Noise(ctx, wl.block_sizes, wl.lam, wl.invtt, idv=idv)
+        if args.precision == "mixed":
+            out = mb.gls_solve_mixed(ctx, P, N, dev["signal"], dev["noise"], tol=TOL, maxiter=MAXITER,
+                                     inner_tol=args.inner_tol)
+        else:
+            out = mb.gls_solve(ctx, P, N, dev["signal"], dev["noise"], tol=TOL, maxiter=MAXITER)
+        x = out[0].cpu()
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+        it = out[5].iterations
+        P.close()
+        N.close()
+        del dev, out
+    ctx.close()
+    t = max(times) if times else 0.0
+    if world > 1:
+        tt_ = torch.tensor([t], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(tt_, op=torch.distributed.ReduceOp.MAX)
+        t = float(tt_)
+    h2d = sum(v.numel() * v.element_size() for v in pinned.values())
+    return {"value": round(t, 4), "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(x.numel() * 8),
+            "api": f"midapack_b200 Pointing + Noise + gls_solve{'_mixed' if args.precision == 'mixed' else ''} "
+                   "from pinned host inputs", "iterations": it}
 
 
 def run_e2e(args, wl, world, pinned):
