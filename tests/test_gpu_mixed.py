@@ -53,8 +53,9 @@ def test_stbmm_fp32_vs_exact(gpu_ctx, lam, sizes, fft):
     assert _rel(out.double().cpu().numpy(), ref) < 1e-5
 
 
+@pytest.mark.parametrize("plan32", [None, "s,5,5"])
 @pytest.mark.parametrize("case", ["gaps", "cut", "cut_gaps"])
-def test_mixed_solve_matches_fp64(gpu_ctx, case):
+def test_mixed_solve_matches_fp64(gpu_ctx, case, plan32):
     import torch
     import midapack_b200 as mb
     wl = solver_cases()[case]()
@@ -64,7 +65,14 @@ def test_mixed_solve_matches_fp64(gpu_ctx, case):
     for mixed in (False, True):
         w = d(wl.weights)
         P = mb.Pointing(gpu_ctx, d(wl.pix), w, m, 3)
-        N = mb.Noise(gpu_ctx, wl.block_sizes, wl.lam, wl.invtt)
+        if plan32:
+            os.environ["MDP_TOEPLITZ_PLAN32"] = plan32
+        try:
+            N = mb.Noise(gpu_ctx, wl.block_sizes, wl.lam, wl.invtt)
+            if mixed:
+                mb.prepare_fp32(gpu_ctx, P, N)
+        finally:
+            os.environ.pop("MDP_TOEPLITZ_PLAN32", None)
         fn = mb.gls_solve_mixed if mixed else mb.gls_solve
         # the map error is bounded by cond(A) x the residual: solve to 1e-12 to compare maps at 1e-8
         x, lst, cond, hits, res, info = fn(gpu_ctx, P, N, d(wl.signal), d(wl.noise), tol=1e-12, maxiter=900)
@@ -89,12 +97,14 @@ def test_mixed_solve_matches_fp64(gpu_ctx, case):
         assert _rel(x32[k::3][sel], o.x[k::3][sel]) < 1e-8
 
 
+@pytest.mark.parametrize("plan", [None, "s,4,5", "s,5,5"])
 @pytest.mark.parametrize("sizes", [[1001, 3095, 39], [4096, 4096], [35, 8190]])
-def test_fp32_operator_ragged_blocks(gpu_ctx, sizes):
+def test_fp32_operator_ragged_blocks(gpu_ctx, sizes, plan):
     """The FP32 operator P^T N^-1 P (FP32 P with four samples per thread and
     the chunks' unaligned heads and tails one by one, FP32 N^-1, P^T) against
     the oracle's FP64 operator on blocks whose starts are not multiples of
-    four: within 1e-5 relative; prepare_fp32 ahead of it gives the same product."""
+    four, with the plan the tuner picks and with split plans: within 1e-5
+    relative; prepare_fp32 ahead of it gives the same product."""
     import torch
     import midapack_b200 as mb
     m = int(sum(sizes))
@@ -108,9 +118,18 @@ def test_fp32_operator_ragged_blocks(gpu_ctx, sizes):
     outs = []
     for prepare in (False, True):
         P = mb.Pointing(gpu_ctx, d(wl.pix), d(wl.weights), m, 3)
-        N = mb.Noise(gpu_ctx, sizes, 32, invtt)
-        if prepare:
-            mb.prepare_fp32(gpu_ctx, P, N)
+        if plan:
+            os.environ["MDP_TOEPLITZ_PLAN32"] = plan
+        try:
+            N = mb.Noise(gpu_ctx, sizes, 32, invtt)
+            if prepare:
+                mb.prepare_fp32(gpu_ctx, P, N)
+            else:
+                N.tile_fp32()
+        finally:
+            os.environ.pop("MDP_TOEPLITZ_PLAN32", None)
+        if plan:
+            assert N.tile_fp32()["split"] == [1 << int(v) for v in plan.split(",")[1:]]
         q = torch.empty(A.n, dtype=torch.float64, device="cuda")
         mb.check(mb.lib().mdp_apply_op(gpu_ctx.h, P.h, N.h, hd.data_ptr(), q.data_ptr(), 1), "mdp_apply_op")
         torch.cuda.synchronize()
