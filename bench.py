@@ -622,7 +622,7 @@ def main():
         t32 = N.tile_fp32()
         ab = algorithmic_bytes32(ns, n_map, (t32["n_tiles"], t32["fft_n"] // 2))
         tile = {"fp64": tile, "fp32": t32}
-        kname = {"P": "matvec32_chunk_sums_kernel", "Ninv": ninv_kernel(t32, "float"),
+        kname = {"P": "matvec32_chunk_sums4_kernel", "Ninv": ninv_kernel(t32, "float"),
                  "Pt": "trmatvec32_binned_kernel"}
         ninv_tile, ninv_prec = t32, "f32"
         dom = max(("P", "Ninv", "Pt"), key=lambda k: per[k])
@@ -637,6 +637,12 @@ def main():
                 "traffic": traffic, "peak_source": "measured" if peaks else "fallback",
                 "per_application_ms": {k: round(v, 4) for k, v in per.items()},
                 "algorithmic_bytes": ab}
+    if dom == "Ninv" and ninv_tile.get("split"):
+        # what the ncu captures show about the split kernels (profiles/)
+        roofline["limiter"] = ("not DRAM (1.8-2.7 TB/s of DRAM traffic, ~3x the algorithmic bytes from the "
+                               "four-step scratch): instruction issue in the row and inverse-column passes (issue "
+                               "slot ~65 % busy, top stall 'not selected') and load latency in the forward-column "
+                               "pass; profiles/ninv_split_fp32_256x512_sections.md")
 
     # the reference's CPU path on a bounded sample (before any large host allocation)
     cpu = None
