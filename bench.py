@@ -183,9 +183,8 @@ def cpu_reference(wl_host, iterations: int, sample_dets: int, full_samples: int,
                            capture_output=True, text=True, timeout=900)
         lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
         if r.returncode != 0 or not lines:
-            os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-            with open(os.path.join(ROOT, "gpurun_out", "cpu_baseline_failure.log"), "w") as fh:
-                fh.write(r.stdout[-20000:] + "\n----- stderr -----\n" + r.stderr[-20000:])
+            sys.stderr.write("reference baseline output (tail):\n" + r.stdout[-4000:] + "\n----- stderr -----\n" +
+                             r.stderr[-4000:] + "\n")
             errs = [ln for ln in r.stderr.splitlines() if "shim_mpi" in ln or "Error" in ln]
             raise RuntimeError(f"reference baseline failed: {' | '.join(errs[-3:])}")
         t = json.loads(lines[-1])["seconds_per_application"]

@@ -1,6 +1,6 @@
 """Times the reference's own C operator P^T N^-1 P (oracle/_ref) on host cores.
 
-TEST/BASELINE INFRASTRUCTURE ONLY: bench.py's CPU-baseline leg runs this as a
+TEST AND CPU-BASELINE INFRASTRUCTURE ONLY: bench.py's CPU-baseline leg runs this as a
 separate process (a fresh interpreter that never touched CUDA, since the
 oracle forks one process per rank).
 
