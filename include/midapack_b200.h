@@ -135,7 +135,9 @@ typedef struct {
     int    verbose;  /* 1: print the reference's per-iteration line on stdout */
     int    precond;  /* 0: block Jacobi; 1: two-level a priori (build_Z); 2: two-level
                         a posteriori (Lanczos Ritz vectors); precond.c:1310-1423.
-                        Two-level: mdp_gls_solve only (FP64) */
+                        mdp_gls_solve and mdp_gls_solve_mixed (there the deflation
+                        columns are built with the FP64 operator and precondition
+                        the inner FP32-operator PCGs) */
     int    z_2lvl;   /* deflation columns of the two-level preconditioners, 1..128
                         (0: one, the reference's default of one per rank) */
 } mdp_solve_params;

@@ -363,8 +363,10 @@ def prepare_fp32(ctx: Context, A: Pointing, N: Noise):
 
 
 def gls_solve_mixed(ctx: Context, A: Pointing, N: Noise, signal, noise, tol=1e-8, maxiter=500, inner_tol=1e-4,
-                    inner_maxiter=100, verbose=False):
-    """Mixed-precision solve (FP32 operator inside FP64 iterative refinement); same outputs as gls_solve."""
+                    inner_maxiter=100, verbose=False, precond=0, z_2lvl=0):
+    """Mixed-precision solve (FP32 operator inside FP64 iterative refinement); same outputs as gls_solve.
+
+    precond / z_2lvl as gls_solve: the two-level columns precondition the inner PCGs."""
     import torch
     n0 = A.shape()["n_map"]
     x = torch.empty(max(n0, 1), dtype=torch.float64, device="cuda")
@@ -372,7 +374,7 @@ def gls_solve_mixed(ctx: Context, A: Pointing, N: Noise, signal, noise, tol=1e-8
     cond = torch.empty(max(n0 // 3, 1), dtype=torch.float64, device="cuda")
     hits = torch.empty(max(n0 // 3, 1), dtype=torch.int32, device="cuda")
     res = np.zeros(maxiter + 1)
-    prm = SolveParams(tol, maxiter, 1 if verbose else 0)
+    prm = SolveParams(tol, maxiter, 1 if verbose else 0, precond, z_2lvl)
     info = SolveInfo()
     check(lib().mdp_gls_solve_mixed(ctx.h, A.h, N.h, ct.c_void_p(_ptr(signal)), ct.c_void_p(_ptr(noise)),
                                     ct.byref(prm), inner_tol, inner_maxiter, ct.c_void_p(x.data_ptr()),

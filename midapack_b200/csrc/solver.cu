@@ -908,10 +908,6 @@ extern "C" int mdp_gls_solve_mixed(mdp_context *ctx, mdp_pointing *A, const mdp_
         mdp_set_error("mdp_gls_solve_mixed: noise blocks extend past the pointing rows");
         return MDP_EINVAL;
     }
-    if (params->precond != 0) {
-        mdp_set_error("mdp_gls_solve_mixed: the two-level preconditioners run on the FP64 path (mdp_gls_solve)");
-        return MDP_EUNSUPPORTED;
-    }
     MDP_CUDA(cudaSetDevice(ctx->device));
     auto           tp0 = std::chrono::steady_clock::now();
     const BJState *bjp = nullptr;
@@ -978,6 +974,14 @@ extern "C" int mdp_gls_solve_mixed(mdp_context *ctx, mdp_pointing *A, const mdp_
     }
     const double tol2rel = params->tol * params->tol * res0;
     if (h_res_rel) h_res_rel[0] = 1.0;
+    // two-level preconditioners of the inner PCGs: Z, AZ and E^+ with the FP64
+    // operator; the a-posteriori columns start from the first residual r
+    mdp_twolevel  tlv;
+    mdp_twolevel *tl = nullptr;
+    if (params->precond != 0) {
+        MDP_TRY(mdp_twolevel_build(ctx, A, N, params->precond, params->z_2lvl, r, &tlv));
+        tl = &tlv;
+    }
     double res = res0;
     int    outer = 0, inner_total = 0, converged = (res0 <= params->tol);
     const bool prof = ctx->profile != 0;
@@ -985,7 +989,14 @@ extern "C" int mdp_gls_solve_mixed(mdp_context *ctx, mdp_pointing *A, const mdp_
         // inner PCG on A32 delta = r, delta0 = 0: g = r, Cg = M^-1 g, h = Cg
         MDP_CUDA(cudaMemcpyAsync(g, r, 8 * n, cudaMemcpyDeviceToDevice, st));
         MDP_CUDA(cudaMemsetAsync(dl, 0, 8 * nmap, st));
-        pcg_init_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(inv, g, Cg, h, npix, S);
+        if (tl) {
+            MDP_TRY(mdp_twolevel_qtx(ctx, tl, g));
+            pcg_init_tl_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(inv, g, Cg, h, npix, tl->Z.as<double>(),
+                                                                   tl->AZ.as<double>(), tl->qtx.as<double>(), tl->zn,
+                                                                   S);
+        } else {
+            pcg_init_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(inv, g, Cg, h, npix, S);
+        }
         MDP_CHECK_LAUNCH(ctx);
         MDP_TRY(fetch());
         const double rin0 = hs->res;
@@ -1006,7 +1017,16 @@ extern "C" int mdp_gls_solve_mixed(mdp_context *ctx, mdp_pointing *A, const mdp_
             if (prof) cudaEventRecord(ctx->ev[3], st);
             pcg_coeff_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(h, q, n, S);
             MDP_CHECK_LAUNCH(ctx);
-            pcg_update_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(inv, dl, h, q, gp, g, Cg, npix, S);
+            if (tl) {
+                pcg_step_kernel<<<grid_for(n, 256, ctx->sm_count * 8), 256, 0, st>>>(dl, h, q, gp, g, n, S);
+                MDP_CHECK_LAUNCH(ctx);
+                MDP_TRY(mdp_twolevel_qtx(ctx, tl, g));
+                pcg_precond_tl_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(inv, g, gp, Cg, npix, tl->Z.as<double>(),
+                                                                          tl->AZ.as<double>(), tl->qtx.as<double>(),
+                                                                          tl->zn, S);
+            } else {
+                pcg_update_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(inv, dl, h, q, gp, g, Cg, npix, S);
+            }
             MDP_CHECK_LAUNCH(ctx);
             if (prof) cudaEventRecord(ctx->ev[4], st);
             MDP_TRY(fetch());

@@ -211,3 +211,36 @@ def test_pcg_gls_true_and_mlmap_two_level(gpu_ctx, ref_lib):
     for k in range(3):
         assert np.linalg.norm(maps[k] - refmaps[k]) <= MAP_TOL * np.linalg.norm(refmaps[k])
     assert np.array_equal(maps[4], refmaps[4])
+
+
+@pytest.mark.parametrize("case", ["gaps", "cut_gaps"])
+@pytest.mark.parametrize("precond,zn", [(1, 4), (2, 8)])
+def test_two_level_mixed_precision(gpu_ctx, case, precond, zn):
+    """The two-level preconditioners inside the mixed-precision solve (columns
+    built with the FP64 operator, inner PCGs on the FP32 operator): the map
+    equals the FP64 block-Jacobi solve within 1e-8 on the determined pixels
+    (both to 1e-12)."""
+    import torch
+    import midapack_b200 as mb
+    wl = solver_cases()[case]()
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    outs = []
+    for mixed in (False, True):
+        P = mb.Pointing(gpu_ctx, d(wl.pix), d(wl.weights), wl.n_samples, 3)
+        N = mb.Noise(gpu_ctx, wl.block_sizes, wl.lam, wl.invtt)
+        if mixed:
+            r = mb.gls_solve_mixed(gpu_ctx, P, N, d(wl.signal), d(wl.noise), tol=1e-12, maxiter=900, precond=precond,
+                                   z_2lvl=zn)
+        else:
+            r = mb.gls_solve(gpu_ctx, P, N, d(wl.signal), d(wl.noise), tol=1e-12, maxiter=900)
+        assert r[5].converged
+        outs.append((r[0].cpu().numpy(), r[1].cpu().numpy()))
+    (x64, l64), (x32, l32) = outs
+    assert np.array_equal(l64, l32)
+    o = R.pcg(wl.pix, wl.weights, wl.signal, wl.noise, wl.block_sizes, wl.lam, wl.invtt, tol=1e-10, maxiter=400)
+    W, _ = R.local_W(o.bj.A, wl.block_sizes, wl.lam, wl.invtt)
+    ev = np.linalg.eigvalsh(W)
+    det = np.repeat(ev[:, 0] > 1e-6 * ev[:, 2], 3)
+    for s in range(3):
+        sel = det[s::3]
+        assert _rel(x32[s::3][sel], x64[s::3][sel]) < 1e-8, (s, _rel(x32[s::3][sel], x64[s::3][sel]))
