@@ -314,6 +314,19 @@ def bench_fknee(args, device):
     return out
 
 
+def run_part(fn, args, device):
+    """One auxiliary part of the bench line; a part that fails is reported on
+    the line (its error) instead of ending the run without a line."""
+    try:
+        return fn(args, device)
+    except Exception as ex:  # noqa: BLE001
+        import torch
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        sys.stderr.write(f"bench part {fn.__name__} failed: {type(ex).__name__}: {ex}\n")
+        return {"error": f"{type(ex).__name__}: {ex}"}
+
+
 def bench_c1(args, device):
     """The CPU-runnable configuration (4 detectors x 2^20 samples, 256x192 px,
     lambda 2^12, one Toeplitz block per detector) with 1% flagged samples (without
@@ -669,9 +682,13 @@ def main():
     # end to end through the reference-facing API with host buffers
     e2e = None
     if pinned:
-        e2e = run_e2e_device_api(args, wl, world, pinned)
-        # the reference's own entry point (MLmap: FP64, host maps out) on the same inputs
-        e2e["mlmap_fp64"] = run_e2e(args, wl, world, pinned)
+        try:
+            e2e = run_e2e_device_api(args, wl, world, pinned)
+            # the reference's own entry point (MLmap: FP64, host maps out) on the same inputs
+            e2e["mlmap_fp64"] = run_e2e(args, wl, world, pinned)
+        except Exception as ex:  # noqa: BLE001 - reported on the line
+            sys.stderr.write(f"e2e failed: {type(ex).__name__}: {ex}\n")
+            e2e = dict(e2e or {"value": None, "unit": "s"}, error=f"{type(ex).__name__}: {ex}")
     pinned = None
 
     # multi-RHS and serving configurations (one GPU: rank 0 of a single-process run)
@@ -679,16 +696,16 @@ def main():
     ctx.trim()
     c1 = None
     if world == 1 and not args.no_c1:
-        c1 = bench_c1(args, local)
+        c1 = run_part(bench_c1, args, local)
     if world == 1 and not args.no_fknee:
-        fknee = bench_fknee(args, local)
+        fknee = run_part(bench_fknee, args, local)
     solvers = None
     if world == 1 and not args.no_solvers:
-        solvers = bench_solvers(args, local)
+        solvers = run_part(bench_solvers, args, local)
     if world == 1 and not args.no_multi:
-        multi = bench_multi(args, local)
+        multi = run_part(bench_multi, args, local)
     if world == 1 and not args.no_serve:
-        serve_out = bench_serving(args, local)
+        serve_out = run_part(bench_serving, args, local)
 
     if rank == 0:
         line = {
