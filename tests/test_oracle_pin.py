@@ -177,3 +177,26 @@ def test_ecg_restatement_solves_the_reference_system(ref_lib, case, enl, ortho, 
     for k in range(3):
         s = det[k::3]
         assert _rel(e.x[k::3][s], xr[k::3][s]) < 1e-8
+
+
+def test_cpu_baseline_mlmap_mode(ref_lib, tmp_path):
+    """bench.py's reference-MLmap leg (python -m oracle.cpu_baseline --mlmap):
+    its maps equal the in-process reference MLmap on the same case."""
+    import json
+    import subprocess
+    import sys
+    wl = synth.small(n_det=2, n_samp=2048, block_len=1024, lam=32, seed=52, gap_frac=0.02)
+    case, out = tmp_path / "case.npz", tmp_path / "maps.npz"
+    np.savez(case, pix=wl.pix, weights=wl.weights, signal=wl.signal, noise=wl.noise, block_sizes=wl.block_sizes,
+             lam=wl.lam, invtt=wl.invtt, nside=wl.nside, tol=1e-10, maxiter=300)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-m", "oracle.cpu_baseline", "--mlmap", str(case), "2", str(out)], cwd=root,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
+    assert line["ranks"] == 2 and line["iterations"] > 0
+    m = np.load(out)
+    ref = ref_lib.mlmap(2, [wl.n_samples // 2] * 2, [len(wl.block_sizes) // 2] * 2, wl.block_sizes, wl.pix, wl.weights,
+                        wl.signal, wl.noise, wl.lam, wl.invtt, wl.nside, tol=1e-10, maxiter=300)
+    for k, name in enumerate(("I", "Q", "U")):
+        assert np.array_equal(m[name], ref[k])
