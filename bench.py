@@ -67,7 +67,8 @@ def parse():
     ap.add_argument("--no-fknee", action="store_true", help="skip the f_knee sweep part")
     ap.add_argument("--no-c1", action="store_true", help="skip the CPU-runnable reference comparison")
     ap.add_argument("--no-solvers", action="store_true", help="skip the two-level / ECG part")
-    ap.add_argument("--only", default="", choices=["", "multi", "serve", "fknee", "c1", "solvers"],
+    ap.add_argument("--no-noise", action="store_true", help="skip the noise2invtt part")
+    ap.add_argument("--only", default="", choices=["", "multi", "serve", "fknee", "c1", "solvers", "noise"],
                     help="run only the multi-RHS, serving or f_knee part (prints their JSON)")
     ap.add_argument("--multi-rhs", type=int, default=128, help="right-hand sides of the multi-RHS part")
     ap.add_argument("--multi-fp64-cols", type=int, default=2, help="columns timed with the plain FP64 path")
@@ -401,6 +402,63 @@ def bench_c1(args, device):
     return out
 
 
+def bench_noise2invtt(args, device):
+    """noise2invtt (mappraiser/python/TOAST_interface/utils.py:500-602) for every
+    stationary interval of the at-scale workload: 1024 intervals x 2^20 samples,
+    lambda 2^14, chebwin window.  The device path (periodogram, fit, inverse row of
+    each interval; noise resident on the device; CUDA events around the call, best
+    of 2 after a warm-up) against the reference's algorithm (the scipy
+    restatement with curve_fit's default tolerances, one host core) on a sample of
+    2 intervals, extrapolated to all 1024, and the device rows' error against that
+    restatement's rows (bounded by curve_fit's ftol = 1e-8)."""
+    import torch
+    import midapack_b200 as mb
+    from midapack_b200 import noise as mn
+    from midapack_b200 import synth
+    from oracle import restate
+    nblk, n, lam, distinct = 1024, 1 << 20, 1 << 14, 8
+    rng = np.random.default_rng(20261212)
+    blocks = [synth.noise_tod(n, fk, rng) for fk in np.linspace(0.1, 5.0, distinct)]
+    d_noise = torch.from_numpy(np.concatenate(blocks)).cuda().repeat(nblk // distinct)
+    sizes = np.full(nblk, n, dtype=np.int32)
+    ctx = mb.Context(device)
+    times = []
+    for rep in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        l0 = ctx.launches
+        e0.record()
+        out, params, evals = mn.invtt_blocks(d_noise, sizes, lam, 100.0, "chebwin", ctx=ctx, return_fit=True)
+        e1.record()
+        torch.cuda.synchronize()
+        launches = ctx.launches - l0
+        if rep:
+            times.append(e0.elapsed_time(e1) / 1e3)
+    rows = out.view(nblk, lam).cpu().numpy()
+    del d_noise, out
+    cpu_t, errs = [], []
+    for b in range(2):
+        t0 = time.perf_counter()
+        r, _, _ = restate.noise2invtt(blocks[b], n, lam, 100.0, "chebwin")
+        cpu_t.append(time.perf_counter() - t0)
+        errs.append(float(np.linalg.norm(rows[b] - r) / np.linalg.norm(r)))
+    dev = min(times)
+    cpu_all = float(np.mean(cpu_t)) * nblk
+    ctx.close()
+    torch.cuda.empty_cache()
+    return {"workload": f"{nblk} intervals x 2^20 samples, lambda 2^14, chebwin ({distinct} distinct seeded 1/f "
+                        f"streams, f_knee 0.1-5 Hz, tiled)",
+            "device_s": round(dev, 4), "intervals_per_s": round(nblk / dev, 1),
+            "samples_per_s": round(nblk * n / dev, 1), "gpu_launches": int(launches),
+            "fit_evaluations_mean": round(float(evals.mean()), 1), "fit_evaluations_max": int(evals.max()),
+            "cpu_reference_algorithm": {"kind": "port", "cores": 1, "sample": "2 intervals (scipy welch + "
+                                        "curve_fit + irfft), extrapolated x512",
+                                        "s_per_interval": round(float(np.mean(cpu_t)), 3),
+                                        "extrapolated_s": round(cpu_all, 1)},
+            "speedup_vs_cpu": round(cpu_all / dev, 1),
+            "row_rel_err_vs_reference_algorithm": max(errs)}
+
+
 def bench_solvers(args, device):
     """The reference's other solvers and preconditioners on the CPU-runnable
     workload at low f_knee (0.1 Hz, the ill-conditioned end of the sweep), 1%
@@ -533,7 +591,7 @@ def main():
     torch.cuda.set_device(local)
     if args.only:
         r = {"multi": bench_multi, "serve": bench_serving, "fknee": bench_fknee, "c1": bench_c1,
-             "solvers": bench_solvers}[args.only](args, local)
+             "solvers": bench_solvers, "noise": bench_noise2invtt}[args.only](args, local)
         print(json.dumps({args.only: r}), flush=True)
         return 0
     if world > 1:
@@ -702,6 +760,9 @@ def main():
     solvers = None
     if world == 1 and not args.no_solvers:
         solvers = run_part(bench_solvers, args, local)
+    noise_part = None
+    if world == 1 and not args.no_noise:
+        noise_part = run_part(bench_noise2invtt, args, local)
     if world == 1 and not args.no_multi:
         multi = run_part(bench_multi, args, local)
     if world == 1 and not args.no_serve:
@@ -736,6 +797,8 @@ def main():
             line["mixed_fknee_sweep"] = fknee
         if solvers:
             line["solvers_low_fknee"] = solvers
+        if noise_part:
+            line["noise2invtt"] = noise_part
         if multi:
             line["multi_rhs"] = multi
         if serve_out:

@@ -30,6 +30,7 @@ extern "C" {
 #define MDP_EUNSUPPORTED 4 /* valid input this build does not handle */
 #define MDP_ENAN         5 /* NaN/Inf met in a reduction */
 #define MDP_ETIMEOUT     6 /* a bounded device-side wait gave up */
+#define MDP_ENOCONV      7 /* an iterative fit did not converge within its evaluation limit */
 
 typedef struct mdp_context  mdp_context;
 typedef struct mdp_pointing mdp_pointing;
@@ -276,6 +277,34 @@ int  mdp_gls_residual(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, con
 /* d_q = P^T N^-1 P d_h (maps FP64); fp32 = 1 runs the FP32 operator of the
  * mixed-precision solver. */
 int  mdp_apply_op(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *d_h, double *d_q, int fp32);
+
+/* ---- inverse-noise first rows from noise timestreams -------------------
+ * compute_invtt / noise2invtt (mappraiser/python/TOAST_interface/utils.py:439-481,
+ * 500-602), which the reference runs in Python (scipy) before MLmap.  Blocks are
+ * consecutive in d_noise: block b has h_n[b] samples.  FP64 throughout. */
+#define MDP_APOD_CHEBWIN  0   /* scipy get_window(("chebwin", 150), 2*lambda) */
+#define MDP_APOD_GAUSSIAN 1   /* scipy get_window(("general_gaussian", 1, lambda/3), 2*lambda) */
+/* The apodisation window after ifftshift, first lambda points (utils.py:567-582). */
+int  mdp_apod_window(mdp_context *ctx, int lambda, int apod, double *d_window);
+/* scipy.signal.welch(x_b, fsamp, window='hann', nperseg=h_n[b], detrend='linear')
+ * of every block (utils.py:531): d_psd gets h_n[b]/2 + 1 values per block, blocks
+ * one after the other.  h_n[b] >= 4. */
+int  mdp_periodogram(mdp_context *ctx, int nb, const int32_t *h_n, const double *d_noise, double fsamp,
+                     double *d_psd);
+/* noise2invtt of every block: periodogram, fit of the log PSD model
+ * a + log10(1 + ((f + fmin)/fknee)^alpha) under the reference's bounds and
+ * starting point (bounded Levenberg-Marquardt run to the least-squares minimum),
+ * inverse PSD, irfft, times the window.  d_invtt gets nb*lambda doubles (block
+ * b at b*lambda); h_params (nb*4: a, alpha, fknee, fmin) and h_evals (model
+ * evaluations per block, -1 when not converged) may be NULL.  Errors: MDP_EINVAL
+ * when lambda > h_n[b]/2 ("Bandwidth cannot be larger than timestream") or a
+ * block has fewer than 8 samples; MDP_EUNSUPPORTED when a block needs a
+ * transform longer than 2^24 points (a power of two above 2^24 samples, any
+ * other length above 2^23); MDP_ENAN when a periodogram value is zero or not
+ * finite; MDP_ENOCONV (outputs written) when a fit used 1000 evaluations,
+ * curve_fit's maxfev. */
+int  mdp_noise2invtt(mdp_context *ctx, int nb, const int32_t *h_n, const double *d_noise, int lambda, double fsamp,
+                     int apod, double *d_invtt, double *h_params, int32_t *h_evals);
 
 #ifdef __cplusplus
 }

@@ -17,6 +17,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libmidapack_b200.so")
 
 MDP_OK = 0
+MDP_ENOCONV = 7
 _lib = None
 
 c_i32p = ct.POINTER(ct.c_int32)
@@ -114,6 +115,10 @@ _SIGS = {
     "mdp_ecg_solve": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                  ct.POINTER(ECGParams), ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                  c_f64p, ct.POINTER(SolveInfo)]),
+    "mdp_apod_window": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p]),
+    "mdp_periodogram": (ct.c_int, [ct.c_void_p, ct.c_int, c_i32p, ct.c_void_p, ct.c_double, ct.c_void_p]),
+    "mdp_noise2invtt": (ct.c_int, [ct.c_void_p, ct.c_int, c_i32p, ct.c_void_p, ct.c_int, ct.c_double, ct.c_int,
+                                   ct.c_void_p, c_f64p, c_i32p]),
     # reference-compatible host API (include/mapmat.h, toeplitz.h, mappraiser.h)
     "MatInit": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, c_i32p, c_f64p, ct.c_int, ct.c_int]),
     "MatSetIndices": (None, [ct.c_void_p, ct.c_int, ct.c_int, c_i32p]),

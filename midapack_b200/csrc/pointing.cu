@@ -32,6 +32,7 @@ extern "C" const char *mdp_strerror(int code) {
         case MDP_EUNSUPPORTED: return "unsupported input";
         case MDP_ENAN: return "NaN or Inf in a reduction";
         case MDP_ETIMEOUT: return "device wait timed out";
+        case MDP_ENOCONV: return "fit did not converge";
         default: return "unknown error";
     }
 }

@@ -553,3 +553,56 @@ def x2map_pol(x, lstid, cond, hits, npix):
     Cond[p] = cond
     Hits[p] = hits
     return mapI, mapQ, mapU, Cond, Hits
+
+
+# --------------------------------------------------------------------------- noise2invtt
+NOISE_FIT_P0 = (-7.0, -1.0, 0.1, 1e-6)
+NOISE_FIT_BOUNDS = ([-20.0, -10.0, 0.0, 0.0], [0.0, 0.0, 20.0, 1.0])
+
+
+def logpsd_model(f, a, alpha, fknee, fmin):
+    """logpsd_model (mappraiser/python/TOAST_interface/utils.py:488-489)."""
+    return a + np.log10(1 + ((f + fmin) / fknee) ** alpha)
+
+
+def inversepsd_model(f, sigma, alpha, fknee, fmin):
+    """inversepsd_model (utils.py:492-493)."""
+    return sigma * 1.0 / (1 + ((f + fmin) / fknee) ** alpha)
+
+
+def apod_window(lam: int, apod: str = "chebwin") -> np.ndarray:
+    """Apodisation window after ifftshift, first lam points (utils.py:567-582)."""
+    from scipy.signal import get_window
+    if apod == "gaussian":
+        w = get_window(("general_gaussian", 1, 1 / 3 * lam), 2 * lam)
+    elif apod == "chebwin":
+        w = get_window(("chebwin", 150), 2 * lam)
+    else:
+        raise RuntimeError(f"Apodisation window '{apod}' is not supported.")
+    return np.fft.ifftshift(w)[:lam]
+
+
+def periodogram(x: np.ndarray, fsamp: float):
+    """One-segment Welch periodogram of a block (utils.py:531)."""
+    import scipy.signal
+    return scipy.signal.welch(x, fsamp, window="hann", nperseg=x.size, detrend="linear")
+
+
+def noise2invtt(nsetod: np.ndarray, nn: int, lam: int, fsamp: float, apod: str = "chebwin", tight: bool = False):
+    """noise2invtt (utils.py:500-584): Welch periodogram, curve_fit of the log PSD
+    model, irfft of the inverse PSD, apodisation.  tight=True runs curve_fit to
+    ftol = xtol = gtol = 1e-15 (maxfev 20000): the least-squares minimum, which the
+    reference's defaults (ftol = 1e-8) approach to about 1e-5.  Returns
+    (invtt, popt, psd)."""
+    from scipy.optimize import curve_fit
+    f, psd = periodogram(np.asarray(nsetod, dtype=np.float64), fsamp)
+    kw = dict(ftol=1e-15, xtol=1e-15, gtol=1e-15, maxfev=20000) if tight else dict(maxfev=1000)
+    popt, _ = curve_fit(logpsd_model, f[1:], np.log10(psd[1:]), p0=np.array(NOISE_FIT_P0),
+                        bounds=NOISE_FIT_BOUNDS, **kw)
+    f_full = np.fft.rfftfreq(nn, 1.0 / fsamp)
+    with np.errstate(divide="ignore"):
+        psdm1 = inversepsd_model(f_full, 10 ** (-popt[0]), *popt[1:])
+    inv_tt = np.fft.irfft(psdm1, n=nn)
+    if lam > nn // 2:
+        raise RuntimeError("Bandwidth cannot be larger than timestream.")
+    return np.multiply(apod_window(lam, apod), inv_tt[:lam], dtype=np.float64), popt, psd

@@ -29,3 +29,24 @@ def solver_cases():
             synth.small(n_det=2, n_samp=4096, block_len=2048, lam=64, gap_frac=0.02, seed=24), seed=1),
         "white": lambda: synth.small(n_det=2, n_samp=2048, block_len=1024, lam=1, seed=25),
     }
+
+
+def noise_golden():
+    """Cases of tests/golden/noise2invtt/noise2invtt_ref.npz with their inputs
+    (regenerated from the seed, or the reference's own test noise) and the
+    reference noise2invtt output."""
+    import os
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    d = np.load(os.path.join(here, "noise2invtt", "noise2invtt_ref.npz"))
+    cases, at = [], 0
+    for i, name in enumerate(d["names"]):
+        n, lam, fs, fk, seed = (int(d["n"][i]), int(d["lam"][i]), float(d["fsamp"][i]), float(d["fknee"][i]),
+                                int(d["seed"][i]))
+        if fk == 0.0:
+            x = np.load(os.path.join(here, "ref_fixture_rank1_12000.npz"))["noise"][:n].copy()
+        else:
+            x = synth.noise_tod(n, fk, np.random.default_rng(seed))
+        cases.append(dict(name=str(name), n=n, lam=lam, fsamp=fs, apod=str(d["apod"][i]), noise=x,
+                          invtt=d["invtt"][at:at + lam]))
+        at += lam
+    return cases
