@@ -522,16 +522,23 @@ __global__ void invtt_out_kernel(const double2 *buf, int64_t L, int blue, int64_
 
 // ------------------------------------------------------------------ apodisation windows
 // Dolph-Chebyshev window of M = 2 lam + 1 points (scipy.signal.windows.chebwin, odd M):
-// p_k = T_{M-1}(beta cos(pi k / M)), w_n = sum_k p_k cos(2 pi n k / M) (p_k = p_{M-k}).
-__global__ void cheb_p_kernel(double *p, int lam, double beta) {
+// p_k = T_{M-1}(x_k), x_k = beta cos(pi k / M), w_n = sum_k p_k cos(2 pi n k / M)
+// (p_k = p_{M-k}).  Near x = 1, T_{M-1} amplifies the rounding of x by up to (M-1)^2,
+// so x - 1 is formed directly, (beta - 1) - 2 beta sin^2(pi k / 2M) with
+// beta - 1 = 2 sinh^2(t/2), and T_{M-1}(x) = cos((M-1) 2 asin(sqrt((1-x)/2))) for
+// |x| <= 1, cosh((M-1) 2 asinh(sqrt((x-1)/2))) for x > 1.  (scipy evaluates
+// cos((M-1) acos(x)) of a rounded x: its window is off by up to 5e-9 at lam = 2^14;
+// this form is exact to about 1e-15.)
+__global__ void cheb_p_kernel(double *p, int lam, double beta, double beta_m1) {
     const int64_t M = 2 * (int64_t) lam + 1;
     const double order = (double) (M - 1);
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= lam; k += gridDim.x * blockDim.x) {
-        const double x = beta * cospi((double) k / (double) M);
+        const double s = sinpi((double) k / (double) (2 * M));
+        const double d = beta_m1 - 2.0 * beta * s * s;   // x - 1
         double v;
-        if (x > 1.0) v = cosh(order * acosh(x));
-        else if (x < -1.0) v = cosh(order * acosh(-x));   // M odd
-        else v = cos(order * acos(x));
+        if (d > 0.0) v = cosh(order * 2.0 * asinh(sqrt(0.5 * d)));
+        else if (d >= -2.0) v = cos(order * 2.0 * asin(sqrt(-0.5 * d)));
+        else v = cosh(order * acosh(-1.0 - d));   // x < -1: not reached for k <= lam, M odd
         p[k] = v;
     }
 }
@@ -605,8 +612,9 @@ int window_impl(mdp_context *ctx, int lam, int apod, double *d_win) {
     MDP_TRY(cbh.alloc((size_t) sh.L * sizeof(double2)));
     double *p = pw.as<double>(), *w = p + lam + 1;
     const double order = 2.0 * lam;
-    const double beta = std::cosh(1.0 / order * std::acosh(std::pow(10.0, 150.0 / 20.0)));
-    cheb_p_kernel<<<grid_for(lam + 1, 256), 256, 0, ctx->stream>>>(p, lam, beta);
+    const double t = 1.0 / order * std::acosh(std::pow(10.0, 150.0 / 20.0));
+    const double sht = std::sinh(0.5 * t);
+    cheb_p_kernel<<<grid_for(lam + 1, 256), 256, 0, ctx->stream>>>(p, lam, std::cosh(t), 2.0 * sht * sht);
     MDP_CHECK_LAUNCH(ctx);
     const int g = grid_for(sh.L, 256);
     chirp_filter_kernel<<<g, 256, 0, ctx->stream>>>(cbh.as<double2>(), M, sh.L, -1);

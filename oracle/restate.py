@@ -582,6 +582,24 @@ def apod_window(lam: int, apod: str = "chebwin") -> np.ndarray:
     return np.fft.ifftshift(w)[:lam]
 
 
+def chebwin_exact(lam: int) -> np.ndarray:
+    """Arbiter for the chebwin window of apod_window: the same Dolph-Chebyshev
+    window (scipy.signal.windows.chebwin, 2*lam + 1 points, 150 dB, ifftshift,
+    first lam) with its samples T_{2 lam}(beta cos(pi k/M)) evaluated in 30-digit
+    arithmetic (mpmath), then an FP64 FFT.  scipy's own window differs from it by
+    up to 5e-9 at lam = 2^14 (rounding of beta cos(pi k/M) amplified near 1)."""
+    import mpmath
+    mpmath.mp.dps = 30
+    M = 2 * lam + 1
+    beta = mpmath.cosh(mpmath.acosh(mpmath.mpf(10) ** (mpmath.mpf(150) / 20)) / (M - 1))
+    p = np.empty(lam + 1)
+    for k in range(lam + 1):
+        x = beta * mpmath.cos(mpmath.pi * k / M)
+        p[k] = float(mpmath.cosh((M - 1) * mpmath.acosh(x)) if x > 1 else mpmath.cos((M - 1) * mpmath.acos(x)))
+    w = np.real(np.fft.fft(np.concatenate([p, p[1:][::-1]])))[:lam + 1]
+    return w[:lam] / w.max()
+
+
 def periodogram(x: np.ndarray, fsamp: float):
     """One-segment Welch periodogram of a block (utils.py:531)."""
     import scipy.signal
