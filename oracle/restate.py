@@ -606,6 +606,14 @@ def periodogram(x: np.ndarray, fsamp: float):
     return scipy.signal.welch(x, fsamp, window="hann", nperseg=x.size, detrend="linear")
 
 
+def fit_cost(psd: np.ndarray, nn: int, fsamp: float, params) -> float:
+    """Least-squares cost of noise2invtt's fit (utils.py:534-541) at params:
+    0.5 * sum (logpsd_model(f[1:], *params) - log10 psd[1:])^2."""
+    f = np.fft.rfftfreq(nn, 1.0 / fsamp)
+    r = logpsd_model(f[1:], *params) - np.log10(psd[1:])
+    return 0.5 * float(r @ r)
+
+
 def noise2invtt(nsetod: np.ndarray, nn: int, lam: int, fsamp: float, apod: str = "chebwin", tight: bool = False):
     """noise2invtt (utils.py:500-584): Welch periodogram, curve_fit of the log PSD
     model, irfft of the inverse PSD, apodisation.  tight=True runs curve_fit to

@@ -8,9 +8,12 @@ checked to 1e-14 (absolute, windows peak at 1; the chebwin against a 30-digit
 evaluation, since scipy's own chebwin is off by up to 5e-9) and 1e-12
 (relative norm).  The
 inverse-noise rows come out of a nonlinear fit: the device fit runs to the
-least-squares minimum, checked to 1e-7 (relative norm) against curve_fit run
-to ftol = xtol = gtol = 1e-15; the reference's own curve_fit stops at
-ftol = 1e-8, so its rows are checked to 1e-4."""
+least-squares minimum, so its cost is checked to be no higher than that of
+curve_fit run to ftol = xtol = gtol = 1e-15 (times 1 + 1e-12), and its rows
+against that fit's rows to 1e-6 (relative norm: the minimum is flat along
+(alpha, fmin), where costs equal to 1e-14 still move the rows by ~1e-7); the
+reference's own curve_fit stops at ftol = 1e-8, so its rows are checked to
+1e-4."""
 import numpy as np
 import pytest
 
@@ -72,9 +75,11 @@ def test_noise2invtt_matches_oracle_and_reference(gpu_ctx, case):
     out, params, evals = noise.invtt_blocks(case["noise"], [case["n"]], case["lam"], case["fsamp"], case["apod"],
                                             ctx=gpu_ctx, return_fit=True)
     got = out.cpu().numpy()
-    tight, popt, _ = restate.noise2invtt(case["noise"], case["n"], case["lam"], case["fsamp"], case["apod"],
-                                         tight=True)
-    assert rel(got, tight) <= 1e-7
+    tight, popt, psd = restate.noise2invtt(case["noise"], case["n"], case["lam"], case["fsamp"], case["apod"],
+                                           tight=True)
+    assert restate.fit_cost(psd, case["n"], case["fsamp"], params[0]) <= \
+        restate.fit_cost(psd, case["n"], case["fsamp"], popt) * (1 + 1e-12)
+    assert rel(got, tight) <= 1e-6
     assert rel(got, case["invtt"]) <= 1e-4
     assert 0 < evals[0] < 1000
     np.testing.assert_allclose(params[0][:3], popt[:3], rtol=1e-4)
@@ -94,7 +99,7 @@ def test_compute_invtt_ragged_blocks(gpu_ctx):
     assert noise.compute_invtt(2, 3, x, np.array(sizes), lam, 100.0, buf, np.float64, ctx=gpu_ctx) is None
     for b, blk in enumerate(blocks):
         tight, _, _ = restate.noise2invtt(blk, sizes[b], lam, 100.0, "chebwin", tight=True)
-        assert rel(buf[b * lam:(b + 1) * lam], tight) <= 1e-7, b
+        assert rel(buf[b * lam:(b + 1) * lam], tight) <= 1e-6, b
     assert np.all(buf[-3:] == -7.0)
 
 
@@ -107,7 +112,7 @@ def test_noise2invtt_interval_of_2p20_samples(gpu_ctx):
     out = noise.invtt_blocks(np.concatenate([x, x]), [n, n], lam, 100.0, "chebwin", ctx=gpu_ctx).cpu().numpy()
     assert np.array_equal(out[:lam], out[lam:])
     tight, _, _ = restate.noise2invtt(x, n, lam, 100.0, "chebwin", tight=True)
-    assert rel(out[:lam], tight) <= 1e-7
+    assert rel(out[:lam], tight) <= 1e-6
 
 
 def test_noise2invtt_single_block_api(gpu_ctx):
