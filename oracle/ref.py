@@ -137,3 +137,58 @@ def operator_time(nranks, data_size_proc, nb_blocks_proc, block_sizes, pix, weig
         if rc != 0:
             raise RuntimeError(f"reference operator timing failed (status {rc})")
         return float(np.fromfile(path, dtype=np.float64)[0])
+
+
+def _scan_args(sc):
+    nsweeps = np.array([len(s) - 1 for s in sc.sweeps], dtype=np.int32)
+    flat = lambda rows, dt: np.ascontiguousarray(np.concatenate([np.asarray(r) for r in rows]), dtype=dt)  # noqa: E731
+    sweeps = flat(sc.sweeps, np.int32)
+    az = flat(sc.az, np.float64) if sc.ground else np.zeros(int(sum(sc.ces_length(i) for i in range(sc.nces))))
+    hwp = flat(sc.hwp, np.float64) if sc.nhwp else np.zeros_like(az)
+    azmin = np.ascontiguousarray(sc.az_min, dtype=np.float64)
+    azmax = np.ascontiguousarray(sc.az_max, dtype=np.float64)
+    return nsweeps, sweeps, az, azmin, azmax, hwp
+
+
+def templates_ops(sc, w_block, d, tau):
+    """The reference's TrTVecProd, TVecProd, BuildKernel and InvKernel on the template
+    classes MTmap builds (ref_templates_ops).  Returns (T^T d, T tau, kernels,
+    pseudo-inverses), kernels block after block."""
+    nsw, sw, az, azmin, azmax, hwp = _scan_args(sc)
+    wb = np.ascontiguousarray(w_block, dtype=np.float64)
+    dd = np.ascontiguousarray(d, dtype=np.float64)
+    tt = np.ascontiguousarray(tau, dtype=np.float64)
+    amp = np.zeros(sc.n_templates)
+    tod = np.zeros(dd.size)
+    kern = np.zeros(sc.kernel_size)
+    kinv = np.zeros(sc.kernel_size)
+    r = lib().ref_templates_ops(sc.nces, sc.ndet, _p(nsw, I32), _p(sw, I32), _p(az, F64), _p(azmin, F64),
+                                _p(azmax, F64), _p(hwp, F64), sc.npoly, sc.ground, sc.n_sss_bins, sc.nhwp,
+                                F64(sc.delta_t), F64(sc.fs), _p(wb, F64), _p(dd, F64), _p(tt, F64), _p(amp, F64),
+                                _p(tod, F64), _p(kern, F64), _p(kinv, F64))
+    if r != sc.n_templates:
+        raise RuntimeError(f"reference built {r} templates, expected {sc.n_templates}")
+    return amp, tod, kern, kinv
+
+
+def mtmap(sc, pix, weights, signal, noise, invtt, nside, tol=1e-8, maxiter=500, nnz=3):
+    """MTmap on one rank (ref_mtmap); returns the I, Q, U, Cond, Hits maps and the
+    residual history."""
+    nsw, sw, az, azmin, azmax, hwp = _scan_args(sc)
+    px = np.ascontiguousarray(pix, dtype=np.int32)
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    s = np.ascontiguousarray(signal, dtype=np.float64)
+    nz = np.ascontiguousarray(noise, dtype=np.float64)
+    tt = np.ascontiguousarray(invtt, dtype=np.float64)
+    with tempfile.TemporaryDirectory() as td:
+        rc = lib().ref_mtmap(td.encode(), b"oracle", sc.nces, sc.ndet, _p(nsw, I32), _p(sw, I32), _p(az, F64),
+                             _p(azmin, F64), _p(azmax, F64), _p(hwp, F64), sc.npoly, sc.ground, sc.n_sss_bins,
+                             sc.nhwp, F64(sc.delta_t), F64(sc.fs), F64(tol), maxiter, nside, nnz, _p(px, I32),
+                             _p(w, F64), _p(s, F64), _p(nz, F64), _p(tt, F64))
+        if rc != 0:
+            raise RuntimeError(f"reference MTmap failed (status {rc})")
+        rd = lambda name, dt: np.fromfile(os.path.join(td, f"{name}_oracle.fits"), dtype=dt)  # noqa: E731
+        out = (rd("mapI", np.float64), rd("mapQ", np.float64), rd("mapU", np.float64), rd("Cond", np.float64),
+               rd("Hits", np.int32))
+        res = np.fromfile(os.path.join(td, "pcg_residuals_oracle.dat"), dtype=np.float64)
+    return out + (res,)

@@ -14,7 +14,11 @@
  *   ref_pcg           MLmap's set-up (mappraiser.c:64-200) + PCG_GLS_true (pcg_true.c:20-241)
  *   ref_mlmap         MLmap on n forked ranks (mappraiser.c:34-385)
  *   ref_operator_time one A = P^T N^-1 P application, timed (CPU baseline)
+ *   ref_templates_ops MTmap's template classes (Tlist_init) + TrTVecProd, TVecProd,
+ *                     BuildKernel, InvKernel (algebra/src/templates/templates.c)
+ *   ref_mtmap         MTmap on one rank (mappraiser.c:387-800, PCG_GLS_templates)
  */
+#include <math.h>
 #include <mpi.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -269,4 +273,149 @@ int ref_operator_time(int nranks, int nnz, int lambda, int reps, int *data_size_
     optime_args a = {nranks, nnz, lambda, reps, data_size_proc, nb_blocks_proc, block_sizes, pix, weights,
                      invtt,  NULL, (double *) result_path};
     return shim_mpi_run(nranks, optime_rank, &a);
+}
+
+/* ---- templates: the operators of MTmap's filtered solve ------------------
+ * (algebra/src/templates/templates.c; MTmap's set-up, mappraiser/src/mappraiser.c:586-660).
+ * nces CESs x ndet detectors, block (i, j) = i*ndet + j of ces_length[i] =
+ * sweeps[i][nsweeps[i]] samples.  sweeps_flat: the nces rows of nsweeps[i] + 1 stamps one
+ * after the other; az_flat, hwp_flat: the nces rows of ces_length[i] samples.  As MTmap:
+ * az bins by bin_az, hwp_mod = (cos, sin) of the HWP angle, classes by Tlist_init with
+ * weights on the fly.  Outputs: amp = T^T d (TrTVecProd), tod = T tau (TVecProd), and per
+ * block the kernel w_b T_b^T T_b (BuildKernel) in kern and its pseudo-inverse (InvKernel)
+ * in kinv, blocks one after the other.  Returns the number of template amplitudes. */
+#include "templates.h"
+
+static int **rows_i(int nces, const int *len, int *flat) {
+    int **r = (int **) malloc(sizeof(int *) * (size_t) nces);
+    for (int i = 0, at = 0; i < nces; at += len[i], i++) r[i] = flat + at;
+    return r;
+}
+static double **rows_d(int nces, const int *len, double *flat) {
+    double **r = (double **) malloc(sizeof(double *) * (size_t) nces);
+    for (int i = 0, at = 0; i < nces; at += len[i], i++) r[i] = flat + at;
+    return r;
+}
+
+int ref_templates_ops(int nces, int ndet, int *nsweeps, int *sweeps_flat, double *az_flat, double *az_min,
+                      double *az_max, double *hwp_flat, int npoly, int ground, int n_sss_bins, int nhwp,
+                      double delta_t, double fs, double *w_block, double *d, double *tau, double *amp, double *tod,
+                      double *kern, double *kinv) {
+    int *slen = (int *) malloc(sizeof(int) * (size_t) nces);
+    for (int i = 0; i < nces; i++) slen[i] = nsweeps[i] + 1;
+    int **sweeptstamps = rows_i(nces, slen, sweeps_flat);
+    int *ces_length = (int *) malloc(sizeof(int) * (size_t) nces);
+    int *hwp_bins = (int *) malloc(sizeof(int) * (size_t) nces);
+    int **detnsweeps = (int **) malloc(sizeof(int *) * (size_t) nces);
+    for (int i = 0; i < nces; i++) {
+        ces_length[i] = sweeptstamps[i][nsweeps[i]];
+        hwp_bins[i] = (int) ceil(ces_length[i] / (delta_t * fs));
+        detnsweeps[i] = (int *) malloc(sizeof(int) * (size_t) ndet);
+        for (int j = 0; j < ndet; j++) detnsweeps[i][j] = nsweeps[i];
+    }
+    double **az = rows_d(nces, ces_length, az_flat);
+    double **hwp_angle = rows_d(nces, ces_length, hwp_flat);
+    int **az_binned = bin_az(az, az_min, az_max, ces_length, ground, n_sss_bins, nces);
+    double ***hwp_mod = (double ***) malloc(sizeof(double **) * (size_t) nces);
+    for (int i = 0; i < nces && nhwp; i++) {
+        hwp_mod[i] = (double **) malloc(2 * sizeof(double *));
+        hwp_mod[i][0] = (double *) malloc(sizeof(double) * (size_t) ces_length[i]);
+        hwp_mod[i][1] = (double *) malloc(sizeof(double) * (size_t) ces_length[i]);
+        for (int t = 0; t < ces_length[i]; t++) {
+            hwp_mod[i][0][t] = cos(hwp_angle[i][t]);
+            hwp_mod[i][1][t] = sin(hwp_angle[i][t]);
+        }
+    }
+    int nb = nces * ndet;
+    int *block_sizes = (int *) malloc(sizeof(int) * (size_t) nb);
+    for (int i = 0; i < nces; i++)
+        for (int j = 0; j < ndet; j++) block_sizes[i * ndet + j] = ces_length[i];
+    int n_class = npoly + ground + 2 * nhwp;
+    TemplateClass *X = (TemplateClass *) malloc(sizeof(TemplateClass) * (size_t) n_class * nb);
+    Tlist_init(X, ndet, nces, block_sizes, detnsweeps, ces_length, sweeptstamps, n_sss_bins, az_binned, fs, npoly,
+               ground, nhwp, delta_t, 0, hwp_mod);
+    TrTVecProd(X, nces, n_class * ndet, fs, ces_length, sweeptstamps, az_binned, hwp_mod, nhwp, delta_t, 0, d, amp);
+    TVecProd(X, nces, n_class * ndet, fs, ces_length, sweeptstamps, az_binned, hwp_mod, nhwp, delta_t, 0, tau, tod);
+    int ntot = 0;
+    size_t at = 0;
+    for (int i = 0; i < nces; i++) {
+        hwpss_w hw;
+        memset(&hw, 0, sizeof(hw));
+        if (nhwp) build_hwpss_w(&hw, hwp_mod[i], ces_length[i], nhwp, i);
+        int nt = npoly * nsweeps[i] + ground * n_sss_bins + 2 * nhwp * hwp_bins[i];
+        for (int j = 0; j < ndet; j++) {
+            double *Bk = kern + at;
+            memset(Bk, 0, sizeof(double) * (size_t) nt * nt);
+            BuildKernel(X + (i * ndet + j) * n_class, n_class, Bk, w_block[i * ndet + j], sweeptstamps[i],
+                        ground ? az_binned[i] : NULL, hw, delta_t, fs);
+            double *tmp = (double *) malloc(sizeof(double) * (size_t) nt * nt);
+            double *binv = (double *) calloc((size_t) nt * nt, sizeof(double));
+            memcpy(tmp, Bk, sizeof(double) * (size_t) nt * nt);
+            InvKernel(tmp, nt, binv);
+            memcpy(kinv + at, binv, sizeof(double) * (size_t) nt * nt);
+            free(tmp);
+            free(binv);
+            at += (size_t) nt * nt;
+            ntot += nt;
+        }
+        if (nhwp) free_hwpss_w(&hw, nhwp);
+    }
+    return ntot;
+}
+
+/* ---- MTmap on one rank (mappraiser/src/mappraiser.c:387-800): the template-filtered
+ * solve (PCG_GLS_templates, pcg_true.c:243-560) with white noise per block (invtt: one
+ * weight per block); maps written like MLmap's. */
+typedef struct {
+    const char *outpath, *ref;
+    int nces, ndet, npoly, ground, n_sss_bins, nhwp, maxiter, nside, nnz;
+    double delta_t, fs, tol;
+    int *nsweeps, *sweeps_flat, *pix;
+    double *az_flat, *az_min, *az_max, *hwp_flat, *weights, *signal, *noise, *invtt;
+} mtmap_args;
+
+static void mtmap_rank(int rank, void *vp) {
+    (void) rank;
+    mtmap_args *a = (mtmap_args *) vp;
+    int nces = a->nces;
+    int *slen = (int *) malloc(sizeof(int) * (size_t) nces);
+    for (int i = 0; i < nces; i++) slen[i] = a->nsweeps[i] + 1;
+    int **sweeptstamps = rows_i(nces, slen, a->sweeps_flat);
+    int *ces_length = (int *) malloc(sizeof(int) * (size_t) nces);
+    int m = 0;
+    for (int i = 0; i < nces; i++) {
+        ces_length[i] = sweeptstamps[i][a->nsweeps[i]];
+        m += ces_length[i] * a->ndet;
+    }
+    double **az = rows_d(nces, ces_length, a->az_flat);
+    double **hwp_angle = rows_d(nces, ces_length, a->hwp_flat);
+    int nb = nces * a->ndet;
+    int *block_sizes = (int *) malloc(sizeof(int) * (size_t) nb);
+    for (int i = 0; i < nces; i++)
+        for (int j = 0; j < a->ndet; j++) block_sizes[i * a->ndet + j] = ces_length[i];
+    int *pix = (int *) malloc(sizeof(int) * (size_t) m * a->nnz);
+    double *w = (double *) malloc(sizeof(double) * (size_t) m * a->nnz);
+    double *sig = (double *) malloc(sizeof(double) * (size_t) m);
+    double *noi = (double *) malloc(sizeof(double) * (size_t) m);
+    memcpy(pix, a->pix, sizeof(int) * (size_t) m * a->nnz);
+    memcpy(w, a->weights, sizeof(double) * (size_t) m * a->nnz);
+    memcpy(sig, a->signal, sizeof(double) * (size_t) m);
+    memcpy(noi, a->noise, sizeof(double) * (size_t) m);
+    int dsp[1] = {m};
+    MTmap(MPI_COMM_WORLD, (char *) a->outpath, (char *) a->ref, 0, 0, 0, ALLREDUCE, a->npoly, a->nhwp, a->delta_t,
+          a->ground, a->n_sss_bins, a->tol, a->maxiter, 0, 0, 0, a->nside, sweeptstamps, a->nsweeps, az, a->az_min,
+          a->az_max, hwp_angle, nces, dsp, nb, block_sizes, a->nnz, pix, w, sig, noi, a->fs, a->invtt);
+    free(pix);
+    free(w);
+    free(sig);
+    free(noi);
+}
+
+int ref_mtmap(const char *outpath, const char *ref, int nces, int ndet, int *nsweeps, int *sweeps_flat,
+              double *az_flat, double *az_min, double *az_max, double *hwp_flat, int npoly, int ground,
+              int n_sss_bins, int nhwp, double delta_t, double fs, double tol, int maxiter, int nside, int nnz,
+              int *pix, double *weights, double *signal, double *noise, double *invtt) {
+    mtmap_args a = {outpath, ref, nces, ndet, npoly, ground, n_sss_bins, nhwp, maxiter, nside, nnz, delta_t, fs, tol,
+                    nsweeps, sweeps_flat, pix, az_flat, az_min, az_max, hwp_flat, weights, signal, noise, invtt};
+    return shim_mpi_run(1, mtmap_rank, &a);
 }

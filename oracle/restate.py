@@ -632,3 +632,178 @@ def noise2invtt(nsetod: np.ndarray, nn: int, lam: int, fsamp: float, apod: str =
     if lam > nn // 2:
         raise RuntimeError("Bandwidth cannot be larger than timestream.")
     return np.multiply(apod_window(lam, apod), inv_tt[:lam], dtype=np.float64), popt, psd
+
+
+# --------------------------------------------------------------------------- templates (MTmap)
+@dataclass
+class TemplateScan:
+    """The scan description MTmap takes (mappraiser/src/mappraiser.c:387-391): per CES
+    the sweep time stamps (nsweeps + 1 values, the last = the CES length), boresight
+    azimuth and its range, HWP angle; the template set (npoly Legendre orders per sweep,
+    ground = azimuth-binned scan-synchronous signal with n_sss_bins bins, nhwp HWP
+    harmonics as cos/sin amplitudes constant over delta_t seconds).  Block b = i*ndet + j
+    is detector j in CES i, ces_length(i) samples."""
+    sweeps: list
+    az: list
+    az_min: np.ndarray
+    az_max: np.ndarray
+    hwp: list
+    ndet: int
+    npoly: int
+    ground: int
+    n_sss_bins: int
+    nhwp: int
+    delta_t: float
+    fs: float
+
+    @property
+    def nces(self) -> int:
+        return len(self.sweeps)
+
+    def ces_length(self, i: int) -> int:
+        return int(self.sweeps[i][-1])
+
+    def hwp_bins(self, i: int) -> int:
+        return int(np.ceil(self.ces_length(i) / (self.delta_t * self.fs)))
+
+    def n_templates_block(self, i: int) -> int:
+        return (self.npoly * (len(self.sweeps[i]) - 1) + self.ground * self.n_sss_bins
+                + 2 * self.nhwp * self.hwp_bins(i))
+
+    @property
+    def block_sizes(self) -> np.ndarray:
+        return np.array([self.ces_length(i) for i in range(self.nces) for _ in range(self.ndet)], dtype=np.int32)
+
+    @property
+    def n_templates(self) -> int:
+        return sum(self.ndet * self.n_templates_block(i) for i in range(self.nces))
+
+    @property
+    def kernel_size(self) -> int:
+        return sum(self.ndet * self.n_templates_block(i) ** 2 for i in range(self.nces))
+
+
+def legendre(x: np.ndarray, a: float, b: float, n: int) -> np.ndarray:
+    """Legendre (algebra/src/templates/templates.c:526-549): P_n on [a, b] by the
+    three-term recurrence."""
+    t = (2 * x - a - b) / (b - a)
+    p0, p1 = np.ones_like(t), t
+    if n == 0:
+        return p0
+    for k in range(2, n + 1):
+        p0, p1 = p1, ((2 * k - 1) * t * p1 - (k - 1) * p0) / k
+    return p1
+
+
+def template_basis(sc: TemplateScan, i: int) -> np.ndarray:
+    """Dense template matrix of CES i, [ces_length, n_templates_block] in the
+    reference's amplitude order (Tlist_init, templates.c:634-677): Legendre order k
+    on sweep s (expandpolydata), then the azimuth bins (bin_az, expandSSSdata), then
+    per HWP harmonic h its cos and its sin over delta_t chunks (build_hwpss_w,
+    expandHWPSSdata)."""
+    L = sc.ces_length(i)
+    sw = np.asarray(sc.sweeps[i])
+    nsw = len(sw) - 1
+    Phi = np.zeros((L, sc.n_templates_block(i)))
+    j = np.arange(L)
+    for k in range(sc.npoly):
+        for s in range(nsw):
+            r = np.arange(sw[s], sw[s + 1])
+            Phi[r, k * nsw + s] = legendre(r / sc.fs, sw[s] / sc.fs, (sw[s + 1] - 1) / sc.fs, k)
+    col = sc.npoly * nsw
+    if sc.ground:
+        az = np.asarray(sc.az[i])
+        width = (sc.az_max[i] - sc.az_min[i]) / sc.n_sss_bins
+        b = np.minimum(sc.n_sss_bins - 1, np.floor((az - sc.az_min[i]) / width).astype(np.int64))
+        Phi[j, col + b] = 1.0
+        col += sc.n_sss_bins
+    if sc.nhwp:
+        hb = sc.hwp_bins(i)
+        c1, s1 = np.cos(sc.hwp[i]), np.sin(sc.hwp[i])
+        ch, sh = c1.copy(), s1.copy()
+        b = np.floor(j / (sc.fs * sc.delta_t)).astype(np.int64)
+        for h in range(1, sc.nhwp + 1):
+            if h > 1:
+                ch, sh = ch * c1 - sh * s1, sh * c1 + ch * s1
+            Phi[j, col + 2 * (h - 1) * hb + b] = ch
+            Phi[j, col + (2 * h - 1) * hb + b] = sh
+    return Phi
+
+
+def templates_ops(sc: TemplateScan, w_block, d, tau):
+    """TrTVecProd, TVecProd (templates.c:28-190) and the pseudo-inverted kernels
+    w_b T_b^T T_b (BuildKernel, InvKernel with rcond 1e-12: templates.c:192-418),
+    blocks one after the other.  Returns (T^T d, T tau, kernels, pseudo-inverses)."""
+    amp, tod, kern, kinv = np.zeros(sc.n_templates), np.zeros(len(d)), [], []
+    at = ta = 0
+    for i in range(sc.nces):
+        Phi = template_basis(sc, i)
+        L, nt = Phi.shape
+        for jd in range(sc.ndet):
+            amp[ta:ta + nt] = Phi.T @ d[at:at + L]
+            tod[at:at + L] = Phi @ tau[ta:ta + nt]
+            K = w_block[i * sc.ndet + jd] * (Phi.T @ Phi)
+            kern.append(K.ravel())
+            kinv.append(np.linalg.pinv(K, rcond=1e-12).ravel())
+            at += L
+            ta += nt
+    return amp, tod, np.concatenate(kern), np.concatenate(kinv)
+
+
+def pcg_templates(gindices, values, signal, noise, sc: TemplateScan, invtt, tol=1e-8, maxiter=500, nnz: int = 3):
+    """PCG_GLS_templates (mappraiser/src/pcg_true.c:243-560) as MTmap runs it
+    (mappraiser.c:586-680): white noise per block (invtt[b], MTmap's lambda = 1), the
+    weighting F v = N^-1 v - N^-1 T B T^T N^-1 v with B_b = pinv(invtt[b] T_b^T T_b), block
+    Jacobi from N^-1 alone, the PCG_GLS_true recurrences and stop test."""
+    m = len(signal)
+    bs = sc.block_sizes
+    A = local_shape(gindices, values, m, nnz)
+    bj = precond_blockjacobi(A, signal, bs, 1, invtt)
+    A = bj.A
+    n = A.n
+    blocks = []
+    at = 0
+    for i in range(sc.nces):
+        Phi = template_basis(sc, i)
+        for jd in range(sc.ndet):
+            b = i * sc.ndet + jd
+            B = np.linalg.pinv(invtt[b] * (Phi.T @ Phi), rcond=1e-12)
+            blocks.append((at, at + Phi.shape[0], invtt[b], Phi, B))
+            at += Phi.shape[0]
+
+    def F(v):
+        out = np.empty_like(v)
+        for s, e, w, Phi, B in blocks:
+            u = w * v[s:e]
+            out[s:e] = u - w * (Phi @ (B @ (Phi.T @ u)))
+        return out
+
+    x = np.zeros(n)
+    g = trmatvec(A, F(bj.signal + noise - matvec(A, x)))
+    Cg = apply_bj(bj.inv, g)
+    h = Cg.copy()
+    g2pix = float(np.dot(Cg, g))
+    res = float(np.dot(g, g))
+    res0 = res
+    tol2rel = tol * tol * res
+    res_rel = [1.0]
+    k = 1
+    if res <= tol:
+        return PCGResult(x, 0, res_rel, bj)
+    while k < maxiter:
+        gp = g
+        AtFAh = trmatvec(A, F(matvec(A, h)))
+        ro = g2pix / float(np.dot(h, AtFAh))
+        x = x + ro * h
+        g = gp - ro * AtFAh
+        Cg = apply_bj(bj.inv, g)
+        g2pixp = g2pix
+        g2pix = float(np.dot(Cg, g))
+        g2pix_polak = float(np.dot(Cg, g - gp))
+        res = float(np.dot(g, g))
+        res_rel.append(float(np.sqrt(res) / np.sqrt(res0)))
+        if res <= tol2rel:
+            break
+        h = h * (g2pix_polak / g2pixp) + Cg
+        k += 1
+    return PCGResult(x, k, res_rel, bj)
