@@ -306,6 +306,41 @@ int  mdp_periodogram(mdp_context *ctx, int nb, const int32_t *h_n, const double 
 int  mdp_noise2invtt(mdp_context *ctx, int nb, const int32_t *h_n, const double *d_noise, int lambda, double fsamp,
                      int apod, double *d_invtt, double *h_params, int32_t *h_evals);
 
+/* ---- templates of MTmap's filtered solve: set-up (host) ------------------
+ * MTmap (mappraiser/src/mappraiser.c:387-391) takes the scan as per-CES rows:
+ * sweep time stamps (nsweeps[i] + 1, the last one the CES length), boresight
+ * azimuth and its range, HWP angle.  Here the rows are flattened one CES after
+ * the other.  Block b = i*ndet + j is detector j in CES i (ces_length(i) samples). */
+typedef struct {
+    int            nces, ndet;
+    int            npoly;        /* Legendre orders 0..npoly-1 per sweep */
+    int            ground;       /* 1: scan-synchronous signal in n_sss_bins azimuth bins */
+    int            n_sss_bins;
+    int            nhwp;         /* HWP harmonics (cos and sin amplitudes per delta_t) */
+    double         delta_t;      /* seconds */
+    double         fs;           /* sampling frequency, Hz */
+    const int32_t *nsweeps;      /* [nces] */
+    const int32_t *sweeps;       /* rows of nsweeps[i] + 1 stamps, sweeps[row 0] = 0 */
+    const double  *az;           /* rows of ces_length(i) samples (ground = 1) */
+    const double  *az_min, *az_max;   /* [nces] (ground = 1) */
+    const double  *hwp;          /* rows of ces_length(i) samples (nhwp > 0) */
+} mdp_template_scan;
+/* The template classes of every CES in ELL form (Tlist_init + expandpolydata /
+ * expandSSSdata / expandHWPSSdata, algebra/src/templates/templates.c:634-800):
+ * h_bins/h_wghts [sum ces_length][n_class], n_class = npoly + ground + 2*nhwp, bins
+ * numbered from 0 within a block in the reference's amplitude order (Legendre order
+ * k on sweep q: k*nsweeps + q; azimuth bins; per harmonic h its cos chunks then its
+ * sin chunks); h_nt [nces] (may be NULL) receives the amplitudes per block.  A
+ * first stamp other than 0, a sweep of fewer than 2 samples or an azimuth below
+ * az_min is MDP_EINVAL (the reference leaves such samples on a foreign bin or
+ * divides by zero). */
+int  mdp_template_layout(const mdp_template_scan *scan, int32_t *h_bins, double *h_wghts, int32_t *h_nt);
+/* The kernels B_b = pinv(w_b T_b^T T_b) of every block (BuildKernel + InvKernel,
+ * templates.c:192-418: singular values <= 1e-12 s_max dropped), block after
+ * block in h_kinv (nt_i^2 doubles each, row-major); h_w_block [nces*ndet] = the
+ * white-noise weight of each block (MTmap: invtt[b], lambda = 1). */
+int  mdp_template_kernels(const mdp_template_scan *scan, const double *h_w_block, double *h_kinv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -119,6 +119,8 @@ _SIGS = {
     "mdp_periodogram": (ct.c_int, [ct.c_void_p, ct.c_int, c_i32p, ct.c_void_p, ct.c_double, ct.c_void_p]),
     "mdp_noise2invtt": (ct.c_int, [ct.c_void_p, ct.c_int, c_i32p, ct.c_void_p, ct.c_int, ct.c_double, ct.c_int,
                                    ct.c_void_p, c_f64p, c_i32p]),
+    "mdp_template_layout": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mdp_template_kernels": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     # reference-compatible host API (include/mapmat.h, toeplitz.h, mappraiser.h)
     "MatInit": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, c_i32p, c_f64p, ct.c_int, ct.c_int]),
     "MatSetIndices": (None, [ct.c_void_p, ct.c_int, ct.c_int, c_i32p]),

@@ -13,7 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmidapack_b200.so")
-SOURCES = ["pointing.cu", "toeplitz.cu", "solver.cu", "twolevel.cu", "ecg.cu", "multirhs.cu", "noise.cu", "dropin.cu"]
+SOURCES = ["pointing.cu", "toeplitz.cu", "solver.cu", "twolevel.cu", "ecg.cu", "multirhs.cu", "noise.cu", "templates.cu",
+           "dropin.cu"]
 
 
 def nvcc() -> str:

@@ -66,3 +66,53 @@ def test_filter_removes_the_template_space():
             at += L
             ta += nt
             ka += nt * nt
+
+
+def _product_scan(sc):
+    from midapack_b200 import templates
+    return templates.Scan(sc.sweeps, sc.az, sc.az_min, sc.az_max, sc.hwp, sc.ndet, sc.npoly, sc.ground,
+                          sc.n_sss_bins, sc.nhwp, sc.delta_t, sc.fs)
+
+
+@pytest.mark.parametrize("name", list(VARIANTS))
+def test_library_layout_matches_restatement(name):
+    """mdp_template_layout (host set-up in the library) against the restated basis."""
+    from midapack_b200 import templates
+    sc, *_ = template_case(**VARIANTS[name])
+    bins, wg, nt = templates.layout(_product_scan(sc))
+    at = 0
+    for i in range(sc.nces):
+        Phi = restate.template_basis(sc, i)
+        L = Phi.shape[0]
+        assert nt[i] == Phi.shape[1]
+        mine = np.zeros_like(Phi)
+        for c in range(bins.shape[1]):
+            np.add.at(mine, (np.arange(L), bins[at:at + L, c]), wg[at:at + L, c])
+        assert np.abs(mine - Phi).max() <= 1e-14
+        at += L
+
+
+@pytest.mark.parametrize("name", list(VARIANTS))
+def test_library_kernels_match_reference(ref_lib, name):
+    """mdp_template_kernels against the reference's BuildKernel + InvKernel."""
+    from midapack_b200 import templates
+    sc, pix, w, sig, noi, invtt, nside = template_case(**VARIANTS[name])
+    _, _, _, kinv = ref_lib.templates_ops(sc, invtt, np.zeros(sig.size), np.zeros(sc.n_templates))
+    mine = templates.kernels(_product_scan(sc), invtt)
+    assert rel(mine, kinv) <= 1e-9
+
+
+def test_library_layout_rejects_bad_scans():
+    from midapack_b200 import MidapackError, templates
+    sc, *_ = template_case()
+    bad = _product_scan(sc)
+    bad.sweeps = [np.array([5, 600, 1200]), sc.sweeps[1]]
+    with pytest.raises(MidapackError, match="sample 0"):
+        templates.layout(bad)
+    bad.sweeps = [np.array([0, 1, 1200]), sc.sweeps[1]]
+    with pytest.raises(MidapackError, match="fewer than 2"):
+        templates.layout(bad)
+    bad = _product_scan(sc)
+    bad.az_min = np.array([15.0, 10.0])
+    with pytest.raises(MidapackError, match="below az_min"):
+        templates.layout(bad)
