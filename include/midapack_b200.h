@@ -340,6 +340,20 @@ int  mdp_template_layout(const mdp_template_scan *scan, int32_t *h_bins, double 
  * block in h_kinv (nt_i^2 doubles each, row-major); h_w_block [nces*ndet] = the
  * white-noise weight of each block (MTmap: invtt[b], lambda = 1). */
 int  mdp_template_kernels(const mdp_template_scan *scan, const double *h_w_block, double *h_kinv);
+/* The weighting of MTmap's PCG on the device (PCG_GLS_templates,
+ * mappraiser/src/pcg_true.c:301-365, 433-462): d_out = W d_in - W T B T^T W d_in
+ * with W = diag(h_w_block[b]) per block (MTmap's white N^-1, lambda = 1) and B the
+ * kernels above.  TOD blocks are consecutive, block b = i*ndet + j of
+ * ces_length(i) samples; d_out may be d_in.  At most 6144 amplitudes per block
+ * (MDP_EUNSUPPORTED beyond).  The template amplitude sums use atomic adds, so
+ * results vary in the last bits from call to call. */
+typedef struct mdp_templates mdp_templates;
+int  mdp_templates_create(mdp_context *ctx, const mdp_template_scan *scan, const double *h_w_block,
+                          mdp_templates **out);
+void mdp_templates_destroy(mdp_templates *T);
+/* samples of the TOD the filter covers and its template amplitudes in total */
+int  mdp_templates_samples(const mdp_templates *T, int64_t *m, int64_t *n_amplitudes);
+int  mdp_templates_filter(mdp_context *ctx, const mdp_templates *T, const double *d_in, double *d_out);
 
 #ifdef __cplusplus
 }

@@ -1,4 +1,5 @@
-// Set-up of MTmap's template-filtered solve (host side, as in the reference).
+// MTmap's template filter: set-up on the host (as in the reference) and the
+// weighting of its PCG on the device.
 //
 // MTmap (mappraiser/src/mappraiser.c:387-800) marginalises per-block template
 // amplitudes: Legendre polynomials of orders 0..npoly-1 on every sweep, the
@@ -14,7 +15,9 @@
 #include "mdp_internal.cuh"
 #include "smalldense.h"
 
+#include <algorithm>
 #include <cmath>
+#include <memory>
 #include <vector>
 
 namespace {
@@ -158,13 +161,11 @@ extern "C" int mdp_template_layout(const mdp_template_scan *scan, int32_t *h_bin
     return MDP_OK;
 }
 
-extern "C" int mdp_template_kernels(const mdp_template_scan *scan, const double *h_w_block, double *h_kinv) {
-    Scan sc;
-    MDP_TRY(make_scan(scan, &sc));
-    if (!h_w_block || !h_kinv) {
-        mdp_set_error("mdp_template_kernels: bad argument");
-        return MDP_EINVAL;
-    }
+namespace {
+
+// pinv(w_b T_b^T T_b) of every block, block after block into h_kinv
+int kernels_impl(const Scan &sc, const double *h_w_block, double *h_kinv) {
+    const mdp_template_scan *scan = sc.s;
     const int nc = sc.n_class;
     int64_t at = 0;
     std::vector<int32_t> bins;
@@ -190,5 +191,216 @@ extern "C" int mdp_template_kernels(const mdp_template_scan *scan, const double 
             at += (int64_t) nt * nt;
         }
     }
+    return MDP_OK;
+}
+
+}  // namespace
+
+extern "C" int mdp_template_kernels(const mdp_template_scan *scan, const double *h_w_block, double *h_kinv) {
+    Scan sc;
+    MDP_TRY(make_scan(scan, &sc));
+    if (!h_w_block || !h_kinv) {
+        mdp_set_error("mdp_template_kernels: bad argument");
+        return MDP_EINVAL;
+    }
+    return kernels_impl(sc, h_w_block, h_kinv);
+}
+
+// ====================================================================== device filter
+// F x = W x - W T B T^T W x, W = diag(w_b) per block (MTmap's white N^-1, lambda = 1),
+// B_b = pinv(w_b T_b^T T_b): the weighting of PCG_GLS_templates
+// (mappraiser/src/pcg_true.c:301-365, 433-462).  TOD blocks are consecutive, block
+// b = i*ndet + j of ces_length(i) samples; the ELL rows of CES i are shared by its
+// detectors.
+struct mdp_templates {
+    int     nb = 0, nc = 0, max_nt = 0, max_len = 0;
+    int64_t m = 0, namp = 0;
+    DevBuf  bins, wg;                       // int32 / double [sum ces_length][nc]
+    DevBuf  blk_off, blk_row, blk_amp, blk_kinv;   // int64 [nb]
+    DevBuf  blk_len, blk_nt;                // int32 [nb]
+    DevBuf  blk_w;                          // double [nb]
+    DevBuf  kinv;                           // double [sum nt^2]
+    DevBuf  amp, coef;                      // double [namp] work
+};
+
+namespace {
+
+constexpr int kTplThreads = 256;
+constexpr int kTplMaxNt = 6144;   // one block's amplitudes in 48 KB of shared memory
+
+// a_b += T_b^T (w_b x_b) over a chunk of the block's samples (grid: chunks x blocks):
+// a shared-memory histogram of the block's amplitudes, then one global add per amplitude
+__global__ void __launch_bounds__(kTplThreads) tpl_tt_kernel(const double *x, const int32_t *bins, const double *wg,
+                                                             int nc, const int64_t *blk_off, const int64_t *blk_row,
+                                                             const int32_t *blk_len, const int32_t *blk_nt,
+                                                             const int64_t *blk_amp, const double *blk_w,
+                                                             double *amp) {
+    extern __shared__ double hist[];
+    const int b = blockIdx.y;
+    const int nt = blk_nt[b];
+    const int64_t L = blk_len[b];
+    for (int k = threadIdx.x; k < nt; k += blockDim.x) hist[k] = 0.0;
+    __syncthreads();
+    const double w = blk_w[b];
+    const double *xb = x + blk_off[b];
+    const int32_t *bb = bins + blk_row[b] * nc;
+    const double *wb = wg + blk_row[b] * nc;
+    for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < L; t += (int64_t) gridDim.x * blockDim.x) {
+        const double v = w * xb[t];
+        for (int c = 0; c < nc; ++c) {
+            const int k = bb[t * nc + c];
+            if ((unsigned) k < (unsigned) nt) atomicAdd(&hist[k], wb[t * nc + c] * v);
+        }
+    }
+    __syncthreads();
+    double *ab = amp + blk_amp[b];
+    for (int k = threadIdx.x; k < nt; k += blockDim.x)
+        if (hist[k] != 0.0) atomicAdd(&ab[k], hist[k]);
+}
+
+// c_b = B_b a_b (row-major B_b, as PCG_GLS_templates applies it): one CTA per block
+__global__ void __launch_bounds__(kTplThreads) tpl_b_kernel(const double *kinv, const int64_t *blk_kinv,
+                                                            const int32_t *blk_nt, const int64_t *blk_amp,
+                                                            const double *amp, double *coef) {
+    const int b = blockIdx.x;
+    const int nt = blk_nt[b];
+    const double *K = kinv + blk_kinv[b];
+    const double *a = amp + blk_amp[b];
+    double *c = coef + blk_amp[b];
+    for (int r = threadIdx.x; r < nt; r += blockDim.x) {
+        double acc = 0.0;
+        for (int l = 0; l < nt; ++l) acc += K[(int64_t) r * nt + l] * a[l];
+        c[r] = acc;
+    }
+}
+
+// y_b = w_b x_b - w_b T_b c_b (y may be x)
+__global__ void __launch_bounds__(kTplThreads) tpl_t_kernel(const double *x, const int32_t *bins, const double *wg,
+                                                            int nc, const int64_t *blk_off, const int64_t *blk_row,
+                                                            const int32_t *blk_len, const int32_t *blk_nt,
+                                                            const int64_t *blk_amp, const double *blk_w,
+                                                            const double *coef, double *y) {
+    const int b = blockIdx.y;
+    const int nt = blk_nt[b];
+    const int64_t L = blk_len[b];
+    const double w = blk_w[b];
+    const int64_t off = blk_off[b];
+    const int32_t *bb = bins + blk_row[b] * nc;
+    const double *wb = wg + blk_row[b] * nc;
+    const double *cb = coef + blk_amp[b];
+    for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < L; t += (int64_t) gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int c = 0; c < nc; ++c) {
+            const int k = bb[t * nc + c];
+            if ((unsigned) k < (unsigned) nt) s += wb[t * nc + c] * cb[k];
+        }
+        y[off + t] = w * x[off + t] - w * s;
+    }
+}
+
+template <class T>
+int upload(DevBuf &d, const std::vector<T> &h) {
+    MDP_TRY(d.alloc(h.size() * sizeof(T)));
+    if (!h.empty()) MDP_CUDA(cudaMemcpy(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return MDP_OK;
+}
+
+}  // namespace
+
+extern "C" int mdp_templates_create(mdp_context *ctx, const mdp_template_scan *scan, const double *h_w_block,
+                                    mdp_templates **out) {
+    if (!ctx || !out || !h_w_block) {
+        mdp_set_error("mdp_templates_create: bad argument");
+        return MDP_EINVAL;
+    }
+    *out = nullptr;
+    Scan sc;
+    MDP_TRY(make_scan(scan, &sc));
+    const int nc = sc.n_class, nces = scan->nces, ndet = scan->ndet;
+    auto T = new mdp_templates();
+    std::unique_ptr<mdp_templates> guard(T);
+    T->nb = nces * ndet;
+    T->nc = nc;
+    const int64_t rows = sc.sample_row[nces];
+    std::vector<int32_t> bins((size_t) rows * nc);
+    std::vector<double> wg((size_t) rows * nc);
+    std::vector<int64_t> off(T->nb), row(T->nb), ampo(T->nb), kino(T->nb);
+    std::vector<int32_t> len(T->nb), nt(T->nb);
+    std::vector<double> w(h_w_block, h_w_block + T->nb);
+    int64_t at = 0, na = 0, nk = 0;
+    for (int i = 0; i < nces; ++i) {
+        MDP_TRY(layout_ces(sc, i, bins.data() + sc.sample_row[i] * nc, wg.data() + sc.sample_row[i] * nc));
+        const int nti = sc.nt(i);
+        if (nti > kTplMaxNt) {
+            mdp_set_error("mdp_templates_create: CES %d has %d template amplitudes per block (at most %d)", i, nti,
+                          kTplMaxNt);
+            return MDP_EUNSUPPORTED;
+        }
+        T->max_nt = std::max(T->max_nt, nti);
+        T->max_len = std::max(T->max_len, sc.length(i));
+        for (int j = 0; j < ndet; ++j) {
+            const int b = i * ndet + j;
+            off[b] = at;
+            row[b] = sc.sample_row[i];
+            len[b] = sc.length(i);
+            nt[b] = nti;
+            ampo[b] = na;
+            kino[b] = nk;
+            at += sc.length(i);
+            na += nti;
+            nk += (int64_t) nti * nti;
+        }
+    }
+    T->m = at;
+    T->namp = na;
+    std::vector<double> kinv((size_t) nk);
+    MDP_TRY(kernels_impl(sc, h_w_block, kinv.data()));
+    MDP_TRY(upload(T->bins, bins));
+    MDP_TRY(upload(T->wg, wg));
+    MDP_TRY(upload(T->blk_off, off));
+    MDP_TRY(upload(T->blk_row, row));
+    MDP_TRY(upload(T->blk_amp, ampo));
+    MDP_TRY(upload(T->blk_kinv, kino));
+    MDP_TRY(upload(T->blk_len, len));
+    MDP_TRY(upload(T->blk_nt, nt));
+    MDP_TRY(upload(T->blk_w, w));
+    MDP_TRY(upload(T->kinv, kinv));
+    MDP_TRY(T->amp.alloc((size_t) na * sizeof(double)));
+    MDP_TRY(T->coef.alloc((size_t) na * sizeof(double)));
+    *out = guard.release();
+    return MDP_OK;
+}
+
+extern "C" void mdp_templates_destroy(mdp_templates *T) { delete T; }
+
+extern "C" int mdp_templates_samples(const mdp_templates *T, int64_t *m, int64_t *n_amplitudes) {
+    if (!T) return MDP_EINVAL;
+    if (m) *m = T->m;
+    if (n_amplitudes) *n_amplitudes = T->namp;
+    return MDP_OK;
+}
+
+extern "C" int mdp_templates_filter(mdp_context *ctx, const mdp_templates *T, const double *d_in, double *d_out) {
+    if (!ctx || !T || !d_in || !d_out) {
+        mdp_set_error("mdp_templates_filter: bad argument");
+        return MDP_EINVAL;
+    }
+    double *amp = T->amp.as<double>(), *coef = T->coef.as<double>();
+    MDP_CUDA(cudaMemsetAsync(amp, 0, (size_t) T->namp * sizeof(double), ctx->stream));
+    const int chunks = (int) std::max<int64_t>(1, std::min<int64_t>(64, (T->max_len + 2047) / 2048));
+    const dim3 grid(chunks, T->nb);
+    tpl_tt_kernel<<<grid, kTplThreads, (size_t) T->max_nt * sizeof(double), ctx->stream>>>(
+        d_in, T->bins.as<int32_t>(), T->wg.as<double>(), T->nc, T->blk_off.as<int64_t>(), T->blk_row.as<int64_t>(),
+        T->blk_len.as<int32_t>(), T->blk_nt.as<int32_t>(), T->blk_amp.as<int64_t>(), T->blk_w.as<double>(), amp);
+    MDP_CHECK_LAUNCH(ctx);
+    tpl_b_kernel<<<T->nb, kTplThreads, 0, ctx->stream>>>(T->kinv.as<double>(), T->blk_kinv.as<int64_t>(),
+                                                         T->blk_nt.as<int32_t>(), T->blk_amp.as<int64_t>(), amp,
+                                                         coef);
+    MDP_CHECK_LAUNCH(ctx);
+    tpl_t_kernel<<<grid, kTplThreads, 0, ctx->stream>>>(
+        d_in, T->bins.as<int32_t>(), T->wg.as<double>(), T->nc, T->blk_off.as<int64_t>(), T->blk_row.as<int64_t>(),
+        T->blk_len.as<int32_t>(), T->blk_nt.as<int32_t>(), T->blk_amp.as<int64_t>(), T->blk_w.as<double>(), coef,
+        d_out);
+    MDP_CHECK_LAUNCH(ctx);
     return MDP_OK;
 }

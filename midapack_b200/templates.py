@@ -5,8 +5,9 @@ amplitudes (algebra/src/templates/templates.c): Legendre polynomials per sweep,
 the azimuth-binned ground signal, HWP harmonics over delta_t chunks.  ``layout``
 gives the template matrix of every CES in ELL form (one (bin, weight) pair per
 class per sample), ``kernels`` the per-block pseudo-inverses
-``pinv(w_b T_b^T T_b)`` that MTmap's PCG applies.  Both run on the host, as in
-the reference.
+``pinv(w_b T_b^T T_b)`` that MTmap's PCG applies (both on the host, as in the
+reference); ``Filter`` applies MTmap's weighting ``W - W T B T^T W`` to a TOD on
+the device.
 """
 from __future__ import annotations
 
@@ -15,7 +16,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import check, lib
+from . import Context, _ptr, check, lib
 
 
 class _ScanC(ct.Structure):
@@ -92,3 +93,42 @@ def kernels(scan: Scan, w_block):
     out = np.zeros(int(scan.ndet * (nt.astype(np.int64) ** 2).sum()))
     check(lib().mdp_template_kernels(ct.addressof(s), w.ctypes.data, out.ctypes.data), "mdp_template_kernels")
     return out
+
+
+class Filter:
+    """MTmap's TOD weighting on the device (mdp_templates_filter):
+    ``y = W x - W T B T^T W x`` with W the white-noise weight of each block."""
+
+    def __init__(self, ctx: Context, scan: Scan, w_block):
+        self.ctx = ctx
+        s, keep = scan._c()
+        w = np.ascontiguousarray(w_block, dtype=np.float64)
+        if w.size != scan.nces * scan.ndet:
+            raise ValueError("one weight per block (nces * ndet)")
+        self.h = ct.c_void_p()
+        check(lib().mdp_templates_create(ctx.h, ct.addressof(s), w.ctypes.data, ct.byref(self.h)),
+              "mdp_templates_create")
+        m, na = ct.c_int64(), ct.c_int64()
+        check(lib().mdp_templates_samples(self.h, ct.byref(m), ct.byref(na)), "mdp_templates_samples")
+        self.m, self.n_amplitudes = m.value, na.value
+
+    def __call__(self, x, out=None):
+        """Filtered copy of the CUDA float64 tensor x (or into `out`, which may be x)."""
+        import torch
+        if x.numel() != self.m or x.dtype != torch.float64:
+            raise ValueError(f"expected {self.m} float64 samples")
+        y = torch.empty_like(x) if out is None else out
+        check(lib().mdp_templates_filter(self.ctx.h, self.h, ct.c_void_p(_ptr(x)), ct.c_void_p(_ptr(y))),
+              "mdp_templates_filter")
+        return y
+
+    def close(self):
+        if self.h:
+            lib().mdp_templates_destroy(self.h)
+            self.h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
