@@ -750,11 +750,13 @@ def templates_ops(sc: TemplateScan, w_block, d, tau):
     return amp, tod, np.concatenate(kern), np.concatenate(kinv)
 
 
-def pcg_templates(gindices, values, signal, noise, sc: TemplateScan, invtt, tol=1e-8, maxiter=500, nnz: int = 3):
+def pcg_templates(gindices, values, signal, noise, sc: TemplateScan, invtt, tol=1e-8, maxiter=500, nnz: int = 3,
+                  kinv=None):
     """PCG_GLS_templates (mappraiser/src/pcg_true.c:243-560) as MTmap runs it
     (mappraiser.c:586-680): white noise per block (invtt[b], MTmap's lambda = 1), the
     weighting F v = N^-1 v - N^-1 T B T^T N^-1 v with B_b = pinv(invtt[b] T_b^T T_b), block
-    Jacobi from N^-1 alone, the PCG_GLS_true recurrences and stop test."""
+    Jacobi from N^-1 alone, the PCG_GLS_true recurrences and stop test.  kinv: the B_b
+    to use instead (block after block, row-major), e.g. another implementation's."""
     m = len(signal)
     bs = sc.block_sizes
     A = local_shape(gindices, values, m, nnz)
@@ -762,14 +764,19 @@ def pcg_templates(gindices, values, signal, noise, sc: TemplateScan, invtt, tol=
     A = bj.A
     n = A.n
     blocks = []
-    at = 0
+    at = ka = 0
     for i in range(sc.nces):
         Phi = template_basis(sc, i)
+        nt = Phi.shape[1]
         for jd in range(sc.ndet):
             b = i * sc.ndet + jd
-            B = np.linalg.pinv(invtt[b] * (Phi.T @ Phi), rcond=1e-12)
+            if kinv is None:
+                B = np.linalg.pinv(invtt[b] * (Phi.T @ Phi), rcond=1e-12)
+            else:
+                B = np.asarray(kinv[ka:ka + nt * nt]).reshape(nt, nt)
             blocks.append((at, at + Phi.shape[0], invtt[b], Phi, B))
             at += Phi.shape[0]
+            ka += nt * nt
 
     def F(v):
         out = np.empty_like(v)

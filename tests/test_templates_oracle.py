@@ -116,3 +116,20 @@ def test_library_layout_rejects_bad_scans():
     bad.az_min = np.array([15.0, 10.0])
     with pytest.raises(MidapackError, match="below az_min"):
         templates.layout(bad)
+
+
+def test_mtmap_with_library_kernels_matches_reference(ref_lib):
+    """The templates solve with the library's kernels (mdp_template_kernels) in place
+    of numpy's gives the reference MTmap's maps."""
+    from midapack_b200 import templates
+    sc, pix, w, sig, noi, invtt, nside = template_case()
+    I, Q, U, Cond, Hits, res = ref_lib.mtmap(sc, pix, w, sig, noi, invtt, nside, tol=1e-10, maxiter=500)
+    kinv = templates.kernels(_product_scan(sc), invtt)
+    r = restate.pcg_templates(pix, w, sig, noi, sc, invtt, tol=1e-10, maxiter=500, kinv=kinv)
+    assert r.iters == len(res) - 1
+    A = r.bj.A
+    mI, mQ, mU, _, _ = restate.x2map_pol(r.x, A.lindices[A.nnz * A.trash_pix:], np.zeros(r.x.size // 3),
+                                         np.zeros(r.x.size // 3, dtype=np.int32), 12 * nside * nside)
+    obs = Hits > 0
+    for mine, theirs in ((mI, I), (mQ, Q), (mU, U)):
+        assert rel(mine[obs], theirs[obs]) <= 1e-9
