@@ -354,6 +354,15 @@ void mdp_templates_destroy(mdp_templates *T);
 /* samples of the TOD the filter covers and its template amplitudes in total */
 int  mdp_templates_samples(const mdp_templates *T, int64_t *m, int64_t *n_amplitudes);
 int  mdp_templates_filter(mdp_context *ctx, const mdp_templates *T, const double *d_in, double *d_out);
+/* MTmap's solve (PCG_GLS_templates, pcg_true.c:243-560): block Jacobi from the
+ * white noise operator N (lambda = 1, first row = the block's weight; one block
+ * per template block) with the rcond cut applied to A, then the PCG_GLS_true
+ * recurrences and stop test with the weighting of mdp_templates_filter in place of
+ * N^-1.  Outputs as mdp_gls_solve.  params->precond must be 0. */
+int  mdp_gls_solve_templates(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const mdp_templates *T,
+                             const double *d_signal, const double *d_noise, const mdp_solve_params *params,
+                             double *d_x, int32_t *d_lstid, double *d_cond, int32_t *d_hits, double *h_res_rel,
+                             mdp_solve_info *info);
 
 #ifdef __cplusplus
 }

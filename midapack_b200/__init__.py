@@ -125,6 +125,9 @@ _SIGS = {
     "mdp_templates_destroy": (None, [ct.c_void_p]),
     "mdp_templates_samples": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_int64), ct.POINTER(ct.c_int64)]),
     "mdp_templates_filter": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mdp_gls_solve_templates": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                           ct.c_void_p, ct.POINTER(SolveParams), ct.c_void_p, ct.c_void_p,
+                                           ct.c_void_p, ct.c_void_p, c_f64p, ct.POINTER(SolveInfo)]),
     # reference-compatible host API (include/mapmat.h, toeplitz.h, mappraiser.h)
     "MatInit": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, c_i32p, c_f64p, ct.c_int, ct.c_int]),
     "MatSetIndices": (None, [ct.c_void_p, ct.c_int, ct.c_int, c_i32p]),

@@ -215,9 +215,11 @@ int mdp_ecg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const dou
                 const double *d_signal, const double *d_noise, const mdp_ecg_params *prm, double *d_x,
                 double *h_res_rel, mdp_solve_info *info);
 int mdp_bj_cached(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const BJState **bj);
+// tpl != nullptr: MTmap's weighting W - W T B T^T W (templates.cu) in place of N^-1
 int mdp_pcg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *inv, int64_t npix,
                 const double *d_signal, const double *d_noise, const mdp_solve_params *params, double *d_x,
-                double *h_res_rel, mdp_solve_info *info, const mdp_twolevel *tl = nullptr);
+                double *h_res_rel, mdp_solve_info *info, const mdp_twolevel *tl = nullptr,
+                const mdp_templates *tpl = nullptr);
 int mdp_pointing_create_ex(mdp_context *ctx, int64_t m, int nnz, const int32_t *d_g, const double *d_values,
                            int32_t *d_local_out, mdp_pointing **out);
 int mdp_matvec_launch(mdp_context *ctx, const mdp_pointing *A, const double *d_x, double *d_y);

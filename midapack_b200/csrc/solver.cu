@@ -707,7 +707,7 @@ int mdp_bj_build(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, BJState 
 
 int mdp_pcg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const double *inv, int64_t npix,
                 const double *d_signal, const double *d_noise, const mdp_solve_params *params, double *d_x,
-                double *h_res_rel, mdp_solve_info *info, const mdp_twolevel *tl) {
+                double *h_res_rel, mdp_solve_info *info, const mdp_twolevel *tl, const mdp_templates *tpl) {
     cudaStream_t  st = ctx->stream;
     const int64_t m = A->m;
     const int64_t n = 3 * npix;
@@ -730,7 +730,10 @@ int mdp_pcg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const dou
     MDP_CUDA(cudaMemsetAsync(Cg, 0, 8 * nmap, st));
     rhs_kernel<<<gm, 256, 0, st>>>(A->off.as<int32_t>(), d_signal, d_noise, ta, m);
     MDP_CHECK_LAUNCH(ctx);
-    MDP_TRY(mdp_stbmm_impl(ctx, N, ta, tb, nullptr));
+    if (tpl)
+        MDP_TRY(mdp_templates_filter(ctx, tpl, ta, tb));
+    else
+        MDP_TRY(mdp_stbmm_impl(ctx, N, ta, tb, nullptr));
     MDP_TRY(mdp_trmatvec_launch(ctx, A, tb, g));
     if (tl) {
         MDP_TRY(mdp_twolevel_qtx(ctx, tl, g));
@@ -762,11 +765,14 @@ int mdp_pcg_run(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const dou
         std::swap(g, gp);
         if (prof) cudaEventRecord(ctx->ev[0], st);
         // P h with the block means of P h fused in when the blocks tile the rows
-        const int fused = mdp_matvec_blockmeans(ctx, A, N, h, ta);
+        const int fused = tpl ? MDP_EUNSUPPORTED : mdp_matvec_blockmeans(ctx, A, N, h, ta);
         if (fused != MDP_OK && fused != MDP_EUNSUPPORTED) return fused;
         if (fused == MDP_EUNSUPPORTED) MDP_TRY(mdp_matvec_launch(ctx, A, h, ta));
         if (prof) cudaEventRecord(ctx->ev[1], st);
-        MDP_TRY(mdp_stbmm_impl(ctx, N, ta, tb, fused == MDP_OK ? N->means.as<double>() : nullptr));
+        if (tpl)
+            MDP_TRY(mdp_templates_filter(ctx, tpl, ta, tb));
+        else
+            MDP_TRY(mdp_stbmm_impl(ctx, N, ta, tb, fused == MDP_OK ? N->means.as<double>() : nullptr));
         if (prof) cudaEventRecord(ctx->ev[2], st);
         MDP_TRY(mdp_trmatvec_launch(ctx, A, tb, q));
         if (prof) cudaEventRecord(ctx->ev[3], st);

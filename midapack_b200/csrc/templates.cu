@@ -404,3 +404,45 @@ extern "C" int mdp_templates_filter(mdp_context *ctx, const mdp_templates *T, co
     MDP_CHECK_LAUNCH(ctx);
     return MDP_OK;
 }
+
+// MTmap's solve (PCG_GLS_templates, mappraiser/src/pcg_true.c:243-560, as MTmap calls it,
+// mappraiser.c:586-680): block Jacobi from the white noise operator N (lambda = 1, the
+// blocks' weights) with the rcond cut, then the PCG_GLS_true recurrences with the
+// weighting W - W T B T^T W.
+extern "C" int mdp_gls_solve_templates(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, const mdp_templates *T,
+                                       const double *d_signal, const double *d_noise, const mdp_solve_params *params,
+                                       double *d_x, int32_t *d_lstid, double *d_cond, int32_t *d_hits,
+                                       double *h_res_rel, mdp_solve_info *info) {
+    if (!ctx || !A || !N || !T || !d_signal || !d_noise || !params || !d_x) {
+        mdp_set_error("mdp_gls_solve_templates: invalid arguments");
+        return MDP_EINVAL;
+    }
+    if (N->lambda != 1 || N->nb != T->nb || T->m != A->m || N->nrow_end > A->m) {
+        mdp_set_error("mdp_gls_solve_templates: the noise operator must be white (lambda 1) with one block per "
+                      "template block, and the filter must cover the pointing's %lld rows", (long long) A->m);
+        return MDP_EINVAL;
+    }
+    if (params->precond != 0) {
+        mdp_set_error("mdp_gls_solve_templates: only the block-Jacobi preconditioner (precond 0)");
+        return MDP_EUNSUPPORTED;
+    }
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    const BJState *bjp = nullptr;
+    MDP_TRY(mdp_bj_cached(ctx, A, N, &bjp));
+    const BJState &bj = *bjp;
+    cudaStream_t st = ctx->stream;
+    if (d_lstid)
+        MDP_CUDA(cudaMemcpyAsync(d_lstid, A->lindices.as<int32_t>() + 3 * A->trash_pix, 4 * A->n_map(),
+                                 cudaMemcpyDeviceToDevice, st));
+    if (d_cond) MDP_CUDA(cudaMemcpyAsync(d_cond, bj.rcond.p, 8 * bj.npix, cudaMemcpyDeviceToDevice, st));
+    if (d_hits) MDP_CUDA(cudaMemcpyAsync(d_hits, bj.hits.p, 4 * bj.npix, cudaMemcpyDeviceToDevice, st));
+    MDP_TRY(mdp_pcg_run(ctx, A, N, bj.inv.as<double>(), bj.npix, d_signal, d_noise, params, d_x, h_res_rel, info,
+                        nullptr, T));
+    if (info) {
+        info->n_cut = bj.ncut;
+        info->n_map = A->n_map();
+        info->outer_iterations = 0;
+        info->fp64_applications = info->iterations;
+    }
+    return MDP_OK;
+}

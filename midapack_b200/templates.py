@@ -132,3 +132,26 @@ class Filter:
             self.close()
         except Exception:  # noqa: BLE001
             pass
+
+
+def solve(ctx: Context, A, N, F: Filter, signal, noise, tol=1e-8, maxiter=500, verbose=False):
+    """MTmap's template-filtered PCG on device tensors (mdp_gls_solve_templates): N is
+    the white noise operator (``midapack_b200.Noise(ctx, block_sizes, 1, w_block)``), F
+    the filter built from the same weights.  Returns (x, lstid, cond, hits, res_rel,
+    info) like ``midapack_b200.gls_solve``."""
+    import torch
+    from . import SolveInfo, SolveParams, c_f64p
+    n0 = A.shape()["n_map"]
+    x = torch.empty(max(n0, 1), dtype=torch.float64, device="cuda")
+    lst = torch.empty(max(n0, 1), dtype=torch.int32, device="cuda")
+    cond = torch.empty(max(n0 // 3, 1), dtype=torch.float64, device="cuda")
+    hits = torch.empty(max(n0 // 3, 1), dtype=torch.int32, device="cuda")
+    res = np.zeros(maxiter + 1)
+    prm = SolveParams(tol, maxiter, 1 if verbose else 0, 0, 0)
+    info = SolveInfo()
+    check(lib().mdp_gls_solve_templates(ctx.h, A.h, N.h, F.h, ct.c_void_p(_ptr(signal)), ct.c_void_p(_ptr(noise)),
+                                        ct.byref(prm), ct.c_void_p(x.data_ptr()), ct.c_void_p(lst.data_ptr()),
+                                        ct.c_void_p(cond.data_ptr()), ct.c_void_p(hits.data_ptr()),
+                                        res.ctypes.data_as(c_f64p), ct.byref(info)), "mdp_gls_solve_templates")
+    n = info.n_map
+    return x[:n], lst[:n], cond[:n // 3], hits[:n // 3], res[:info.iterations + 1], info
