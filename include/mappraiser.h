@@ -1,15 +1,15 @@
 /*
  * Drop-in MAPPRAISER API (GLS map-making), B200 implementation.
  * Same names and signatures as the reference:
- *   mappraiser/include/mappraiser/map.h:10-13          MLmap
+ *   mappraiser/include/mappraiser/map.h:10-18          MLmap, MTmap
  *   mappraiser/include/mappraiser/pcg_true.h:8-12      get_pixshare_pond, PCG_GLS_true
  *   mappraiser/include/mappraiser/precond.h:6-35       Precond, build_precond, apply_precond, free_precond,
  *                                                      precondblockjacobilike
  *   mappraiser/include/mappraiser/create_toeplitz.h    defineTpltz_avg, defineBlocks_avg
  *   mappraiser/include/mappraiser/ecg.h:6-7            ECG_GLS
  * Scope: solver 0 (PCG) with precond 0 (block Jacobi), 1 and 2 (two-level),
- * solver 1 (ECG, block Jacobi), on one GPU.  Other solver/precond values
- * return an error (MLmap prints it and returns).
+ * solver 1 (ECG, block Jacobi), on one GPU; MTmap with solver 0, precond 0.
+ * Other solver/precond values return an error (MLmap/MTmap print it and return).
  */
 #ifndef MDP_DROPIN_MAPPRAISER_H
 #define MDP_DROPIN_MAPPRAISER_H
@@ -74,6 +74,18 @@ void MLmap(MPI_Comm comm, char *outpath, char *ref, int solver, int precond, int
            double tol, int maxiter, int enlFac, int ortho_alg, int bs_red, int nside, void *data_size_proc,
            int nb_blocks_loc, void *local_blocks_sizes, int Nnz, void *pix, void *pixweights, void *signal,
            double *noise, int lambda, double *invtt);
+
+/* map.h:15-18: MLmap with per-block template amplitudes marginalised
+ * (PCG_GLS_templates, pcg_true.c:243-560): Legendre polynomials per sweep,
+ * azimuth-binned ground signal, HWP harmonics; white noise per block (invtt: one
+ * weight per block).  Here: solver 0 with precond 0, one rank, every block as long
+ * as its CES (sweeptstamps[i][nsweeps[i]] samples), detector-minor within a CES. */
+void MTmap(MPI_Comm comm, char *outpath, char *ref, int solver, int precond, int Z_2lvl, int pointing_commflag,
+           int npoly, int nhwp, double delta_t, int ground, int n_sss_bins, double tol, int maxiter, int enlFac,
+           int ortho_alg, int bs_red, int nside, int **sweeptstamps, int *nsweeps, double **az, double *az_min,
+           double *az_max, double **hwp_angle, int nces, void *data_size_proc, int nb_blocks_loc,
+           void *local_blocks_sizes, int Nnz, void *pix, void *pixweights, void *signal, double *noise,
+           double sampling_freq, double *invtt);
 
 /* Extension (no reference counterpart): MLmap's solve with the maps returned in
  * caller buffers (12*nside^2 each, any may be NULL) instead of files, and the

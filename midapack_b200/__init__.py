@@ -159,6 +159,7 @@ _SIGS = {
     "MLmap": (None, [ct.c_int, ct.c_char_p, ct.c_char_p, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_double,
                      ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int, c_i32p, ct.c_int, c_i32p, ct.c_int, c_i32p,
                      c_f64p, c_f64p, c_f64p, ct.c_int, c_f64p]),
+    "MTmap": (None, None),
     "MLmap_b200": (ct.c_int, [ct.c_int, ct.c_int, ct.c_double, ct.c_int, ct.c_int, ct.c_int, ct.c_int, c_i32p,
                               ct.c_int, c_i32p, c_f64p, c_f64p, c_f64p, ct.c_int, c_f64p, c_f64p, c_f64p, c_f64p,
                               c_f64p, c_i32p, ct.POINTER(ct.c_int), c_f64p]),

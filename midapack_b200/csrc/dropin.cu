@@ -747,11 +747,13 @@ static void x2map(double *mapI, double *mapQ, double *mapU, double *Cond, int *H
     }
 }
 
+// scan != nullptr: MTmap's template-filtered solve (lambda 1, one weight per block in invtt)
 static int mlmap_device(int m, int nb, const int *blocks, const int *pix, const double *w, const double *sig,
                         const double *noi, int lambda, const double *invtt, double tol, int maxiter, int verbose,
                         int precond, int z_2lvl, int solver, int enl_fac, int ortho_alg, int bs_red,
                         std::vector<double> &x, std::vector<int> &lstid, std::vector<double> &cond,
-                        std::vector<int> &hits, int *iters, double *res_rel) {
+                        std::vector<int> &hits, int *iters, double *res_rel,
+                        const mdp_template_scan *scan = nullptr) {
     mdp_context *ctx = default_ctx();
     if (!ctx) return MDP_ECUDA;
     const int64_t n3 = 3LL * m;
@@ -789,7 +791,17 @@ static int mlmap_device(int m, int nb, const int *blocks, const int *pix, const 
     mdp_solve_params    prm = {tol, maxiter, verbose, precond, z_2lvl};
     mdp_solve_info      info = {};
     std::vector<double> res(std::max(maxiter, 1) + 1, 0.0);
-    if (solver == 1) {
+    mdp_templates *T = nullptr;
+    if (scan && (rc = mdp_templates_create(ctx, scan, invtt, &T))) {
+        mdp_pointing_destroy(P);
+        mdp_noise_destroy(N);
+        return rc;
+    }
+    if (T) {
+        rc = mdp_gls_solve_templates(ctx, P, N, T, ds.as<double>(), dn.as<double>(), &prm, dx.as<double>(),
+                                     dl.as<int32_t>(), dc.as<double>(), dh.as<int32_t>(), res.data(), &info);
+        mdp_templates_destroy(T);
+    } else if (solver == 1) {
         mdp_ecg_params eprm = {tol, maxiter, enl_fac, ortho_alg, bs_red, verbose};
         rc = mdp_ecg_solve(ctx, P, N, ds.as<double>(), dn.as<double>(), &eprm, dx.as<double>(), dl.as<int32_t>(),
                            dc.as<double>(), dh.as<int32_t>(), res.data(), &info);
@@ -878,6 +890,11 @@ static int write_fits_map(const char *path, const void *data, bool is_int, int n
     return 0;
 }
 
+// the five maps as FITS files <outpath>/{mapI,mapQ,mapU,Cond,Hits}_<ref>.fits
+static void write_maps(const char *outpath, const char *ref, int nside, const std::vector<double> &x,
+                       const std::vector<int> &lstid, const std::vector<double> &cond, const std::vector<int> &hits,
+                       const char *who);
+
 extern "C" void MLmap(MPI_Comm comm, char *outpath, char *ref, int solver, int precond, int Z_2lvl,
                       int pointing_commflag, double tol, int maxiter, int enlFac, int ortho_alg, int bs_red, int nside,
                       void *data_size_proc, int nb_blocks_loc, void *local_blocks_sizes, int Nnz, void *pix,
@@ -904,6 +921,13 @@ extern "C" void MLmap(MPI_Comm comm, char *outpath, char *ref, int solver, int p
         fail("MLmap", rc);
         return;
     }
+    write_maps(outpath, ref, nside, x, lstid, cond, hits, "MLmap");
+    printf("[midapack_b200] %d iterations, final res_rel %e\n", it, rr);
+}
+
+static void write_maps(const char *outpath, const char *ref, int nside, const std::vector<double> &x,
+                       const std::vector<int> &lstid, const std::vector<double> &cond, const std::vector<int> &hits,
+                       const char *who) {
     const int64_t       npix = 12LL * nside * nside;
     std::vector<double> mI(npix, 0.0), mQ(npix, 0.0), mU(npix, 0.0), mC(npix, 0.0);
     std::vector<int>    mH(npix, 0);
@@ -914,8 +938,63 @@ extern "C" void MLmap(MPI_Comm comm, char *outpath, char *ref, int solver, int p
     for (int i = 0; i < 5; i++) {
         char fn[4096];
         snprintf(fn, sizeof(fn), "%s/%s_%s.fits", outpath, names[i], ref);
-        if (write_fits_map(fn, data[i], i == 4, nside)) fprintf(stderr, "MLmap: cannot write %s\n", fn);
+        if (write_fits_map(fn, data[i], i == 4, nside)) fprintf(stderr, "%s: cannot write %s\n", who, fn);
     }
+}
+
+// MTmap (mappraiser/src/mappraiser.c:387-800; map.h:15-18): MLmap with per-block template
+// amplitudes marginalised (PCG_GLS_templates), white noise per block (invtt: one weight
+// per block, lambda 1).  One rank, solver 0 with precond 0; every block as long as its
+// CES (sweeptstamps[i][nsweeps[i]] samples), detector-minor within each CES.
+extern "C" void MTmap(MPI_Comm comm, char *outpath, char *ref, int solver, int precond, int Z_2lvl,
+                      int pointing_commflag, int npoly, int nhwp, double delta_t, int ground, int n_sss_bins,
+                      double tol, int maxiter, int enlFac, int ortho_alg, int bs_red, int nside, int **sweeptstamps,
+                      int *nsweeps, double **az, double *az_min, double *az_max, double **hwp_angle, int nces,
+                      void *data_size_proc, int nb_blocks_loc, void *local_blocks_sizes, int Nnz, void *pix,
+                      void *pixweights, void *signal, double *noise, double sampling_freq, double *invtt) {
+    (void) comm, (void) pointing_commflag, (void) Z_2lvl, (void) enlFac, (void) ortho_alg, (void) bs_red;
+    if (solver != 0 || precond != 0 || Nnz != 3 || nces < 1 || nb_blocks_loc % nces != 0) {
+        fprintf(stderr, "midapack_b200 MTmap: solver 0 with precond 0, Nnz 3, nb_blocks_loc a multiple of nces\n");
+        return;
+    }
+    const int m = ((int *) data_size_proc)[0];
+    const int ndet = nb_blocks_loc / nces;
+    const int *blocks = (const int *) local_blocks_sizes;
+    std::vector<int32_t> nsw(nces), sw;
+    std::vector<double>  azf, hwpf;
+    for (int i = 0; i < nces; ++i) {
+        nsw[i] = nsweeps[i];
+        const int L = sweeptstamps[i][nsweeps[i]];
+        for (int k = 0; k <= nsweeps[i]; ++k) sw.push_back(sweeptstamps[i][k]);
+        for (int j = 0; j < ndet; ++j)
+            if (blocks[i * ndet + j] != L) {
+                fprintf(stderr, "midapack_b200 MTmap: block %d has %d samples, its CES %d has %d\n", i * ndet + j,
+                        blocks[i * ndet + j], i, L);
+                return;
+            }
+        if (ground) azf.insert(azf.end(), az[i], az[i] + L);
+        if (nhwp) hwpf.insert(hwpf.end(), hwp_angle[i], hwp_angle[i] + L);
+    }
+    mdp_template_scan scan = {nces, ndet, npoly, ground, n_sss_bins, nhwp, delta_t, sampling_freq, nsw.data(),
+                              sw.data(), ground ? azf.data() : nullptr, ground ? az_min : nullptr,
+                              ground ? az_max : nullptr, nhwp ? hwpf.data() : nullptr};
+    printf("\n############# MAPPRAISER MTmap (midapack_b200, one GPU) ################\n");
+    std::vector<double> x, cond;
+    std::vector<int>    lstid, hits;
+    int                 it = 0;
+    double              rr = 0;
+    int                 rc;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        rc = mlmap_device(m, nb_blocks_loc, blocks, (const int *) pix, (const double *) pixweights,
+                          (const double *) signal, noise, 1, invtt, tol, maxiter, 1, 0, 0, 0, 1, 1, 0, x, lstid, cond,
+                          hits, &it, &rr, &scan);
+    }
+    if (rc) {
+        fail("MTmap", rc);
+        return;
+    }
+    write_maps(outpath, ref, nside, x, lstid, cond, hits, "MTmap");
     printf("[midapack_b200] %d iterations, final res_rel %e\n", it, rr);
 }
 
