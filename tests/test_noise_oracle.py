@@ -47,3 +47,7 @@ def test_host_argument_checks():
         noise.noise2invtt(x, 64, 8, 100.0, 0, np.float64, "chebwin", save_psd=True)
     with pytest.raises(RuntimeError, match="Bandwidth"):
         noise.compute_invtt(1, 2, np.zeros(96), [64, 32], 17, 100.0, np.zeros(34), np.float64)
+    with pytest.raises(ValueError, match="the blocks need 96"):
+        noise.invtt_blocks(np.zeros(90), [64, 32], 8, 100.0)
+    with pytest.raises(NotImplementedError):
+        noise.noise2invtt(np.zeros(128), 64, 8, 100.0, 0, np.float64, "chebwin")   # several Welch segments
