@@ -23,9 +23,13 @@ latency).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 With --impl reference the reference's own C code (oracle/_ref, built from its
-sources) is timed on the host cores on a bounded sample of the same workload
-(one operator application P^T N^-1 P per rank, one detector per rank) and
-extrapolated to the full solve with the iteration count of the GPU solve.
+sources; no part of this library is loaded) is timed on the host cores on a
+bounded sample of the same workload: W + K operator applications P^T N^-1 P
+(the last K timed), one detector of the at-scale scan per forked rank, as many
+ranks as host cores, extrapolated to all detectors and to the solve's
+applications (REFERENCE_ITERATIONS + 1, a fixed count stated on the line);
+beside it, measured and not extrapolated, the reference's whole MLmap on the
+CPU-runnable workload.
 """
 from __future__ import annotations
 
@@ -47,6 +51,11 @@ MULTI_CONFIG = "c4_16det_2p23_1024x768_lam8192"
 METRIC = "time-to-map at 1e-8 residual, mixed vs FP64 on 1 B200; served p50/p99 latency"
 TOL = 1e-8
 MAXITER = 500
+# PCG iterations of the at-scale workload at TOL (PCG_GLS_true's recurrences and
+# stop test): fixed here for the reference arm, which cannot run the whole solve
+# on the host; the library's FP64 PCG, whose iteration counts equal the
+# reference's within one on every case both run, takes 60 on a B200.
+REFERENCE_ITERATIONS = 60
 
 
 def parse():
@@ -126,6 +135,20 @@ class Clocks:
         reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
+
+
+def workload_config(name: str, world: int) -> dict:
+    """The workload a line is measured on (both arms print the same dict)."""
+    from midapack_b200 import synth
+    c = synth.CONFIGS[name]
+    ns = c["n_det"] * c["n_samp"]
+    return {"workload": name if world == 1 else f"{name} per rank, {world} ranks",
+            "detectors": c["n_det"] * world, "samples_per_detector": c["n_samp"], "samples": ns * world,
+            "grid": f"{c['width']}x{c['height']}", "pixels": c["width"] * c["height"], "lambda": c["lam"],
+            "block_len": c["block_len"], "blocks": ns // c["block_len"] * world,
+            "flagged_fraction": c.get("gap_frac", 0.0), "fknee_hz": c.get("fknee", 1.0), "tol": TOL,
+            "l2": "inputs (tens of GB) far larger than L2",
+            "parallelism": "one solve per GPU" if world == 1 else f"one solve sharded over {world} ranks"}
 
 
 def algorithmic_bytes(ns: int, n_map: int, n_tiles: int, fft_m: int):
@@ -584,9 +607,10 @@ def bench_serving(args, device):
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.impl == "reference":
+        # the reference's own code on the host: no CUDA, no part of this library
+        return run_reference(args, rank, world)
     import torch
-    if args.impl == "reference" and rank != 0:
-        return 0
     local = local % max(torch.cuda.device_count(), 1)
     torch.cuda.set_device(local)
     if args.only:
@@ -622,8 +646,6 @@ def main():
             out = mb.gls_solve(ctx, P, N, wl.signal, wl.noise, tol=TOL, maxiter=MAXITER)
         return P, N, out
 
-    if args.impl == "reference":
-        return run_reference(args, wl, ctx, one_solve)
     if world > 1 and not args.replicas:
         return run_sharded(args, wl, ctx, rank, world, local, idv)
 
@@ -724,7 +746,7 @@ def main():
     # the reference's CPU path on a bounded sample (before any large host allocation)
     cpu = None
     if rank == 0 and not args.no_cpu and world == 1:
-        cpu = run_cpu_baseline(wl, cpu_sample(wl), info.iterations, ns)
+        cpu = run_cpu_baseline(wl, cpu_sample(wl), REFERENCE_ITERATIONS, ns)
     # pinned host inputs for the end-to-end run
     pinned = None
     if not args.no_e2e:
@@ -773,18 +795,15 @@ def main():
             "metric": METRIC, "value": round(ms / 1e3 * 1.0, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 2), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": {"workload": args.config, "samples": ns, "detectors": wl.n_det, "pixels": wl.npix,
-                       "unknowns": int(n_map), "lambda": wl.lam, "blocks": nb, "tol": TOL,
-                       "precision": args.precision, "iterations": info.iterations,
-                       "outer_iterations": info.outer_iterations, "fp64_applications": info.fp64_applications,
-                       "converged": bool(info.converged),
-                       "precond_s": round(info.precond_seconds, 4), "solve_s": round(info.solve_seconds, 4),
-                       "fft_tile": tile, "l2": "inputs (tens of GB) far larger than L2", "parallelism":
-                           "one solve per GPU" if world == 1 else f"{world} independent solves (replicas)"},
+            "config": workload_config(args.config, 1),
+            "solve": {"precision": args.precision, "unknowns": int(n_map), "iterations": info.iterations,
+                      "outer_iterations": info.outer_iterations, "fp64_applications": info.fp64_applications,
+                      "converged": bool(info.converged), "precond_s": round(info.precond_seconds, 4),
+                      "solve_s": round(info.solve_seconds, 4), "fft_tile": tile},
             "roofline": roofline, "clocks": clk, "gpu_launches": int(launches),
         }
         if other:
-            line["config"]["fp64" if other["precision"] == "fp64" else "mixed"] = other
+            line["solve"]["fp64" if other["precision"] == "fp64" else "mixed"] = other
         if args.precision == "mixed":
             line["dtype"] = "f32 operator + f64 refinement"
         if e2e:
@@ -997,13 +1016,10 @@ def run_sharded(args, wl, ctx, rank, world, local, idv):
             "warmup": args.warmup, "ms_per_step": round(ms, 2), "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 operator + f64 refinement" if fp32 else "f64",
             "data": "synthetic (seeded generator)",
-            "config": {"workload": f"{args.config} per rank, sharded over {world} ranks", "samples": ns * world,
-                       "detectors": wl.n_det * world, "pixels": wl.npix, "unknowns": int(info.n_map),
-                       "lambda": wl.lam, "tol": TOL, "precision": args.precision, "iterations": info.iterations,
-                       "outer_iterations": info.outer_iterations, "converged": bool(info.converged),
-                       "l2": "inputs (tens of GB per rank) far larger than L2",
-                       "parallelism": f"one solve sharded over {world} ranks (detectors per rank), one map "
-                                      f"all-reduce per operator application ({dist.get_backend()})"},
+            "config": workload_config(args.config, world),
+            "solve": {"precision": args.precision, "unknowns": int(info.n_map), "iterations": info.iterations,
+                      "outer_iterations": info.outer_iterations, "converged": bool(info.converged),
+                      "exchange": f"one map all-reduce per operator application ({dist.get_backend()})"},
             "roofline": {"bound": "hbm", "kernel": "P^T N^-1 P, one rank's application "
                                                   f"({'FP32' if fp32 else 'FP64'} operator)",
                          "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
@@ -1012,7 +1028,7 @@ def run_sharded(args, wl, ctx, rank, world, local, idv):
             "clocks": clk, "gpu_launches": int(launches),
         }
         if other:
-            line["config"]["fp64" if other["precision"] == "fp64" else "mixed"] = other
+            line["solve"]["fp64" if other["precision"] == "fp64" else "mixed"] = other
         if e2e:
             line["e2e"] = e2e
         print(json.dumps(line), flush=True)
@@ -1068,31 +1084,60 @@ def run_sharded_e2e(args, wl, ctx, world, idv):
             "api": "midapack_b200.dist.ShardedGLS(GpuShard(...)).solve, host inputs (all ranks)"}
 
 
-def run_reference(args, wl, ctx, one_solve):
-    import torch
-    # iteration count of the same solve (device run, untimed) to extrapolate the operator cost
-    _, _, out = one_solve()
-    iters = out[5].iterations
-    sample_dets = max(1, min(host_cores(), wl.n_det))
-    per_det = wl.n_samp
-    pix = wl.pix[:3 * per_det * sample_dets].cpu().numpy()
-    w = wl.weights[:3 * per_det * sample_dets].cpu().numpy()
-    vals = []
-    for _ in range(max(args.steps, 1)):
-        r = cpu_reference((pix, w, wl.block_sizes, wl.lam, wl.invtt, per_det), iters, sample_dets, wl.n_samples,
-                          sample_dets)
-        vals.append(r["time_to_map_s"])
-    v = float(np.mean(vals))
-    line = {"impl": "reference", "metric": METRIC, "value": round(v, 2), "unit": "s", "n_gpus": 0,
-            "steps": len(vals), "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": {"workload": args.config, "iterations": iters},
-            "cpu_baseline": {"value": round(v, 2), "unit": "s", "cores": sample_dets, "kind": "reference",
-                             "sample": f"{sample_dets} detector(s) x 2^24 samples, one P^T N^-1 P per rank, "
-                                       f"extrapolated to 64 detectors x {iters + 1} applications"},
+def run_reference(args, rank, world):
+    """The reference arm: the reference's own C operator (oracle/_ref) on the
+    host cores, on a bounded sample of the workload (W + K applications of
+    P^T N^-1 P on as many detectors as host cores, one forked rank each; the
+    last K timed), extrapolated to all detectors and REFERENCE_ITERATIONS + 1
+    applications; beside it the reference's whole MLmap on the CPU-runnable
+    workload, measured.  Rank 0 alone runs it; nothing here touches CUDA or
+    loads this library."""
+    if rank != 0:
+        return 0
+    from midapack_b200 import synth
+    from oracle import cpu_baseline as cb
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference compiled from its "
+                                                              "sources) is not built"}), flush=True)
+        return 0
+    cfg = synth.CONFIGS[args.config]
+    cores = host_cores()
+    sample = max(1, min(cores, cfg["n_det"]))
+    times = cb.operator_sample(cfg, sample, max(args.warmup, 0) + max(args.steps, 1))
+    timed = times[max(args.warmup, 0):]
+    per_app = float(np.mean(timed))
+    n_det_total = cfg["n_det"] * world
+    # `sample` ranks ran at once on `cores` cores: the full operator is n_det_total/sample such rounds
+    per_app_full = per_app * n_det_total / sample * (sample / min(cores, sample))
+    v = per_app_full * (REFERENCE_ITERATIONS + 1)
+    c1 = None
+    try:
+        c1cfg = dict(synth.CONFIGS["c1_4det_2p20_256x192_lam4096"], gap_frac=0.01)
+        wl1 = synth.make_workload("c1", **c1cfg)
+        t1, it1, _ = cb.mlmap_workload(wl1, 4, TOL, 4 * MAXITER)
+        c1 = {"workload": "c1_4det_2p20_256x192_lam4096 + 1% flagged samples",
+              "path": "reference MLmap (oracle/_ref, shim FFT/MPI/LAPACK), 4 forked host ranks, measured",
+              "time_to_map_s": round(t1, 3), "iterations": it1, "ranks": 4}
+    except Exception as ex:  # noqa: BLE001 - reported on the line
+        c1 = {"error": f"{type(ex).__name__}: {ex}"}
+    sample_txt = (f"reference C (oracle/_ref: the reference's sources, shim FFT/MPI) P^T N^-1 P on {sample} "
+                  f"detector(s) x {cfg['n_samp']} samples as {sample} forked ranks, {len(timed)} timed applications "
+                  f"after {len(times) - len(timed)} untimed: {per_app:.3f} s each; extrapolated x{n_det_total // sample}"
+                  f" detectors x {REFERENCE_ITERATIONS + 1} applications")
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 2), "unit": "s", "n_gpus": world,
+            "steps": len(timed), "warmup": len(times) - len(timed), "ms_per_step": round(v * 1e3, 1),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator)", "config": workload_config(args.config, world),
+            "solve": {"precision": "fp64", "iterations": REFERENCE_ITERATIONS,
+                      "iterations_source": "fixed: the at-scale FP64 PCG iteration count at tol 1e-8",
+                      "seconds_per_application": round(per_app_full, 3),
+                      "sample_application_s": [round(t, 4) for t in timed]},
+            "cpu_baseline": {"value": round(v, 2), "unit": "s", "cores": min(cores, sample), "kind": "reference",
+                             "sample": sample_txt},
+            "c1_reference_mlmap": c1,
             "e2e": {"value": round(v, 2), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-    del torch
     return 0
 
 

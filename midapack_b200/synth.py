@@ -153,6 +153,35 @@ def make_workload(name: str, width: int, height: int, n_det: int, n_samp: int, b
     return wl
 
 
+def make_pointing(width: int, height: int, n_det: int, n_samp: int, block_len: int, lam: int, fknee: float = 1.0,
+                  seed: int = 20261203, gap_frac: float = 0.0, **_unused):
+    """Pointing and noise model of the first ``n_det`` detectors of a workload,
+    without its TOD: (pix int32 [3Ns], weights f64 [3Ns], block_sizes int32,
+    invtt f64 [n_blocks*lam]).  Same scan, angles, flags and Toeplitz rows as
+    make_workload, from its own seeded stream (host, numpy; for timing an
+    operator on a sample of a large workload)."""
+    rng = np.random.default_rng(seed)
+    ns = n_det * n_samp
+    p = scan_pixels(width, height, n_det, n_samp, rng).reshape(-1)
+    if gap_frac > 0:
+        p = np.where(rng.random(ns) < gap_frac, -1, p)
+    idx = np.empty((ns, 3), dtype=np.int32)
+    idx[:] = (3 * p).astype(np.int32)[:, None]
+    del p
+    idx += np.arange(3, dtype=np.int32)[None, :]
+    w = np.empty((ns, 3))
+    w[:, 0] = 1.0
+    two_psi = 2.0 * psi_angles(n_det, n_samp).reshape(-1)
+    w[:, 1] = np.cos(two_psi)
+    w[:, 2] = np.sin(two_psi)
+    del two_psi
+    if n_samp % block_len != 0:
+        raise ValueError("block_len must divide n_samp")
+    nb = ns // block_len
+    return idx.reshape(-1), w.reshape(-1), np.full(nb, block_len, dtype=np.int32), np.tile(
+        invtt_row(block_len, lam, fknee), nb)
+
+
 def mc_noise(n_det: int, n_samp: int, nrhs: int, fknee: float = 1.0, seed: int = 0) -> np.ndarray:
     """Monte-Carlo noise realisations with the workload's PSD: [nrhs, n_det*n_samp]
     float32 (the columns of a multi-RHS solve; FP32 values are exact inputs)."""

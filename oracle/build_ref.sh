@@ -4,12 +4,18 @@
 # project-written shims in oracle/shim/ that stand in for MPI, FFTW3, LAPACKE
 # and CFITSIO, none of which exist in this image.  Test infrastructure only.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh [--if-present] [REFERENCE_ROOT]
+#   REFERENCE_ROOT defaults to $MIDAPACK_REFERENCE, else /root/reference.
+#   --if-present: exit 0 without building when the sources are not there
+#   (a machine that only has the prebuilt oracle/_ref).
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+IF_PRESENT=0
+if [ "${1:-}" = "--if-present" ]; then IF_PRESENT=1; shift; fi
+REF="${1:-${MIDAPACK_REFERENCE:-/root/reference}}"
 OUT="$HERE/_ref"
 if [ ! -d "$REF/algebra" ]; then
+  if [ "$IF_PRESENT" = 1 ]; then exit 0; fi
   echo "build_ref.sh: reference sources not found at $REF" >&2
   exit 2
 fi

@@ -8,6 +8,9 @@ oracle forks one process per rank).
     python -m oracle.cpu_baseline --mlmap CASE.npz RANKS OUT.npz
         -> runs the reference's whole MLmap (RANKS forked ranks, detectors split
            evenly), prints its wall time and iterations (JSON), saves its maps
+
+operator_sample() and mlmap_workload() do the same in the calling process for a
+caller that has not initialised CUDA (the reference arm of bench.py).
 """
 import json
 import sys
@@ -42,6 +45,34 @@ def mlmap(path, ranks, out):
     t = time.perf_counter() - t0
     np.savez(out, I=maps[0], Q=maps[1], U=maps[2], Cond=maps[3], Hits=maps[4], res=maps[5])
     print(json.dumps({"seconds": t, "ranks": ranks, "iterations": int(len(maps[5]) - 1)}))
+
+
+def operator_sample(cfg: dict, ranks: int, reps: int):
+    """The reference's P^T N^-1 P on the first `ranks` detectors of the workload
+    `cfg` (a synth configuration; one detector per forked rank, pointing and
+    Toeplitz rows from synth.make_pointing): seconds of each of `reps`
+    applications, max over ranks."""
+    from midapack_b200 import synth
+    cfg = dict(cfg, n_det=ranks)
+    pix, w, bs, invtt = synth.make_pointing(**cfg)
+    per = int(cfg["n_samp"])
+    nbp = per // int(cfg["block_len"])
+    return ref.operator_time(ranks, [per] * ranks, [nbp] * ranks, bs, pix, w, int(cfg["lam"]), invtt, reps=reps,
+                             each=True)
+
+
+def mlmap_workload(wl, ranks: int, tol: float, maxiter: int):
+    """The reference's whole MLmap on `ranks` forked ranks for a synth workload
+    (detectors and blocks split evenly): (seconds, iterations, maps)."""
+    import time
+    m = int(wl.signal.size)
+    nb = int(wl.block_sizes.size)
+    if m % ranks or nb % ranks:
+        raise ValueError("samples and blocks must split evenly over the ranks")
+    t0 = time.perf_counter()
+    maps = ref.mlmap(ranks, [m // ranks] * ranks, [nb // ranks] * ranks, wl.block_sizes, wl.pix, wl.weights,
+                     wl.signal, wl.noise, int(wl.lam), wl.invtt, int(wl.nside), tol=tol, maxiter=maxiter)
+    return time.perf_counter() - t0, int(len(maps[5]) - 1), maps
 
 
 if __name__ == "__main__":

@@ -122,8 +122,10 @@ def mlmap(nranks, data_size_proc, nb_blocks_proc, block_sizes, pix, weights, sig
     return out + (res,)
 
 
-def operator_time(nranks, data_size_proc, nb_blocks_proc, block_sizes, pix, weights, lam, invtt, reps=1, nnz=3):
-    """Seconds per P^T N^-1 P application (max over ranks), reference code on host cores."""
+def operator_time(nranks, data_size_proc, nb_blocks_proc, block_sizes, pix, weights, lam, invtt, reps=1, nnz=3,
+                  each=False):
+    """Seconds per P^T N^-1 P application (max over ranks), reference code on host cores:
+    the mean over `reps` applications, or (each=True) the list of their times."""
     dsp = np.ascontiguousarray(data_size_proc, dtype=np.int32)
     nbp = np.ascontiguousarray(nb_blocks_proc, dtype=np.int32)
     bs = np.ascontiguousarray(block_sizes, dtype=np.int32)
@@ -136,7 +138,8 @@ def operator_time(nranks, data_size_proc, nb_blocks_proc, block_sizes, pix, weig
                                      _p(w, F64), _p(tt, F64), path.encode())
         if rc != 0:
             raise RuntimeError(f"reference operator timing failed (status {rc})")
-        return float(np.fromfile(path, dtype=np.float64)[0])
+        t = np.fromfile(path, dtype=np.float64)
+        return [float(v) for v in t] if each else float(t.mean())
 
 
 def _scan_args(sc):

@@ -11,13 +11,12 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
-    config.addinivalue_line("markers", "gpu_pending: needs a CUDA device; written, not yet run on a B200 "
-                                       "(run with -m gpu_pending; joins the gpu set once it has passed there)")
-    # the reference oracle library is built from /root/reference where that exists;
-    # elsewhere (the GPU box) the prebuilt oracle/_ref travels with the tree
+    # the reference oracle library is built from the reference's sources where they
+    # exist (oracle/build_ref.sh finds them: $MIDAPACK_REFERENCE or its default);
+    # elsewhere the prebuilt oracle/_ref travels with the tree
     ref_so = os.path.join(ROOT, "oracle", "_ref", "libmidapack_ref.so")
-    if not os.path.exists(ref_so) and os.path.isdir("/root/reference/algebra"):
-        subprocess.run([os.path.join(ROOT, "oracle", "build_ref.sh")], check=False,
+    if not os.path.exists(ref_so):
+        subprocess.run([os.path.join(ROOT, "oracle", "build_ref.sh"), "--if-present"], check=False,
                        stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
 
 

@@ -2,15 +2,13 @@
 white noise operator, the PCG_GLS_true recurrences with the template weighting
 W - W T B T^T W) against the reference's own MTmap (oracle/_ref, one rank):
 maps on the observed pixels within 1e-10, same cut, cond and hits, iteration
-count +-1.
-
-Marked gpu_pending: written but not yet run on a B200."""
+count +-1."""
 import numpy as np
 import pytest
 
 from tests._cases import template_case
 
-pytestmark = pytest.mark.gpu_pending
+pytestmark = pytest.mark.gpu
 
 VARIANTS = {
     "poly2_sss8_hwp2": dict(npoly=2, ground=1, n_sss_bins=8, nhwp=2),
