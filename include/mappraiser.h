@@ -7,6 +7,7 @@
  *                                                      precondblockjacobilike
  *   mappraiser/include/mappraiser/create_toeplitz.h    defineTpltz_avg, defineBlocks_avg
  *   mappraiser/include/mappraiser/ecg.h:6-7            ECG_GLS
+ *   mappraiser/include/mappraiser/iofiles.h:24         write_map
  * Scope: solver 0 (PCG) with precond 0 (block Jacobi), 1 and 2 (two-level),
  * solver 1 (ECG, block Jacobi), on one GPU; MTmap with solver 0, precond 0.
  * Other solver/precond values return an error (MLmap/MTmap print it and return).
@@ -86,6 +87,13 @@ void MTmap(MPI_Comm comm, char *outpath, char *ref, int solver, int precond, int
            double *az_max, double **hwp_angle, int nces, void *data_size_proc, int nb_blocks_loc,
            void *local_blocks_sizes, int Nnz, void *pix, void *pixweights, void *signal, double *noise,
            double sampling_freq, double *invtt);
+
+/* iofiles.h:24 -> iofiles.c:19-52: one HEALPix map (12*nside^2 values of type
+ * 82 = TDOUBLE or 31 = TINT, CFITSIO's codes) as a FITS binary table with one
+ * column SIGNAL of 8-byte doubles (integers converted, as CFITSIO converts them),
+ * ORDERING NESTED (nest != 0) or RING, COORDSYS from coordsys[0].  Written by
+ * the library itself (CFITSIO is not needed). */
+void write_map(void *signal, int type, long nside, const char *filename, char nest, const char *coordsys);
 
 /* Extension (no reference counterpart): MLmap's solve with the maps returned in
  * caller buffers (12*nside^2 each, any may be NULL) instead of files, and the

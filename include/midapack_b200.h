@@ -109,11 +109,21 @@ int  mdp_prepare_fp32(mdp_context *ctx, mdp_pointing *A, mdp_noise *N);
  * threads per CTA, and whether the autotuner picked it (1) by timing the
  * candidate plans on this device, or the cost model did (0).  A split plan
  * (three kernels, four-step FFT of 2^split_log_m1 x 2^split_log_m2 points)
- * reports split_log_m1 > 0 and cluster 0.  The autotuner runs once per
- * precision, band (ceil log2 lambda) and block length class;
- * MDP_TOEPLITZ_TUNE=0 switches it off. */
+ * reports split_log_m1 > 0 and cluster 0; a cluster four-step plan (one
+ * cluster of C CTAs per tile, 2C x 4096 points, the tile on chip) reports
+ * split_log_m1 = log2(2C), split_log_m2 = 12 and cluster C.  The autotuner runs
+ * once per precision, band (ceil log2 lambda) and block length class. */
 int  mdp_noise_plan(mdp_context *ctx, mdp_noise *N, int fp32, int *log2_cta_points, int *cluster_ctas,
                     int *threads, int *tuned, int *split_log_m1, int *split_log_m2);
+/* No counterpart in the reference.  Replaces the tile plan of one precision
+ * (fp32 = 0: the FP64 operator, 1: the FP32 operator of the mixed solves):
+ * "auto" (the autotuner's choice), "model" (the cost model's choice, nothing
+ * timed), "fft:N" (the cost model's choice among one-kernel tiles of N real
+ * samples), "log2_cta_points,cluster,threads" (one-kernel tiles),
+ * "s,log_m1,log_m2" (three-kernel split tiles) or "c,C" (cluster four-step
+ * tiles of C CTAs).  For tests and tuning; MDP_EINVAL when the plan does not
+ * hold the band. */
+int  mdp_noise_set_plan(mdp_context *ctx, mdp_noise *N, int fp32, const char *plan);
 /* No counterpart in the reference.  out = N^-1 in like mdp_stbmm, but the call
  * allocates no device memory: for callers that cannot call cudaMalloc while
  * they apply the operator (a memory arena or pool that owns the device memory,
@@ -124,9 +134,11 @@ int  mdp_noise_plan(mdp_context *ctx, mdp_noise *N, int fp32, int *log2_cta_poin
  * operator needing more (one double per block plus one per 65536-row chunk of
  * every block) is rejected with MDP_EINVAL, as is d_in == d_out.  The first
  * call on a device looks up that array's device address (once per device), so
- * make the first call before any stream capture.  All calls share the array:
- * calls that overlap on the GPU (other streams, other threads, other contexts
- * on the same device) race on it and must be serialised by the caller. */
+ * make the first call before any stream capture.  The cached address belongs
+ * to the device's primary context (the runtime's): calls from another context
+ * on that device, or after cudaDeviceReset, are not supported.  All calls
+ * share the array: calls that overlap on the GPU (other streams, other
+ * threads) race on it and must be serialised by the caller. */
 int  mdp_stbmm_noalloc(mdp_context *ctx, const mdp_noise *N, const double *d_in, double *d_out);
 
 /* ---- GLS solve (reference PCG_GLS_true, pcg_true.c:20-241) ---- */

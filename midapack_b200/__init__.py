@@ -85,6 +85,8 @@ _SIGS = {
     "mdp_trmatvec": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "mdp_noise_create": (ct.c_int, [ct.c_void_p, ct.c_int, ct.POINTER(ct.c_int64), c_i32p, ct.c_int, c_f64p,
                                     ct.POINTER(ct.c_void_p)]),
+    "write_map": (None, [ct.c_void_p, ct.c_int, ct.c_long, ct.c_char_p, ct.c_char, ct.c_char_p]),
+    "mdp_noise_set_plan": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_char_p]),
     "mdp_noise_destroy": (None, [ct.c_void_p]),
     "mdp_stbmm": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "mdp_stbmm_noalloc": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
@@ -305,10 +307,18 @@ class Noise:
                                      bs.ctypes.data_as(c_i32p), lam, tt.ctypes.data_as(c_f64p), ct.byref(self.h)),
               "mdp_noise_create")
 
+    def set_plan(self, plan: str, fp32: bool = False):
+        """Replaces the tile plan of one precision (see mdp_noise_set_plan):
+        "auto", "model", "fft:N", "log2_ml,cluster,threads", "s,log_m1,log_m2", "c,C"."""
+        check(lib().mdp_noise_set_plan(self.ctx.h, self.h, int(fp32), plan.encode()), "mdp_noise_set_plan")
+        return self
+
     def _plan(self, fp32: int):
         lm, c, th, tu, s1, s2 = (ct.c_int() for _ in range(6))
         check(lib().mdp_noise_plan(self.ctx.h, self.h, fp32, ct.byref(lm), ct.byref(c), ct.byref(th), ct.byref(tu),
                                    ct.byref(s1), ct.byref(s2)))
+        if s1.value and c.value:
+            return dict(cluster_four_step=[1 << s1.value, 1 << s2.value], tuned=bool(tu.value))
         if s1.value:
             return dict(split=[1 << s1.value, 1 << s2.value], tuned=bool(tu.value))
         return dict(cta_points=1 << lm.value, threads=th.value, tuned=bool(tu.value))

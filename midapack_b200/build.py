@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmidapack_b200.so")
-SOURCES = ["pointing.cu", "toeplitz.cu", "solver.cu", "twolevel.cu", "ecg.cu", "multirhs.cu", "noise.cu", "templates.cu",
+SOURCES = ["pointing.cu", "toeplitz.cu", "ninv4.cu", "solver.cu", "twolevel.cu", "ecg.cu", "multirhs.cu", "noise.cu", "templates.cu",
            "dropin.cu"]
 
 

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <ctime>
 #include <mutex>
 #include <unordered_map>
 
@@ -261,16 +262,12 @@ extern "C" int tpltz_init(int n, int lambda, int *nfft, int *blocksize, fftw_com
     *V_fft = (fftw_complex *) malloc(sizeof(fftw_complex) * (size_t) (*nfft) * h);
     *V_rfft = (double *) malloc(sizeof(double) * (size_t) (*nfft) * bs);
     if (!*T_fft || !*V_fft || !*V_rfft) return 2;  // toeplitz.c error 2: bad allocation
-    // spectrum of the circulant embedding (real, even): T0 + 2 sum T[i] cos(2 pi i k / bs)
-    for (int k = 0; k < h; k++) {
-        long double acc = 0.0L;
-        for (int i = 1; i < lambda && i < bs; i++) {
-            long double ang = 2.0L * 3.14159265358979323846264338327950288L * (long double) (((int64_t) i * k) % bs) /
-                              (long double) bs;
-            acc += (long double) T[i] * cosl(ang);
-        }
-        (*T_fft)[k][0] = (double) ((long double) T[0] + 2.0L * acc);
-        (*T_fft)[k][1] = 0.0;
+    // spectrum of the circulant embedding, computed on the device (circ_init_fftw's
+    // r2c transform of c[0] = T[0], c[i] = c[bs-i] = T[i])
+    mdp_context *ctx = default_ctx();
+    if (!ctx || mdp_circulant_spectrum(ctx, T, lambda, bs, &(*T_fft)[0][0]) != MDP_OK) {
+        fprintf(stderr, "tpltz_init: %s\n", mdp_last_error());
+        return 3;
     }
     HostPlan *pf = new HostPlan{bs}, *pb = new HostPlan{bs};
     *plan_f = (fftw_plan) pf;
@@ -828,7 +825,12 @@ static int mlmap_device(int m, int nb, const int *blocks, const int *pix, const 
     return rc;
 }
 
-// minimal HEALPix FITS binary table writer (the layout of write_map, iofiles.c:19-52)
+// HEALPix FITS map writer with the layout the reference's write_map
+// (iofiles.c:19-52) gets from CFITSIO: an empty primary array (BITPIX 16,
+// NAXIS 0, EXTEND) with its creation DATE, then one binary table of 12 nside^2
+// rows and one column SIGNAL of format 1D (8-byte doubles, big endian; integer
+// maps are converted, as fits_write_col converts them into that column) with
+// PIXTYPE, ORDERING, NSIDE, COORDSYS and the coordinate-system comment.
 static void fits_card(std::string &h, const char *key, const char *val, const char *comment) {
     char c[81];
     if (val)
@@ -839,55 +841,87 @@ static void fits_card(std::string &h, const char *key, const char *val, const ch
     s.resize(80, ' ');
     h += s;
 }
+static void fits_string_card(std::string &h, const char *key, const char *val, const char *comment) {
+    char q[72];
+    snprintf(q, sizeof(q), "'%-8s'", val);  // strings padded to at least 8 characters
+    char c[81];
+    snprintf(c, sizeof(c), "%-8.8s= %-20s / %-47.47s", key, q, comment);
+    std::string s(c);
+    s.resize(80, ' ');
+    h += s;
+}
 static void fits_pad(std::string &h, char fill) {
     while (h.size() % 2880) h.push_back(fill);
 }
-static int write_fits_map(const char *path, const void *data, bool is_int, int nside) {
+// CFITSIO's data type codes of the two maps MLmap writes
+#define MDP_FITS_TINT 31
+#define MDP_FITS_TDOUBLE 82
+static int write_fits_map(const char *path, const void *data, int type, long nside, bool nest, char coordsys) {
     const int64_t npix = 12LL * nside * nside;
     std::string   hdr;
     fits_card(hdr, "SIMPLE", "T", "file does conform to FITS standard");
     fits_card(hdr, "BITPIX", "16", "number of bits per data pixel");
     fits_card(hdr, "NAXIS", "0", "number of data axes");
     fits_card(hdr, "EXTEND", "T", "FITS dataset may contain extensions");
+    {
+        char           date[32];
+        const time_t   now = time(nullptr);
+        struct tm      ut;
+        gmtime_r(&now, &ut);
+        strftime(date, sizeof(date), "%Y-%m-%dT%H:%M:%S", &ut);
+        fits_string_card(hdr, "DATE", date, "file creation date (YYYY-MM-DDThh:mm:ss UT)");
+    }
     fits_card(hdr, "END", nullptr, nullptr);
     fits_pad(hdr, ' ');
     std::string ext;
     char        v[32];
-    fits_card(ext, "XTENSION", "'BINTABLE'", "binary table extension");
+    fits_string_card(ext, "XTENSION", "BINTABLE", "binary table extension");
     fits_card(ext, "BITPIX", "8", "8-bit bytes");
     fits_card(ext, "NAXIS", "2", "2-dimensional binary table");
-    snprintf(v, sizeof(v), "%d", is_int ? 4 : 8);
-    fits_card(ext, "NAXIS1", v, "width of table in bytes");
+    fits_card(ext, "NAXIS1", "8", "width of table in bytes");
     snprintf(v, sizeof(v), "%lld", (long long) npix);
     fits_card(ext, "NAXIS2", v, "number of rows in table");
     fits_card(ext, "PCOUNT", "0", "size of special data area");
     fits_card(ext, "GCOUNT", "1", "one data group (required keyword)");
     fits_card(ext, "TFIELDS", "1", "number of fields in each row");
-    fits_card(ext, "TTYPE1", "'SIGNAL  '", "label for field 1");
-    fits_card(ext, "TFORM1", is_int ? "'1J      '" : "'1D      '", "data format of field");
-    fits_card(ext, "EXTNAME", "'BINTABLE'", "name of this binary table extension");
-    fits_card(ext, "PIXTYPE", "'HEALPIX '", "HEALPIX Pixelisation");
-    fits_card(ext, "ORDERING", "'NESTED  '", "Pixel ordering scheme, either RING or NESTED");
-    snprintf(v, sizeof(v), "%d", nside);
+    fits_string_card(ext, "TTYPE1", "SIGNAL", "label for field   1");
+    fits_string_card(ext, "TFORM1", "1D", "data format of field: 8-byte DOUBLE");
+    fits_string_card(ext, "TUNIT1", " ", "physical unit of field");
+    fits_string_card(ext, "EXTNAME", "BINTABLE", "name of this binary table extension");
+    fits_string_card(ext, "PIXTYPE", "HEALPIX", "HEALPIX Pixelisation");
+    fits_string_card(ext, "ORDERING", nest ? "NESTED" : "RING", "Pixel ordering scheme, either RING or NESTED");
+    snprintf(v, sizeof(v), "%ld", nside);
     fits_card(ext, "NSIDE", v, "Resolution parameter for HEALPIX");
-    fits_card(ext, "COORDSYS", "'C       '", "Pixelisation coordinate system");
+    const char cs[2] = {coordsys, 0};
+    fits_string_card(ext, "COORDSYS", cs, "Pixelisation coordinate system");
+    fits_card(ext, "COMMENT G = Galactic, E = ecliptic, C = celestial = equatorial", nullptr, nullptr);
     fits_card(ext, "END", nullptr, nullptr);
     fits_pad(ext, ' ');
     FILE *f = fopen(path, "wb");
     if (!f) return 1;
     fwrite(hdr.data(), 1, hdr.size(), f);
     fwrite(ext.data(), 1, ext.size(), f);
-    const size_t        es = is_int ? 4 : 8;
-    std::vector<char>   buf(es * (size_t) npix);
-    const unsigned char *src = (const unsigned char *) data;
-    for (int64_t i = 0; i < npix; i++)
-        for (size_t b = 0; b < es; b++) buf[es * i + b] = (char) src[es * i + (es - 1 - b)];  // big endian
+    std::vector<char> buf(8 * (size_t) npix);
+    for (int64_t i = 0; i < npix; i++) {
+        const double d = (type == MDP_FITS_TINT) ? (double) ((const int *) data)[i] : ((const double *) data)[i];
+        const unsigned char *src = (const unsigned char *) &d;
+        for (int b = 0; b < 8; b++) buf[8 * i + b] = (char) src[7 - b];  // big endian
+    }
     fwrite(buf.data(), 1, buf.size(), f);
-    size_t tail = (2880 - buf.size() % 2880) % 2880;
+    size_t            tail = (2880 - buf.size() % 2880) % 2880;
     std::vector<char> z(tail, 0);
     fwrite(z.data(), 1, tail, f);
-    fclose(f);
-    return 0;
+    return fclose(f) == 0 ? 0 : 1;
+}
+
+// iofiles.h:24 -> iofiles.c:19-52
+extern "C" void write_map(void *signal, int type, long nside, const char *filename, char nest, const char *coordsys) {
+    if (!signal || !filename || nside < 1 || (type != MDP_FITS_TINT && type != MDP_FITS_TDOUBLE)) {
+        fprintf(stderr, "write_map: a TDOUBLE (82) or TINT (31) map of nside >= 1 is needed\n");
+        return;
+    }
+    const char c = (coordsys && coordsys[0]) ? coordsys[0] : 'C';
+    if (write_fits_map(filename, signal, type, nside, nest != 0, c)) fprintf(stderr, "write_map: cannot write %s\n", filename);
 }
 
 // the five maps as FITS files <outpath>/{mapI,mapQ,mapU,Cond,Hits}_<ref>.fits
@@ -938,7 +972,8 @@ static void write_maps(const char *outpath, const char *ref, int nside, const st
     for (int i = 0; i < 5; i++) {
         char fn[4096];
         snprintf(fn, sizeof(fn), "%s/%s_%s.fits", outpath, names[i], ref);
-        if (write_fits_map(fn, data[i], i == 4, nside)) fprintf(stderr, "%s: cannot write %s\n", who, fn);
+        if (write_fits_map(fn, data[i], i == 4 ? MDP_FITS_TINT : MDP_FITS_TDOUBLE, nside, true, 'C'))
+            fprintf(stderr, "%s: cannot write %s\n", who, fn);
     }
 }
 

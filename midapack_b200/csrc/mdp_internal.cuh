@@ -145,7 +145,8 @@ struct mdp_pointing {
 // solver).  V = double2 or float2.
 struct mdp_tile_plan {
     int     ready = 0;
-    int     split = 0;     // 0: one kernel (one CTA or cluster per tile); 1: three-kernel four-step FFT
+    int     split = 0;     // 0: one kernel (one CTA or cluster per tile); 1: three-kernel four-step FFT;
+                           // 2: cluster four-step (ninv4.cu: C = cluster CTAs, M = 2C x 4096 points)
     int     log_m1 = 0, log_m2 = 0;  // split: M = 2^log_m1 * 2^log_m2 complex points per tile
     DevBuf  scratch;       // split: [n_tiles][M] complex work array
     DevBuf  ltw2, wa, wb;  // split: row-pass twiddles, W_M factor tables
@@ -159,6 +160,13 @@ struct mdp_tile_plan {
     DevBuf  tile_block;    // int32 [n_tiles]
     DevBuf  spectra;       // V [n_spec][N/4+1]: spectrum pairs in tile position order
     DevBuf  ltw, twm, ttw; // packed local-pass, cross-CTA and twist twiddles
+    void reset() {         // back to an unbuilt plan, device buffers released
+        ready = split = log_m1 = log_m2 = log2_ml = threads = fft_n = tuned = 0;
+        cluster = 1;
+        n_tiles = 0;
+        for (DevBuf *b : {&scratch, &ltw2, &wa, &wb, &tile_start, &tile_block, &spectra, &ltw, &twm, &ttw})
+            b->release();
+    }
 };
 
 struct mdp_noise {
@@ -231,6 +239,17 @@ int mdp_exclusive_scan_u32(mdp_context *ctx, const uint32_t *d_in, uint32_t *d_o
 int mdp_stbmm_impl(mdp_context *ctx, const mdp_noise *N, const double *d_in, double *d_out,
                    const double *d_means_or_null);
 int mdp_block_means(mdp_context *ctx, const mdp_noise *N, const double *d_v, double *d_means);
+// spectrum of the reference's circulant embedding of T (circ_init_fftw), bs/2+1 complex into h_F
+int mdp_circulant_spectrum(mdp_context *ctx, const double *h_T, int lambda, int bs, double *h_F);
+// H[k], k = 0..Nn/2, of the Nn-point circulant embedding of the band T (device,
+// FP64); d_tw = exp(-2 pi i k / Nn), k < Nn/2
+int mdp_spectrum_H(mdp_context *ctx, const double *h_T, int lambda, int Nn, const double2 *d_tw, double *d_H);
+// cluster four-step tiles of N^-1 (ninv4.cu): tables of a plan, launch
+template <typename T>
+int ninv4_build(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, bool spectra);
+template <typename T>
+int ninv4_launch(mdp_context *ctx, const mdp_noise *N, const mdp_tile_plan &P, const T *d_in, T *d_out,
+                 const double *d_means, int ncols, int64_t col_stride, const int *d_active);
 int mdp_matvec_blockmeans(mdp_context *ctx, const mdp_pointing *A, const mdp_noise *N, const double *d_x,
                           double *d_y);
 // FP32 operator pieces (mixed precision)
@@ -255,3 +274,8 @@ inline int grid_for(int64_t n, int threads, int max_blocks = 148 * 16) {
 
 // sample lists of the pointing's rows grouped by bins of bin_pix pixels
 int mdp_build_bins(mdp_context *ctx, mdp_pointing *A, int bin_pix, mdp_pt_bins *B);
+// P^T and the block-Jacobi sums run over bins of MDP_PT_BIN_PIX pixels when the
+// pointing is a triplet pointing of 2^20 rows or more (pointing.cu)
+#define MDP_PT_BIN_PIX 256
+bool mdp_pointing_binned(const mdp_pointing *A);
+int  mdp_pointing_bins(mdp_context *ctx, mdp_pointing *A);  // builds A->bins when missing

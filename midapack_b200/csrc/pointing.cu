@@ -608,43 +608,89 @@ __global__ void trmatvec_general_kernel(const int32_t *__restrict__ local, const
     }
 }
 
-// ---- P^T by map bins.  The samples of a bin of BIN_PIX consecutive pixels are
-// listed once per pointing (roughly in time order: a warp's 32 consecutive
-// samples that fall in one bin get consecutive slots).  Each CTA then sums a
-// slice of one bin's samples into a shared-memory copy of the bin's map
-// (FP64 shared atomics) and adds it to the map with one global atomic per
-// entry, instead of three global atomics per sample.
-#define PT_BIN_PIX 2048
-#define PT_SPLIT 4
+// ---- P^T by map bins.  The samples of each bin of PT_BIN_PIX consecutive
+// pixels are listed once per pointing, in time order (a stable partition of
+// the rows by bin, so the list is the same on every build): counts per
+// (row chunk, bin), bin totals, an exclusive scan over the bins, per-chunk
+// offsets within each bin, then one warp per row chunk writes its rows in
+// order.  One warp then owns one bin: it walks the bin's list in order, 32
+// rows a step, and adds each row's three products into its shared-memory copy
+// of the bin's map; rows of one step that hit the same pixel are added in
+// lane order.  Every map entry is written once, by its bin's warp: the sums
+// are reproducible bit for bit (the order of every addition is fixed) and no
+// atomic operation touches the map.
+#define PT_BIN_PIX MDP_PT_BIN_PIX
+#define PT_WARPS 8
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
-__global__ void bin_count_kernel(const int32_t *__restrict__ off, int64_t m, int bin3, uint32_t *__restrict__ count) {
-    for (int64_t t0 = (int64_t) blockIdx.x * blockDim.x; t0 < m; t0 += (int64_t) gridDim.x * blockDim.x) {
+// count[c][b] += rows of chunk c (rows [c*chunk, (c+1)*chunk)) in bin b
+__global__ void bin_chunk_count_kernel(const int32_t *__restrict__ off, int64_t m, int bin3, int64_t chunk,
+                                       int64_t nbins, uint32_t *__restrict__ count) {
+    const int64_t c = blockIdx.x;
+    const int64_t r0 = c * chunk, r1 = min(m, r0 + chunk);
+    uint32_t     *row = count + c * nbins;
+    for (int64_t t0 = r0; t0 < r1; t0 += blockDim.x) {
         const int64_t t = t0 + threadIdx.x;
-        const int32_t o = (t < m) ? off[t] : -1;
+        const int32_t o = (t < r1) ? off[t] : -1;
         const int     b = (o >= 0) ? o / bin3 : -1;
         const unsigned peers = __match_any_sync(0xffffffffu, b);
-        if (b >= 0 && lane_id() == __ffs(peers) - 1) atomicAdd(count + b, (uint32_t) __popc(peers));
+        if (b >= 0 && lane_id() == __ffs(peers) - 1) atomicAdd(row + b, (uint32_t) __popc(peers));
     }
 }
 
-__global__ void bin_scatter_kernel(const int32_t *__restrict__ off, int64_t m, int bin3,
-                                   const uint32_t *__restrict__ start, uint32_t *__restrict__ cursor,
-                                   uint32_t *__restrict__ perm) {
-    for (int64_t t0 = (int64_t) blockIdx.x * blockDim.x; t0 < m; t0 += (int64_t) gridDim.x * blockDim.x) {
-        const int64_t t = t0 + threadIdx.x;
-        const int32_t o = (t < m) ? off[t] : -1;
+// tot[b] = sum_c count[c][b]
+__global__ void bin_total_kernel(const uint32_t *__restrict__ count, int64_t nchunks, int64_t nbins,
+                                 uint32_t *__restrict__ tot) {
+    for (int64_t b = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; b < nbins; b += (int64_t) gridDim.x * blockDim.x) {
+        uint32_t s = 0;
+        for (int64_t c = 0; c < nchunks; c++) s += count[c * nbins + b];
+        tot[b] = s;
+    }
+}
+
+// count[c][b] <- start[b] + sum_{c' < c} count[c'][b]: where chunk c's rows of bin b begin
+__global__ void bin_offsets_kernel(uint32_t *__restrict__ count, int64_t nchunks, int64_t nbins,
+                                   const uint32_t *__restrict__ start) {
+    for (int64_t b = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; b < nbins; b += (int64_t) gridDim.x * blockDim.x) {
+        uint32_t run = start[b];
+        for (int64_t c = 0; c < nchunks; c++) {
+            const uint32_t n = count[c * nbins + b];
+            count[c * nbins + b] = run;
+            run += n;
+        }
+    }
+}
+
+// one warp per chunk: its rows in order into their bins' lists (cursor row of
+// the chunk in shared memory when it fits, else in place in global memory)
+__global__ void __launch_bounds__(32) bin_chunk_scatter_kernel(const int32_t *__restrict__ off, int64_t m, int bin3,
+                                                               int64_t chunk, int64_t nbins,
+                                                               uint32_t *__restrict__ offs, uint32_t *__restrict__ perm,
+                                                               int use_smem) {
+    extern __shared__ uint32_t cur_s[];
+    const int64_t c = blockIdx.x;
+    const int64_t r0 = c * chunk, r1 = min(m, r0 + chunk);
+    uint32_t     *cur = use_smem ? cur_s : offs + c * nbins;
+    if (use_smem) {
+        for (int64_t b = lane_id(); b < nbins; b += 32) cur_s[b] = offs[c * nbins + b];
+        __syncwarp();
+    }
+    const unsigned below = (1u << lane_id()) - 1u;
+    for (int64_t t0 = r0; t0 < r1; t0 += 32) {
+        const int64_t t = t0 + lane_id();
+        const int32_t o = (t < r1) ? off[t] : -1;
         const int     b = (o >= 0) ? o / bin3 : -1;
         const unsigned peers = __match_any_sync(0xffffffffu, b);
         const int      leader = __ffs(peers) - 1;
         uint32_t       base = 0;
-        if (b >= 0 && lane_id() == leader) base = atomicAdd(cursor + b, (uint32_t) __popc(peers));
-        base = __shfl_sync(peers, base, leader);
-        if (b >= 0) {
-            const unsigned below = peers & ((1u << lane_id()) - 1u);
-            perm[start[b] + base + __popc(below)] = (uint32_t) t;
+        if (b >= 0 && lane_id() == leader) {
+            base = cur[b];
+            cur[b] = base + (uint32_t) __popc(peers);
         }
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (b >= 0) perm[base + __popc(peers & below)] = (uint32_t) t;
+        __syncwarp();
     }
 }
 
@@ -652,22 +698,47 @@ int mdp_build_bins(mdp_context *ctx, mdp_pointing *A, int bin_pix, mdp_pt_bins *
     const int64_t npix = A->n_map() / 3;
     const int     bin3 = 3 * bin_pix;
     const int64_t nb = (npix + bin_pix - 1) / bin_pix;
-    DevBuf        count, start, cursor;
     B->valid = 0;
-    MDP_TRY(count.alloc(4 * (nb + 1)));
+    if (A->m > 0xffffffffLL) {
+        mdp_set_error("P^T bins: %lld rows exceed 32-bit row indices", (long long) A->m);
+        return MDP_EUNSUPPORTED;
+    }
+    // row chunks: at least 2^20 rows, at most 2^26 (chunk, bin) counters
+    int64_t chunk = 1 << 20;
+    while (((A->m + chunk - 1) / chunk) * std::max<int64_t>(nb, 1) > (1LL << 26)) chunk <<= 1;
+    const int64_t nch = std::max<int64_t>((A->m + chunk - 1) / chunk, 1);
+    DevBuf        count, tot, start;
+    MDP_TRY(count.alloc(4 * (size_t) nch * std::max<int64_t>(nb, 1)));
+    MDP_TRY(tot.alloc(4 * (nb + 1)));
     MDP_TRY(start.alloc(4 * (nb + 1)));
-    MDP_TRY(cursor.alloc(4 * (nb + 1)));
-    MDP_CUDA(cudaMemsetAsync(count.p, 0, 4 * (nb + 1), ctx->stream));
-    MDP_CUDA(cudaMemsetAsync(cursor.p, 0, 4 * (nb + 1), ctx->stream));
-    const int g = grid_for(A->m, 256, ctx->sm_count * 16);
-    bin_count_kernel<<<g, 256, 0, ctx->stream>>>(A->off.as<int32_t>(), A->m, bin3, count.as<uint32_t>());
-    MDP_CHECK_LAUNCH(ctx);
+    MDP_CUDA(cudaMemsetAsync(count.p, 0, 4 * (size_t) nch * std::max<int64_t>(nb, 1), ctx->stream));
+    MDP_CUDA(cudaMemsetAsync(tot.p, 0, 4 * (nb + 1), ctx->stream));
+    if (nb > 0) {
+        bin_chunk_count_kernel<<<(unsigned) nch, 256, 0, ctx->stream>>>(A->off.as<int32_t>(), A->m, bin3, chunk, nb,
+                                                                       count.as<uint32_t>());
+        MDP_CHECK_LAUNCH(ctx);
+        bin_total_kernel<<<grid_for(nb, 256, 1024), 256, 0, ctx->stream>>>(count.as<uint32_t>(), nch, nb,
+                                                                           tot.as<uint32_t>());
+        MDP_CHECK_LAUNCH(ctx);
+    }
     uint32_t total = 0;
-    MDP_TRY(mdp_exclusive_scan_u32(ctx, count.as<uint32_t>(), start.as<uint32_t>(), nb + 1, &total));
+    MDP_TRY(mdp_exclusive_scan_u32(ctx, tot.as<uint32_t>(), start.as<uint32_t>(), nb + 1, &total));
     MDP_TRY(B->perm.alloc(4 * std::max<int64_t>(total, 1)));
-    bin_scatter_kernel<<<g, 256, 0, ctx->stream>>>(A->off.as<int32_t>(), A->m, bin3, start.as<uint32_t>(),
-                                                   cursor.as<uint32_t>(), B->perm.as<uint32_t>());
-    MDP_CHECK_LAUNCH(ctx);
+    if (nb > 0) {
+        bin_offsets_kernel<<<grid_for(nb, 256, 1024), 256, 0, ctx->stream>>>(count.as<uint32_t>(), nch, nb,
+                                                                             start.as<uint32_t>());
+        MDP_CHECK_LAUNCH(ctx);
+        int optin = 0;
+        MDP_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+        const size_t sm = 4 * (size_t) nb;
+        const int    use_smem = sm <= (size_t) optin ? 1 : 0;
+        if (use_smem)
+            MDP_CUDA(cudaFuncSetAttribute((const void *) bin_chunk_scatter_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm));
+        bin_chunk_scatter_kernel<<<(unsigned) nch, 32, use_smem ? sm : 0, ctx->stream>>>(
+                A->off.as<int32_t>(), A->m, bin3, chunk, nb, count.as<uint32_t>(), B->perm.as<uint32_t>(), use_smem);
+        MDP_CHECK_LAUNCH(ctx);
+    }
     std::vector<uint32_t> hs(nb + 1);
     MDP_CUDA(cudaMemcpyAsync(hs.data(), start.p, 4 * (nb + 1), cudaMemcpyDeviceToHost, ctx->stream));
     MDP_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -681,66 +752,72 @@ int mdp_build_bins(mdp_context *ctx, mdp_pointing *A, int bin_pix, mdp_pt_bins *
     return MDP_OK;
 }
 
-__global__ void __launch_bounds__(512) trmatvec_binned_kernel(const int32_t *__restrict__ off,
-                                                              const double *__restrict__ w,
-                                                              const double *__restrict__ y, double *__restrict__ x,
-                                                              const int64_t *__restrict__ bin_start,
-                                                              const uint32_t *__restrict__ perm, int64_t n_map) {
-    __shared__ double acc[3 * PT_BIN_PIX];
-    const int64_t bin = blockIdx.x / PT_SPLIT;
-    const int     part = blockIdx.x % PT_SPLIT;
-    for (int i = threadIdx.x; i < 3 * PT_BIN_PIX; i += blockDim.x) acc[i] = 0.0;
-    __syncthreads();
+// x = P^T y over the bins: warp k of a CTA owns bin PT_WARPS*blockIdx.x + k.
+// TY/TW: TOD and weight types (double, or float for the mixed solver's FP32
+// operator); products and sums in FP64.  U steps of 32 rows are loaded before
+// they are added, for memory-level parallelism.
+template <typename TY, typename TW>
+__global__ void __launch_bounds__(32 * PT_WARPS) trmatvec_bins_kernel(const int32_t *__restrict__ off,
+                                                                      const TW *__restrict__ w,
+                                                                      const TY *__restrict__ y, double *__restrict__ x,
+                                                                      const int64_t *__restrict__ bin_start,
+                                                                      const uint32_t *__restrict__ perm, int64_t nbins,
+                                                                      int64_t n_map) {
+    constexpr int U = 4;
+    __shared__ double acc_s[PT_WARPS][3 * PT_BIN_PIX];
+    const int     wid = threadIdx.x >> 5, lane = lane_id();
+    const int64_t bin = (int64_t) blockIdx.x * PT_WARPS + wid;
+    if (bin >= nbins) return;  // whole warps only; no CTA-wide barrier follows
+    double *acc = acc_s[wid];
+    for (int i = lane; i < 3 * PT_BIN_PIX; i += 32) acc[i] = 0.0;
+    __syncwarp();
     const int64_t s0 = bin_start[bin], s1 = bin_start[bin + 1];
-    const int64_t len = s1 - s0;
-    const int64_t a = s0 + len * part / PT_SPLIT, b = s0 + len * (part + 1) / PT_SPLIT;
     const int64_t base = bin * 3 * PT_BIN_PIX;
-    for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) {
-        const int64_t t = perm[i];
-        const int     o = (int) (off[t] - base);
-        const double  v = y[t];
-        atomicAdd(acc + o, w[3 * t] * v);
-        atomicAdd(acc + o + 1, w[3 * t + 1] * v);
-        atomicAdd(acc + o + 2, w[3 * t + 2] * v);
+    for (int64_t i0 = s0; i0 < s1; i0 += 32 * U) {
+        int    o[U];
+        double c0[U], c1[U], c2[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int64_t i = i0 + 32 * u + lane;
+            o[u] = -1;
+            c0[u] = c1[u] = c2[u] = 0.0;
+            if (i < s1) {
+                const int64_t t = perm[i];
+                const double  v = (double) y[t];
+                o[u] = (int) (off[t] - base);
+                c0[u] = (double) w[3 * t] * v;
+                c1[u] = (double) w[3 * t + 1] * v;
+                c2[u] = (double) w[3 * t + 2] * v;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const unsigned peers = __match_any_sync(0xffffffffu, o[u]);
+            const bool     alone = o[u] < 0 || peers == (1u << lane);
+            if (__all_sync(0xffffffffu, alone)) {
+                if (o[u] >= 0) {  // distinct pixels: one add per entry
+                    acc[o[u]] += c0[u];
+                    acc[o[u] + 1] += c1[u];
+                    acc[o[u] + 2] += c2[u];
+                }
+            } else {
+                for (int src = 0; src < 32; src++) {  // rows in lane order
+                    const int    oo = __shfl_sync(0xffffffffu, o[u], src);
+                    const double d0 = __shfl_sync(0xffffffffu, c0[u], src);
+                    const double d1 = __shfl_sync(0xffffffffu, c1[u], src);
+                    const double d2 = __shfl_sync(0xffffffffu, c2[u], src);
+                    if (lane == 0 && oo >= 0) {
+                        acc[oo] += d0;
+                        acc[oo + 1] += d1;
+                        acc[oo + 2] += d2;
+                    }
+                }
+            }
+            __syncwarp();
+        }
     }
-    __syncthreads();
     const int64_t lim = min((int64_t) 3 * PT_BIN_PIX, n_map - base);
-    for (int i = threadIdx.x; i < lim; i += blockDim.x) {
-        const double v = acc[i];
-        if (v != 0.0) atomicAdd(x + base + i, v);
-    }
-}
-
-// FP32 P^T by map bins for the mixed-precision operator: FP32 TOD and weights
-// in, products and sums in FP64 (shared memory), FP64 map out.
-__global__ void __launch_bounds__(512) trmatvec32_binned_kernel(const int32_t *__restrict__ off,
-                                                                const float *__restrict__ w,
-                                                                const float *__restrict__ y, double *__restrict__ x,
-                                                                const int64_t *__restrict__ bin_start,
-                                                                const uint32_t *__restrict__ perm, int64_t n_map) {
-    __shared__ double acc[3 * PT_BIN_PIX];
-    const int64_t bin = blockIdx.x / PT_SPLIT;
-    const int     part = blockIdx.x % PT_SPLIT;
-    for (int i = threadIdx.x; i < 3 * PT_BIN_PIX; i += blockDim.x) acc[i] = 0.0;
-    __syncthreads();
-    const int64_t s0 = bin_start[bin], s1 = bin_start[bin + 1];
-    const int64_t len = s1 - s0;
-    const int64_t a = s0 + len * part / PT_SPLIT, b = s0 + len * (part + 1) / PT_SPLIT;
-    const int64_t base = bin * 3 * PT_BIN_PIX;
-    for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) {
-        const int64_t t = perm[i];
-        const int     o = (int) (off[t] - base);
-        const double  v = (double) y[t];
-        atomicAdd(acc + o, (double) w[3 * t] * v);
-        atomicAdd(acc + o + 1, (double) w[3 * t + 1] * v);
-        atomicAdd(acc + o + 2, (double) w[3 * t + 2] * v);
-    }
-    __syncthreads();
-    const int64_t lim = min((int64_t) 3 * PT_BIN_PIX, n_map - base);
-    for (int i = threadIdx.x; i < lim; i += blockDim.x) {
-        const double v = acc[i];
-        if (v != 0.0) atomicAdd(x + base + i, v);
-    }
+    for (int i = lane; i < lim; i += 32) x[base + i] = acc[i];
 }
 
 __global__ void trmatvec32_kernel(const int32_t *__restrict__ off, const float *__restrict__ w,
@@ -773,28 +850,27 @@ int mdp_pointing_prepare_fp32(mdp_context *ctx, mdp_pointing *A) {
     return MDP_OK;
 }
 
-static bool use_bins(const mdp_pointing *A) {
-    static int env = -1;
-    if (env < 0) {
-        const char *e = getenv("MDP_PT_BINNED");
-        env = e ? atoi(e) : 1;
-    }
-    return env != 0 && A->triplet && A->m >= (1 << 20);
+static bool use_bins(const mdp_pointing *A) { return A->triplet && A->m >= (1 << 20); }
+bool mdp_pointing_binned(const mdp_pointing *A) { return use_bins(A); }
+int  mdp_pointing_bins(mdp_context *ctx, mdp_pointing *A) {
+    if (!A->bins.valid || A->bins.bin_pix != PT_BIN_PIX) MDP_TRY(mdp_build_bins(ctx, A, PT_BIN_PIX, &A->bins));
+    return MDP_OK;
 }
 
 int mdp_trmatvec_launch(mdp_context *ctx, const mdp_pointing *A, const double *d_y, double *d_x) {
-    MDP_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * A->n_map(), ctx->stream));
     if (use_bins(A)) {
         mdp_pointing *Am = const_cast<mdp_pointing *>(A);  // the bin list is a cache of the pointing
-        if (!Am->bins.valid) MDP_TRY(mdp_build_bins(ctx, Am, PT_BIN_PIX, &Am->bins));
-        if (A->bins.nbins > 0) {
-            trmatvec_binned_kernel<<<(unsigned) (A->bins.nbins * PT_SPLIT), 512, 0, ctx->stream>>>(
+        if (!Am->bins.valid || Am->bins.bin_pix != PT_BIN_PIX) MDP_TRY(mdp_build_bins(ctx, Am, PT_BIN_PIX, &Am->bins));
+        if (A->bins.nbins > 0) {  // every map entry is written by its bin's warp
+            trmatvec_bins_kernel<double, double><<<(unsigned) ((A->bins.nbins + PT_WARPS - 1) / PT_WARPS), 32 * PT_WARPS,
+                                                   0, ctx->stream>>>(
                     A->off.as<int32_t>(), A->values, d_y, d_x, A->bins.start.as<int64_t>(), A->bins.perm.as<uint32_t>(),
-                    A->n_map());
+                    A->bins.nbins, A->n_map());
             MDP_CHECK_LAUNCH(ctx);
         }
         return MDP_OK;
     }
+    MDP_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * A->n_map(), ctx->stream));
     if (A->triplet && !aligned16(A->values, d_y)) {
         trmatvec_triplet_scalar_kernel<<<grid_for(A->m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
                 A->off.as<int32_t>(), A->values, d_y, d_x, A->m);
@@ -818,17 +894,18 @@ extern "C" int mdp_trmatvec(mdp_context *ctx, const mdp_pointing *A, const doubl
 // x (FP64, n_map) = P^T y (FP32 TOD) with the FP32 weights
 int mdp_trmatvec32_launch(mdp_context *ctx, mdp_pointing *A, const float *d_y, double *d_x) {
     MDP_TRY(mdp_pointing_prepare_fp32(ctx, A));
-    MDP_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * A->n_map(), ctx->stream));
     if (use_bins(A)) {
-        if (!A->bins.valid) MDP_TRY(mdp_build_bins(ctx, A, PT_BIN_PIX, &A->bins));
+        if (!A->bins.valid || A->bins.bin_pix != PT_BIN_PIX) MDP_TRY(mdp_build_bins(ctx, A, PT_BIN_PIX, &A->bins));
         if (A->bins.nbins > 0) {
-            trmatvec32_binned_kernel<<<(unsigned) (A->bins.nbins * PT_SPLIT), 512, 0, ctx->stream>>>(
+            trmatvec_bins_kernel<float, float><<<(unsigned) ((A->bins.nbins + PT_WARPS - 1) / PT_WARPS), 32 * PT_WARPS,
+                                                 0, ctx->stream>>>(
                     A->off.as<int32_t>(), A->w32.as<float>(), d_y, d_x, A->bins.start.as<int64_t>(),
-                    A->bins.perm.as<uint32_t>(), A->n_map());
+                    A->bins.perm.as<uint32_t>(), A->bins.nbins, A->n_map());
             MDP_CHECK_LAUNCH(ctx);
         }
         return MDP_OK;
     }
+    MDP_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * A->n_map(), ctx->stream));
     trmatvec32_kernel<<<grid_for(A->m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(
             A->off.as<int32_t>(), A->w32.as<float>(), d_y, d_x, A->m);
     MDP_CHECK_LAUNCH(ctx);

@@ -9,8 +9,9 @@
 // Device layout: map-domain vectors are contiguous FP64 arrays of n = 3*npix
 // unknowns; the 3x3 blocks are row-major [npix][9].  Dot products are
 // deterministic two-level reductions (fixed grid, partials summed in block
-// order by the last block to finish), so a solve is bitwise reproducible
-// except for the FP64 atomics of P^T.
+// order by the last block to finish); P^T and the block-Jacobi blocks add
+// their terms in a fixed order too (map bins, below and in pointing.cu), so a
+// solve on pointings of 2^20 rows or more is bitwise reproducible.
 #include <cfloat>
 #include <chrono>
 #include <cmath>
@@ -57,6 +58,105 @@ __global__ void localW_kernel(const int32_t *__restrict__ off, const double *__r
         atomicAdd(Wq + 8, a22);
         atomicAdd(hits + o / 3, 1);
     }
+}
+
+// The same sums over the P^T map bins (pointing.cu): warp k of a CTA owns bin
+// LW_WARPS*blockIdx.x + k and adds, in the bin's time-ordered row list, each
+// row's six products and its hit into shared-memory accumulators; rows of one
+// step on one pixel are added in lane order.  Every pixel's sums run in time
+// order, as getlocalW's loop over the rows does (precond.c:42-161), and are
+// reproducible bit for bit.
+#define LW_WARPS 3
+__global__ void __launch_bounds__(32 * LW_WARPS) localW_bins_kernel(
+        const int32_t *__restrict__ off, const double *__restrict__ w, const int64_t *__restrict__ bin_start,
+        const uint32_t *__restrict__ perm, int64_t nbins, int64_t npix, const int64_t *__restrict__ bstart,
+        const int32_t *__restrict__ blen, const double *__restrict__ t0, int nb, double *__restrict__ W,
+        int *__restrict__ hits) {
+    constexpr int BP = MDP_PT_BIN_PIX;
+    __shared__ double acc_s[LW_WARPS][BP * 7];  // per pixel: W00 W01 W02 W11 W12 W22 hits
+    const int     wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t bin = (int64_t) blockIdx.x * LW_WARPS + wid;
+    if (bin >= nbins) return;  // whole warps only; no CTA-wide barrier follows
+    double *acc = acc_s[wid];
+    for (int i = lane; i < BP * 7; i += 32) acc[i] = 0.0;
+    __syncwarp();
+    const int64_t s0 = bin_start[bin], s1 = bin_start[bin + 1];
+    const int64_t base = bin * 3 * BP;
+    for (int64_t i0 = s0; i0 < s1; i0 += 32) {
+        const int64_t i = i0 + lane;
+        int           q = -1;
+        double        a[6] = {0, 0, 0, 0, 0, 0};
+        if (i < s1) {
+            const int64_t t = perm[i];
+            q = (int) ((off[t] - base) / 3);
+            const int    b = find_block(bstart, blen, nb, t);
+            const double d = (b >= 0) ? t0[b] : 1.0;
+            const double w0 = w[3 * t], w1 = w[3 * t + 1], w2 = w[3 * t + 2];
+            a[0] = __dmul_rn(__dmul_rn(w0, w0), d);
+            a[1] = __dmul_rn(__dmul_rn(w0, w1), d);
+            a[2] = __dmul_rn(__dmul_rn(w0, w2), d);
+            a[3] = __dmul_rn(__dmul_rn(w1, w1), d);
+            a[4] = __dmul_rn(__dmul_rn(w1, w2), d);
+            a[5] = __dmul_rn(__dmul_rn(w2, w2), d);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, q);
+        const bool     alone = q < 0 || peers == (1u << lane);
+        if (__all_sync(0xffffffffu, alone)) {
+            if (q >= 0) {
+#pragma unroll
+                for (int k = 0; k < 6; k++) acc[7 * q + k] = __dadd_rn(acc[7 * q + k], a[k]);
+                acc[7 * q + 6] += 1.0;
+            }
+        } else {
+            for (int src = 0; src < 32; src++) {  // rows in lane order
+                const int qq = __shfl_sync(0xffffffffu, q, src);
+                double    d[6];
+#pragma unroll
+                for (int k = 0; k < 6; k++) d[k] = __shfl_sync(0xffffffffu, a[k], src);
+                if (lane == 0 && qq >= 0) {
+#pragma unroll
+                    for (int k = 0; k < 6; k++) acc[7 * qq + k] = __dadd_rn(acc[7 * qq + k], d[k]);
+                    acc[7 * qq + 6] += 1.0;
+                }
+            }
+        }
+        __syncwarp();
+    }
+    const int64_t p0 = bin * BP;
+    const int     np = (int) min((int64_t) BP, npix - p0);
+    for (int j = lane; j < np; j += 32) {
+        double *Wq = W + 9 * (p0 + j);
+        const double *s = acc + 7 * j;
+        Wq[0] = s[0];
+        Wq[1] = s[1];
+        Wq[2] = s[2];
+        Wq[3] = 0.0;
+        Wq[4] = s[3];
+        Wq[5] = s[4];
+        Wq[6] = 0.0;
+        Wq[7] = 0.0;
+        Wq[8] = s[5];
+        hits[p0 + j] = (int) s[6];
+    }
+}
+
+// W and hits of every pixel: by map bins (time order) when the pointing has
+// them, else with atomics
+static int localW_launch(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, double *d_W, int *d_hits) {
+    cudaStream_t  st = ctx->stream;
+    const int64_t npix = A->n_map() / 3;
+    if (mdp_pointing_binned(A)) {
+        MDP_TRY(mdp_pointing_bins(ctx, A));
+        if (A->bins.nbins > 0)
+            localW_bins_kernel<<<(unsigned) ((A->bins.nbins + LW_WARPS - 1) / LW_WARPS), 32 * LW_WARPS, 0, st>>>(
+                    A->off.as<int32_t>(), A->values, A->bins.start.as<int64_t>(), A->bins.perm.as<uint32_t>(),
+                    A->bins.nbins, npix, N->blk_start.as<int64_t>(), N->blk_len.as<int32_t>(), N->blk_t0.as<double>(),
+                    N->nb, d_W, d_hits);
+        MDP_CHECK_LAUNCH(ctx);
+        return MDP_OK;
+    }
+    MDP_TRY(localW_launch(ctx, A, N, d_W, d_hits));
+    return MDP_OK;
 }
 
 // ================================================================= 3x3 LAPACK restatement
@@ -630,13 +730,8 @@ int mdp_bj_build(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, BJState 
     if ((rc = W.alloc(72 * npix0)) || (rc = inv.alloc(72 * npix0)) || (rc = rcond.alloc(8 * npix0)) ||
         (rc = cut.alloc(4 * npix0)) || (rc = hits.alloc(4 * npix0)) || (rc = ncut.alloc(4)))
         return rc;
-    MDP_CUDA(cudaMemsetAsync(W.p, 0, 72 * npix0, st));
-    MDP_CUDA(cudaMemsetAsync(hits.p, 0, 4 * npix0, st));
     MDP_CUDA(cudaMemsetAsync(ncut.p, 0, 4, st));
-    localW_kernel<<<grid_for(m, 256, ctx->sm_count * 16), 256, 0, st>>>(
-            A->off.as<int32_t>(), A->values, m, N->blk_start.as<int64_t>(), N->blk_len.as<int32_t>(),
-            N->blk_t0.as<double>(), N->nb, W.as<double>(), hits.as<int>());
-    MDP_CHECK_LAUNCH(ctx);
+    MDP_TRY(localW_launch(ctx, A, N, W.as<double>(), hits.as<int>()));
     bj_pixel_kernel<<<grid_for(npix0, 128, ctx->sm_count * 8), 128, 0, st>>>(W.as<double>(), npix0, inv.as<double>(),
                                                                             rcond.as<double>(), cut.as<int>(),
                                                                             ncut.as<int>());
@@ -1100,12 +1195,7 @@ extern "C" int mdp_local_blocks(mdp_context *ctx, mdp_pointing *A, const mdp_noi
     MDP_CUDA(cudaSetDevice(ctx->device));
     const int64_t npix = A->n_map() / 3;
     cudaStream_t  st = ctx->stream;
-    MDP_CUDA(cudaMemsetAsync(d_W, 0, 72 * npix, st));
-    MDP_CUDA(cudaMemsetAsync(d_hits, 0, 4 * npix, st));
-    localW_kernel<<<grid_for(A->m, 256, ctx->sm_count * 16), 256, 0, st>>>(
-            A->off.as<int32_t>(), A->values, A->m, N->blk_start.as<int64_t>(), N->blk_len.as<int32_t>(),
-            N->blk_t0.as<double>(), N->nb, d_W, d_hits);
-    MDP_CHECK_LAUNCH(ctx);
+    MDP_TRY(localW_launch(ctx, A, N, d_W, d_hits));
     return MDP_OK;
 }
 

@@ -839,6 +839,39 @@ __global__ void spectrum_kernel(const double *__restrict__ T, int lambda, int N,
     }
 }
 
+int mdp_spectrum_H(mdp_context *ctx, const double *h_T, int lambda, int Nn, const double2 *d_tw, double *d_H) {
+    DevBuf dT;
+    MDP_TRY(dT.alloc(sizeof(double) * lambda));
+    MDP_CUDA(cudaMemcpyAsync(dT.p, h_T, sizeof(double) * lambda, cudaMemcpyHostToDevice, ctx->stream));
+    spectrum_kernel<<<grid_for(Nn / 2 + 1, 128, 4096), 128, 0, ctx->stream>>>(dT.as<double>(), lambda, Nn, d_tw, d_H);
+    MDP_CHECK_LAUNCH(ctx);
+    MDP_CUDA(cudaStreamSynchronize(ctx->stream));  // dT is released on return
+    return MDP_OK;
+}
+
+// Spectrum of the circulant embedding exactly as the reference builds it
+// (circ_init_fftw, toeplitz.c:441-470: c[0] = T[0], then for i = 1..lambda-1
+// c[i] = T[i] and c[bs-i] = T[i], later writes winning), for any bs:
+// F[k] = sum_j c[j] exp(-2 pi i j k / bs), k = 0..bs/2, summed over the nonzero
+// entries only (Kahan-compensated FP64), twiddles exp(-2 pi i e / bs), e < bs,
+// from long double on the host.
+__global__ void circ_spectrum_kernel(const int32_t *__restrict__ jidx, const double *__restrict__ cval, int nnz,
+                                     int bs, const double2 *__restrict__ tw, double2 *__restrict__ F) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= bs / 2; k += gridDim.x * blockDim.x) {
+        double re = 0.0, im = 0.0, cre = 0.0, cim = 0.0;
+        for (int t = 0; t < nnz; t++) {
+            const double2 w = tw[((int64_t) jidx[t] * k) % bs];
+            const double  yr = cval[t] * w.x - cre, yi = cval[t] * w.y - cim;
+            const double  tr = re + yr, ti = im + yi;
+            cre = (tr - re) - yr;
+            cim = (ti - im) - yi;
+            re = tr;
+            im = ti;
+        }
+        F[k] = make_double2(re, im);
+    }
+}
+
 // Twist table of one spectrum in tile position order (see TileArgsT); the
 // halves are formed in the tile's precision T from H rounded to T.
 template <typename T>
@@ -878,6 +911,43 @@ static inline void host_cexp(long double num, long double den, double2 *o) {
 static inline void host_cexp(long double num, long double den, float2 *o) {
     const long double ang = -2.0L * 3.14159265358979323846264338327950288L * num / den;
     *o = make_float2((float) cosl(ang), (float) sinl(ang));
+}
+
+int mdp_circulant_spectrum(mdp_context *ctx, const double *h_T, int lambda, int bs, double *h_F) {
+    if (bs < 1 || lambda < 1 || !h_T || !h_F) return MDP_EINVAL;
+    std::vector<double> c(bs, 0.0);
+    c[0] = h_T[0];
+    for (int i = 1; i < lambda; i++) {
+        if (i < bs) c[i] = h_T[i];
+        if (bs - i >= 0 && bs - i < bs) c[bs - i] = h_T[i];
+    }
+    std::vector<int32_t> jn;
+    std::vector<double>  cn;
+    for (int j = 0; j < bs; j++)
+        if (c[j] != 0.0) {
+            jn.push_back(j);
+            cn.push_back(c[j]);
+        }
+    std::vector<double2> tw(bs);
+    for (int e = 0; e < bs; e++) host_cexp(e, bs, &tw[e]);
+    const int nf = bs / 2 + 1;
+    DevBuf    dj, dc, dt, dF;
+    MDP_TRY(dj.alloc(4 * std::max<size_t>(jn.size(), 1)));
+    MDP_TRY(dc.alloc(8 * std::max<size_t>(cn.size(), 1)));
+    MDP_TRY(dt.alloc(sizeof(double2) * bs));
+    MDP_TRY(dF.alloc(sizeof(double2) * nf));
+    if (!jn.empty()) {
+        MDP_CUDA(cudaMemcpyAsync(dj.p, jn.data(), 4 * jn.size(), cudaMemcpyHostToDevice, ctx->stream));
+        MDP_CUDA(cudaMemcpyAsync(dc.p, cn.data(), 8 * cn.size(), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    MDP_CUDA(cudaMemcpyAsync(dt.p, tw.data(), sizeof(double2) * bs, cudaMemcpyHostToDevice, ctx->stream));
+    circ_spectrum_kernel<<<grid_for(nf, 128, 4096), 128, 0, ctx->stream>>>(dj.as<int32_t>(), dc.as<double>(),
+                                                                         (int) jn.size(), bs, dt.as<double2>(),
+                                                                         dF.as<double2>());
+    MDP_CHECK_LAUNCH(ctx);
+    MDP_CUDA(cudaMemcpyAsync(h_F, dF.p, sizeof(double2) * nf, cudaMemcpyDeviceToHost, ctx->stream));
+    MDP_CUDA(cudaStreamSynchronize(ctx->stream));
+    return MDP_OK;
 }
 
 // Twiddle tables of a tile plan (ML = 2^log_ml points per CTA, C CTAs, M = C*ML,
@@ -1005,11 +1075,16 @@ template <> struct SplitShape<double> { static constexpr int CW = 16, RP = 2, M1
 struct TileCand {
     int log_ml, C, threads;
     int split = 0, log_m1 = 0, log_m2 = 0;  // split plan: M = 2^log_m1 * 2^log_m2
+                                            // (split 2: cluster four-step, M = 2C x 4096)
 };
 
 static int64_t cand_N(const TileCand &c) {
+    if (c.split == 2) return 2LL * (2 * c.C) * 4096;
     return c.split ? (2LL << (c.log_m1 + c.log_m2)) : 2LL * c.C * (1LL << c.log_ml);
 }
+// the split plans (1 and 2) keep one output fewer than the band allows, so that
+// every window starts on an even row
+static int64_t cand_E(const TileCand &c, int lambda) { return cand_N(c) - 2LL * (lambda - 1) - (c.split ? 1 : 0); }
 
 // split plans: columns of 16 <= M1 <= 2^m1max points, rows of 32 <= M2 <= 512
 // points; shapes whose transforms end in a lone radix-2 pass (5 or 9 bits) are
@@ -1033,6 +1108,10 @@ static int ceil_log2_i(int64_t v) {
     return b;
 }
 
+// The cluster four-step tiles join the automatic choice once validated; until
+// then they are reached through mdp_noise_set_plan only.
+static const bool g_cluster4_auto = false;
+
 // every launchable configuration whose tile holds the band (E >= 1)
 template <typename T>
 static std::vector<TileCand> tile_candidates(int lambda) {
@@ -1049,7 +1128,13 @@ static std::vector<TileCand> tile_candidates(int lambda) {
     for (int logM = 9; logM <= 17; logM++)
         for (auto ab : split_shapes(logM, SplitShape<T>::M1MAX)) {
             TileCand c{0, 0, 0, 1, ab.first, ab.second};
-            if (cand_N(c) - 2LL * (lambda - 1) - 1 < 1) continue;
+            if (cand_E(c, lambda) < 1) continue;
+            out.push_back(c);
+        }
+    if (g_cluster4_auto)
+        for (int C = 2; C <= 8; C <<= 1) {  // cluster four-step tiles of 2C x 4096 points
+            TileCand c{13, C, 256, 2, 0, 12};
+            if (cand_E(c, lambda) < 1) continue;
             out.push_back(c);
         }
     return out;
@@ -1063,7 +1148,9 @@ static double tile_model_cost(const TileCand &c, int lambda, int64_t max_block) 
     const int     logN = ceil_log2_i(N);
     const double  eff = (double) std::min<int64_t>(E, std::max<int64_t>(max_block, 1));
     double        cost = (double) N / eff * (logN + 3);
-    if (c.split) {
+    if (c.split == 2) {
+        cost *= 0.6;  // the tile stays on chip; paired-lane arithmetic
+    } else if (c.split) {
         cost *= 1.3;  // scratch round trips; the timed choice decides
     } else {
         if (c.C > 1) cost += 3.0 * std::log2((double) c.C);
@@ -1168,37 +1255,42 @@ static int tune_plan(mdp_context *ctx, const mdp_noise *N, const std::vector<Til
     return rc;
 }
 
-// MDP_TOEPLITZ_PLAN[32]="log2_ml,cluster,threads" (one-kernel tiles) or
-// "s,log_m1,log_m2" (split tiles) forces a plan;
-// MDP_TOEPLITZ_FFT[32]=N restricts the choice to tiles of N real samples (cost
-// model only); MDP_TOEPLITZ_TUNE=0 switches the autotuner off.
+// A plan given by name (mdp_noise_set_plan): "log2_ml,cluster,threads"
+// (one-kernel tiles), "s,log_m1,log_m2" (split tiles) or "c,cluster" (cluster
+// four-step tiles).
 template <typename T>
-static int choose_plan(mdp_context *ctx, const mdp_noise *N, TileCand *out, int *tuned) {
-    const bool  f32 = sizeof(T) == 4;
-    const char *plan = getenv(f32 ? "MDP_TOEPLITZ_PLAN32" : "MDP_TOEPLITZ_PLAN");
-    const char *fft = getenv(f32 ? "MDP_TOEPLITZ_FFT32" : "MDP_TOEPLITZ_FFT");
-    const char *tune = getenv("MDP_TOEPLITZ_TUNE");
+static int parse_plan(const char *plan, int lambda, TileCand *out) {
+    TileCand c{0, 0, 0};
+    bool     ok;
+    if (plan[0] == 's') {
+        c.split = 1;
+        ok = sscanf(plan + 1, ",%d,%d", &c.log_m1, &c.log_m2) == 2 && c.log_m1 >= 4 &&
+             c.log_m1 <= SplitShape<T>::M1MAX && c.log_m2 >= 5 && c.log_m2 <= 9;
+    } else if (plan[0] == 'c') {
+        c = TileCand{13, 0, 256, 2, 0, 12};
+        ok = sscanf(plan + 1, ",%d", &c.C) == 1 && (c.C == 2 || c.C == 4 || c.C == 8);
+    } else {
+        ok = sscanf(plan, "%d,%d,%d", &c.log_ml, &c.C, &c.threads) == 3 && pick_kernel<T>(c.log_ml, c.C) &&
+             c.threads >= 32 && c.threads <= 512 && !(c.threads & 31);
+    }
+    if (!ok || cand_E(c, lambda) < 1) {
+        mdp_set_error("invalid tile plan '%s' for lambda=%d", plan, lambda);
+        return MDP_EINVAL;
+    }
+    *out = c;
+    return MDP_OK;
+}
+
+// The plan of a precision: the cheapest candidate by the cost model, or
+// (tune) the fastest of the screened candidates timed on the device, cached
+// per key for the process.  forced > 0 keeps the one-kernel tiles of forced
+// real samples only (cost model).
+template <typename T>
+static int choose_plan(mdp_context *ctx, const mdp_noise *N, TileCand *out, int *tuned, bool tune = true,
+                       int64_t forced = 0) {
+    const bool f32 = sizeof(T) == 4;
     *tuned = 0;
     std::vector<TileCand> cands = tile_candidates<T>(N->lambda);
-    if (plan) {
-        TileCand c{0, 0, 0};
-        bool     ok;
-        if (plan[0] == 's') {  // "s,log_m1,log_m2": split plan
-            c.split = 1;
-            ok = sscanf(plan + 1, ",%d,%d", &c.log_m1, &c.log_m2) == 2 && c.log_m1 >= 4 &&
-                 c.log_m1 <= SplitShape<T>::M1MAX && c.log_m2 >= 5 && c.log_m2 <= 9;
-        } else {
-            ok = sscanf(plan, "%d,%d,%d", &c.log_ml, &c.C, &c.threads) == 3 && pick_kernel<T>(c.log_ml, c.C) &&
-                 c.threads >= 32 && c.threads <= 512 && !(c.threads & 31);
-        }
-        if (!ok || cand_N(c) - 2LL * (N->lambda - 1) < 1) {
-            mdp_set_error("invalid tile plan '%s' for lambda=%d", plan, N->lambda);
-            return MDP_EINVAL;
-        }
-        *out = c;
-        return MDP_OK;
-    }
-    const int forced = fft ? atoi(fft) : 0;
     if (forced) {
         std::vector<TileCand> keep;
         for (const TileCand &c : cands)
@@ -1210,11 +1302,11 @@ static int choose_plan(mdp_context *ctx, const mdp_noise *N, TileCand *out, int 
         return tile_model_cost(a, N->lambda, N->max_block) < tile_model_cost(b, N->lambda, N->max_block);
     });
     *out = cands[0];
-    if (forced || (tune && atoi(tune) == 0) || cands.size() == 1) return MDP_OK;
+    if (forced || !tune || cands.size() == 1) return MDP_OK;
     // screen: tiles at least a quarter useful and not longer than twice the block plus the halo
     std::vector<TileCand> screen;
     for (const TileCand &c : cands) {
-        const int64_t Nn = cand_N(c), E = Nn - 2LL * (N->lambda - 1);
+        const int64_t Nn = cand_N(c), E = cand_E(c, N->lambda);
         if (E * 4 >= Nn && E <= 2 * std::max<int64_t>(N->max_block, 1) + 2LL * N->lambda) screen.push_back(c);
     }
     if (screen.size() <= 1) return MDP_OK;
@@ -1224,7 +1316,7 @@ static int choose_plan(mdp_context *ctx, const mdp_noise *N, TileCand *out, int 
     auto                        it = g_tuned.find(key);
     if (it != g_tuned.end()) {
         const TileCand &c = it->second;
-        if (cand_N(c) - 2LL * (N->lambda - 1) >= 1) {
+        if (cand_E(c, N->lambda) >= 1) {
             *out = c;
             *tuned = 1;
             return MDP_OK;
@@ -1436,7 +1528,7 @@ static int build_plan(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, const Ti
     const int M = (int) (cand_N(c) / 2);
     P.fft_n = 2 * M;
     // split tiles: one output fewer, so that every window can start on an even row
-    const int64_t        E = (int64_t) P.fft_n - 2LL * (N->lambda - 1) - (c.split ? 1 : 0);
+    const int64_t        E = cand_E(c, N->lambda);
     if (E < 1) return MDP_EUNSUPPORTED;
     std::vector<int64_t> ts;
     std::vector<int32_t> tb;
@@ -1455,6 +1547,11 @@ static int build_plan(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, const Ti
     if (!ts.empty()) {
         MDP_CUDA(cudaMemcpy(P.tile_start.p, ts.data(), 8 * ts.size(), cudaMemcpyHostToDevice));
         MDP_CUDA(cudaMemcpy(P.tile_block.p, tb.data(), 4 * tb.size(), cudaMemcpyHostToDevice));
+    }
+    if (c.split == 2) {
+        MDP_TRY(ninv4_build<T>(ctx, N, P, spectra));
+        P.ready = 1;
+        return MDP_OK;
     }
     if (c.split) {
         P.cluster = 0;
@@ -1506,6 +1603,7 @@ static int launch_tiles(mdp_context *ctx, const mdp_noise *N, const mdp_tile_pla
     using V = typename CT<T>::V;
     if (P.n_tiles == 0 || ncols < 1) return MDP_OK;
     if (ncols > 65535) return MDP_EUNSUPPORTED;
+    if (P.split == 2) return ninv4_launch<T>(ctx, N, P, d_in, d_out, d_means, ncols, col_stride, d_active);
     if (P.split) return launch_split<T>(ctx, N, P, d_in, d_out, d_means, ncols, col_stride, d_active);
     TileArgsT<T> a;
     a.vin = d_in;
@@ -1940,6 +2038,38 @@ int mdp_matvec32_blockmeans(mdp_context *ctx, const mdp_pointing *A, const mdp_n
     return MDP_OK;
 }
 
+extern "C" int mdp_noise_set_plan(mdp_context *ctx, mdp_noise *N, int fp32, const char *plan) {
+    if (!ctx || !N || !plan) {
+        mdp_set_error("mdp_noise_set_plan: invalid arguments");
+        return MDP_EINVAL;
+    }
+    MDP_CUDA(cudaSetDevice(ctx->device));
+    if (N->lambda == 1) return MDP_OK;  // white noise: no tiles
+    mdp_tile_plan &P = fp32 ? N->p32 : N->p64;
+    TileCand       c;
+    int            tuned = 0;
+    if (!strcmp(plan, "auto") || !strcmp(plan, "model")) {
+        MDP_TRY(fp32 ? choose_plan<float>(ctx, N, &c, &tuned, plan[0] == 'a')
+                     : choose_plan<double>(ctx, N, &c, &tuned, plan[0] == 'a'));
+    } else if (!strncmp(plan, "fft:", 4)) {
+        const int64_t n = atoll(plan + 4);
+        const int     rc = fp32 ? choose_plan<float>(ctx, N, &c, &tuned, false, n)
+                                : choose_plan<double>(ctx, N, &c, &tuned, false, n);
+        if (rc) {
+            mdp_set_error("mdp_noise_set_plan: no one-kernel tile of %lld samples holds lambda=%d", (long long) n,
+                          N->lambda);
+            return rc;
+        }
+    } else {
+        MDP_TRY(fp32 ? parse_plan<float>(plan, N->lambda, &c) : parse_plan<double>(plan, N->lambda, &c));
+    }
+    MDP_CUDA(cudaStreamSynchronize(ctx->stream));  // no launch of the old plan is in flight
+    P.reset();
+    const int rc = fp32 ? build_plan<float>(ctx, N, P, c, true) : build_plan<double>(ctx, N, P, c, true);
+    P.tuned = tuned;
+    return rc;
+}
+
 extern "C" int mdp_noise_tile_fp32(mdp_context *ctx, mdp_noise *N, int *fft_size, int *cluster_ctas,
                                    int64_t *n_tiles) {
     if (!ctx || !N) return MDP_EINVAL;
@@ -1970,7 +2100,7 @@ extern "C" int mdp_noise_plan(mdp_context *ctx, mdp_noise *N, int fp32, int *log
     if (cluster_ctas) *cluster_ctas = P.cluster;
     if (threads) *threads = P.threads;
     if (tuned) *tuned = P.tuned;
-    if (split_log_m1) *split_log_m1 = P.split ? P.log_m1 : 0;
+    if (split_log_m1) *split_log_m1 = P.split ? (P.split == 2 ? 1 + (P.cluster == 8 ? 3 : P.cluster == 4 ? 2 : 1) : P.log_m1) : 0;
     if (split_log_m2) *split_log_m2 = P.split ? P.log_m2 : 0;
     return MDP_OK;
 }
@@ -2015,7 +2145,9 @@ static double    *g_noalloc_ptr[64] = {nullptr};
 
 // The host-side name g_stbmm_scratch is only a stand-in for the symbol, not a
 // device address: the address is looked up once per device, with that device
-// current, and cached.
+// current, and cached.  It belongs to the device's primary context, the one
+// the runtime API uses; another context on the device or a cudaDeviceReset
+// would need a new lookup, and neither is supported (documented in the header).
 static int noalloc_scratch(int device, double **out) {
     if (device < 0 || device >= 64) return MDP_EINVAL;
     std::lock_guard<std::mutex> lk(g_noalloc_mu);

@@ -256,9 +256,10 @@ class ShardedGLS:
         return x, it, res
 
     def solve(self, tol: float = 1e-8, maxiter: int = 500, precision: str = "fp64", inner_tol: float = 1e-4,
-              inner_maxiter: int = 100):
+              inner_maxiter: int = 100, on_iter=None):
         """Returns (x over the global kept pixels, their global pixel ids, rcond, hits, DistInfo); x is
-        replicated on every rank, pixel-major (I, Q, U)."""
+        replicated on every rank, pixel-major (I, Q, U).  on_iter(res) is called after each FP64 PCG
+        iteration with its residual sum(g^2)."""
         if not hasattr(self, "pg"):
             self.setup()
         b = self._residual(None)
@@ -268,7 +269,7 @@ class ShardedGLS:
             return x, self.pg, self.rcond, self.hits, DistInfo(0, 0, True, res0, res0, self.n, self.n_cut)
         tol2 = tol * tol * res0
         if precision == "fp64":
-            x, it, res = self._pcg(b, tol2, maxiter - 1, False)
+            x, it, res = self._pcg(b, tol2, maxiter - 1, False, on_iter)
             info = DistInfo(it, 0, res <= tol2, res0, res, self.n, self.n_cut)
             return x, self.pg, self.rcond, self.hits, info
         if precision != "mixed":

@@ -67,11 +67,57 @@ def trmatvec(gindices, values, y, m, n, nnz=3):
 
 
 def stbmm(V, block_sizes, lam, invtt):
+    """apply_weights (pcg_true.c:578-600) on the Toeplitz blocks of one rank:
+    stbmmProd, or the white weighting when lam == 1."""
     bs = np.ascontiguousarray(block_sizes, dtype=np.int32).copy()
     tt = np.ascontiguousarray(invtt, dtype=np.float64).copy()
     out = np.ascontiguousarray(V, dtype=np.float64).copy()
     lib().ref_stbmm(len(bs), _p(bs, I32), lam, _p(tt, F64), _p(out, F64))
     return out
+
+
+class Flag(ct.Structure):
+    """The reference's Flag (toeplitz.h:169-182)."""
+    _fields_ = [(n, ct.c_int) for n in ("flag_bs", "flag_nfft", "flag_fftw", "flag_no_rshp", "flag_nofft",
+                                        "flag_blockingcomm", "fixed_nfft", "fixed_bs", "flag_verbose",
+                                        "flag_skip_build_gappy_blocks", "flag_param_distmin_fixed",
+                                        "flag_precompute_lvl")]
+
+
+def define_blocksize(n, lam, bs_flag, fixed_bs=0):
+    """The reference's define_blocksize (toeplitz.c:168-253)."""
+    f = lib().define_blocksize
+    f.restype = ct.c_int
+    return int(f(n, lam, bs_flag, fixed_bs))
+
+
+def tpltz_init(n, lam, T, flag_bs=0, fixed_bs=0, flag_nfft=0, fixed_nfft=0):
+    """The reference's tpltz_init (toeplitz.c:298-367): (nfft, blocksize, T_fft as
+    complex [bs/2+1]); its arrays are released with tpltz_cleanup."""
+    L = lib()
+    fl = Flag()
+    L.flag_stgy_init_auto(ct.byref(fl))
+    fl.flag_bs, fl.fixed_bs, fl.flag_nfft, fl.fixed_nfft = flag_bs, fixed_bs, flag_nfft, fixed_nfft
+    tt = np.ascontiguousarray(T, dtype=np.float64).copy()
+    nfft, bs = ct.c_int(0), ct.c_int(0)
+    tf, vf, vr = ct.c_void_p(), ct.c_void_p(), ct.c_void_p()
+    pf, pb = ct.c_void_p(), ct.c_void_p()
+    L.tpltz_init.argtypes = [ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                             ct.c_void_p, ct.c_void_p, ct.c_void_p, Flag]
+    rc = L.tpltz_init(n, lam, ct.byref(nfft), ct.byref(bs), ct.byref(tf), _p(tt, F64), ct.byref(vf), ct.byref(vr),
+                      ct.byref(pf), ct.byref(pb), fl)
+    if rc != 0:
+        raise RuntimeError(f"reference tpltz_init failed (status {rc})")
+    h = bs.value // 2 + 1
+    out = np.ctypeslib.as_array(ct.cast(tf, ct.POINTER(F64)), shape=(2 * h,)).copy()
+    L.tpltz_cleanup(ct.byref(tf), ct.byref(vf), ct.byref(vr), ct.byref(pf), ct.byref(pb))
+    return nfft.value, bs.value, out[0::2] + 1j * out[1::2]
+
+
+def apply_weights(block_sizes, lam, invtt, tod):
+    """The reference's apply_weights (pcg_true.c:578-600) on one rank: white
+    weighting for lambda 1, stbmmProd otherwise."""
+    return stbmm(tod, block_sizes, lam, invtt)  # ref_stbmm calls apply_weights itself
 
 
 def pcg(gindices, values, signal, noise, block_sizes, lam, invtt, tol=1e-8, maxiter=500, nnz=3, precond=0,

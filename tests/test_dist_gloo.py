@@ -157,3 +157,57 @@ def test_two_gloo_ranks_match_single_process(case, precision):
     for k in range(3):
         sel = det[k::3]
         assert _rel(x0[k::3][sel], o.x[k::3][sel]) < 1e-8, (k, _rel(x0[k::3][sel], o.x[k::3][sel]))
+
+
+def _mlmap_worker(rank, world, port, outdir):
+    """MLmap as a MAPPRAISER caller with one rank per process calls it: each rank
+    passes data_size_proc (all ranks) and its own samples and blocks."""
+    import torch.distributed as dist
+    from midapack_b200 import mappraiser_wrapper as mw
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        wl = _MLMAP_CASE()
+        pix, w, sig, noi, bs, lam, tt = _split(wl, rank, world)
+        dsp = np.array([len(_split(wl, r, world)[2]) for r in range(world)], dtype=np.int32)
+        params = dict(path_output=outdir, ref="sh", solver=0, precond=0, Z_2lvl=0, ptcomm_flag=6, tol=1e-10,
+                      maxiter=600, enlFac=1, ortho_alg=1, bs_red=0, nside=wl.nside, Lambda=lam)
+        mw.MLmap(dist.group.WORLD, params, dsp, len(bs), bs, 3, pix, w, sig, noi, tt,
+                 shard=OracleShard(pix, w, sig, noi, bs, lam, tt))
+    finally:
+        dist.destroy_process_group()
+
+
+# 2 x 8 x 24 flat grid sized so that 12 nside^2 pixels cover it (nside 8)
+_MLMAP_CASE = lambda: synth.make_workload("mlmap2", 32, 24, 4, 2048, 1024, 32, seed=43, gap_frac=0.02)  # noqa: E731
+
+
+def test_mlmap_on_two_ranks_writes_the_reference_maps(ref_lib, tmp_path):
+    """MLmap with a two-rank process group (gloo, CPU; the oracle's operators as
+    each rank's shard): rank 0's FITS maps against the reference's own MLmap
+    (oracle/_ref) on two forked ranks with the same split (mappraiser.c:64-88):
+    Hits equal, Cond within 1e-12, I/Q/U within 1e-8 on the observed pixels."""
+    from midapack_b200 import mappraiser_wrapper as mw
+    wl = _MLMAP_CASE()
+    assert wl.nside == 8
+    ctx = tmp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_mlmap_worker, args=(r, 2, port, str(tmp_path))) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(300)
+        assert p.exitcode == 0
+    maps = [mw.read_fits_map(str(tmp_path / f"{k}_sh.fits")) for k in ("mapI", "mapQ", "mapU", "Cond", "Hits")]
+    half = wl.n_samples // 2
+    nb = len(wl.block_sizes)
+    I, Q, U, Cond, Hits, res = ref_lib.mlmap(2, [half, half], [nb // 2, nb // 2], wl.block_sizes, wl.pix, wl.weights,
+                                             wl.signal, wl.noise, wl.lam, wl.invtt, wl.nside, tol=1e-10, maxiter=600)
+    np.testing.assert_array_equal(maps[4], Hits)
+    obs = Hits > 0
+    np.testing.assert_allclose(maps[3][obs], Cond[obs], rtol=1e-12, atol=0)
+    for mine, theirs in zip(maps[:3], (I, Q, U)):
+        assert _rel(mine[obs], theirs[obs]) < 1e-8
+    rr = np.fromfile(str(tmp_path / "pcg_residuals_sh.dat"))
+    assert rr[0] == 1.0 and abs(len(rr) - len(res)) <= 1

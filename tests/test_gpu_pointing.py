@@ -1,5 +1,5 @@
 """Pointing matrix on the GPU vs the oracle: index compression bit-exact,
-P and P^T within 1e-13 (FP64; P^T accumulates with atomics)."""
+P and P^T within 1e-13 (FP64); P^T by map bins bit-reproducible."""
 import numpy as np
 import pytest
 
@@ -129,3 +129,43 @@ def test_binned_transpose_large(gpu_ctx, gaps):
         torch.cuda.synchronize()
         xr = R.trmatvec(A, t)
         assert np.linalg.norm(xo.cpu().numpy() - xr) <= 1e-13 * np.linalg.norm(xr)
+
+
+@pytest.mark.parametrize("grid", [(40, 30), (4, 3)])
+@pytest.mark.parametrize("fp32", [False, True])
+def test_binned_transpose_is_reproducible(gpu_ctx, fp32, grid):
+    """P^T by map bins adds every row in a fixed order (time order within a bin,
+    lane order for rows of one step on one pixel): repeated applications, and
+    two pointing objects built from the same arrays, give bit-identical maps;
+    FP64 P^T, and the FP32 operator P^T N^-1 P of the mixed solver.  On the
+    4 x 3 grid every step of 32 rows revisits pixels (the lane-order path)."""
+    import torch
+    import midapack_b200 as mb
+    wl = synth.make_workload("rep", grid[0], grid[1], 3, 1 << 19, 1 << 19, 32, gap_frac=0.01, seed=14)
+    m = wl.n_samples
+    rng = np.random.default_rng(5)
+    t = rng.standard_normal(m)
+    outs = []
+    for _ in range(2):
+        P = mb.Pointing(gpu_ctx, _dev(wl.pix), _dev(wl.weights), m, 3)
+        n = P.shape()["n_map"]
+        h = _dev(np.random.default_rng(6).standard_normal(n))
+        N = mb.Noise(gpu_ctx, wl.block_sizes, wl.lam, wl.invtt) if fp32 else None
+        for _ in range(2):
+            xo = torch.full((n,), np.nan, dtype=torch.float64, device="cuda")
+            if fp32:
+                mb.check(mb.lib().mdp_apply_op(gpu_ctx.h, P.h, N.h, h.data_ptr(), xo.data_ptr(), 1), "mdp_apply_op")
+            else:
+                P.trmatvec(_dev(t), xo)
+            torch.cuda.synchronize()
+            outs.append(xo.cpu().numpy())
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])
+    A = R.local_shape(wl.pix, wl.weights, m, 3)
+    if fp32:
+        hh = np.random.default_rng(6).standard_normal(A.n)
+        xr = R.trmatvec(A, R.stbmm(R.matvec(A, hh), wl.block_sizes, wl.lam, wl.invtt))
+        assert np.linalg.norm(outs[0] - xr) <= 1e-5 * np.linalg.norm(xr)
+    else:
+        xr = R.trmatvec(A, t)
+        assert np.linalg.norm(outs[0] - xr) <= 1e-13 * np.linalg.norm(xr)

@@ -1,7 +1,6 @@
 """N^-1 (block mean removal + banded Toeplitz, overlap-save FFT) on the GPU vs
 the oracle's exact long-double banded product.  Tolerance: 1e-12 norm-wise
 relative per application (FP64)."""
-import os
 
 import numpy as np
 import pytest
@@ -16,17 +15,9 @@ TOL = 1e-12
 def _run(gpu_ctx, block_sizes, lam, invtt, v, fft=None):
     import torch
     import midapack_b200 as mb
-    old = os.environ.get("MDP_TOEPLITZ_FFT")
+    N = mb.Noise(gpu_ctx, block_sizes, lam, invtt)
     if fft:
-        os.environ["MDP_TOEPLITZ_FFT"] = str(fft)
-    try:
-        N = mb.Noise(gpu_ctx, block_sizes, lam, invtt)
-    finally:
-        if fft:
-            if old is None:
-                del os.environ["MDP_TOEPLITZ_FFT"]
-            else:
-                os.environ["MDP_TOEPLITZ_FFT"] = old
+        N.set_plan(fft if isinstance(fft, str) else f"fft:{fft}")
     vin = torch.from_numpy(v).cuda()
     vout = torch.empty_like(vin)
     N.apply(vin, vout)
@@ -51,6 +42,11 @@ def _rel(a, b):
     (8192, [24000, 24000], None),     # the reference fixture's shape
     (8192, [70000], 65536),           # 4-CTA cluster tile
     (16384, [140000], 131072),        # 8-CTA cluster tile
+    (4096, [40000, 9000], "c,2"),     # cluster four-step tiles: 2, 4, 8 CTAs (2C x 4096 points)
+    (8192, [70000, 9000], "c,4"),
+    (16384, [140000, 40000], "c,8"),
+    (16384, [1 << 20], "c,8"),        # the at-scale block: 11 tiles, interior and edge tiles
+    (100, [300000, 5000], "c,8"),     # narrow band: blocks shorter than a tile, windows past both ends
 ])
 def test_stbmm_vs_exact(gpu_ctx, lam, sizes, fft):
     rng = np.random.default_rng(lam + len(sizes))
@@ -117,9 +113,13 @@ def test_stbmm_rejects_band_wider_than_block(gpu_ctx):
     (4096, [40000, 9000], "s,7,8"),
     (8192, [70000], "s,8,8"),
     (16384, [140000, 3 * 16384], "s,8,9"),    # largest split tile: 256 x 512 points
+    (64, [4096, 777, 130], "c,2"),            # cluster four-step tiles: blocks far shorter than a tile
+    (2048, [20000, 4100, 65537], "c,4"),
+    (16384, [140000, 3 * 16384], "c,8"),
 ])
 def test_stbmm_split_plan_vs_exact(gpu_ctx, lam, sizes, plan):
-    """The three-kernel (four-step FFT) tile plan, FP64 and FP32."""
+    """The three-kernel (four-step FFT) tile plans and the cluster four-step
+    plans, FP64 and FP32."""
     import torch
     import midapack_b200 as mb
     rng = np.random.default_rng(lam + 7)
@@ -128,16 +128,14 @@ def test_stbmm_split_plan_vs_exact(gpu_ctx, lam, sizes, plan):
     t[1:] = rng.standard_normal(lam - 1) * np.exp(-np.arange(1, lam) / (0.3 * lam))
     invtt = np.tile(t, len(sizes))
     v = rng.standard_normal(int(sum(sizes))) + 3.0
-    os.environ["MDP_TOEPLITZ_PLAN"] = plan
-    os.environ["MDP_TOEPLITZ_PLAN32"] = plan
-    try:
-        N = mb.Noise(gpu_ctx, sizes, lam, invtt)
-        tile, tile32 = N.tile(), N.tile_fp32()
-    finally:
-        del os.environ["MDP_TOEPLITZ_PLAN"]
-        del os.environ["MDP_TOEPLITZ_PLAN32"]
-    m1, m2 = (int(x) for x in plan.split(",")[1:])
-    assert tile["split"] == [1 << m1, 1 << m2] and tile32["split"] == [1 << m1, 1 << m2]
+    N = mb.Noise(gpu_ctx, sizes, lam, invtt).set_plan(plan).set_plan(plan, fp32=True)
+    tile, tile32 = N.tile(), N.tile_fp32()
+    if plan[0] == "s":
+        m1, m2 = (int(x) for x in plan.split(",")[1:])
+        assert tile["split"] == [1 << m1, 1 << m2] and tile32["split"] == [1 << m1, 1 << m2]
+    else:
+        shape = [2 * int(plan.split(",")[1]), 4096]
+        assert tile["cluster_four_step"] == shape and tile32["cluster_four_step"] == shape
     vin = torch.from_numpy(v).cuda()
     vout = torch.empty_like(vin)
     N.apply(vin, vout)
@@ -163,14 +161,7 @@ def test_split_plans_of_two_operators_share_kernels(gpu_ctx):
         t = np.zeros(lam)
         t[0] = 2.0
         t[1:] = rng.standard_normal(lam - 1) * np.exp(-np.arange(1, lam) / (0.3 * lam))
-        os.environ["MDP_TOEPLITZ_PLAN"] = plan
-        os.environ["MDP_TOEPLITZ_PLAN32"] = plan
-        try:
-            N = mb.Noise(gpu_ctx, sizes, lam, np.tile(t, len(sizes)))
-            N.tile_fp32()
-        finally:
-            del os.environ["MDP_TOEPLITZ_PLAN"]
-            del os.environ["MDP_TOEPLITZ_PLAN32"]
+        N = mb.Noise(gpu_ctx, sizes, lam, np.tile(t, len(sizes))).set_plan(plan).set_plan(plan, fp32=True)
         ops.append((N, sizes, lam, np.tile(t, len(sizes))))
     for N, sizes, lam, invtt in ops:
         v = np.random.default_rng(lam + 1).standard_normal(int(sum(sizes)))

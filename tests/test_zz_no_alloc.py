@@ -43,6 +43,40 @@ def test_noalloc_matches_regular_two_calls(gpu_ctx):
         assert _rel(out.cpu().numpy(), ref.cpu().numpy()) < TOL
 
 
+@pytest.mark.parametrize("case", ["gaps_between_blocks", "white"])
+def test_noalloc_gapped_and_white_operators(gpu_ctx, case):
+    """Blocks that leave rows uncovered (those rows pass through unchanged, a copy
+    made before the blocks are applied) and the white-noise operator (lambda 1,
+    no mean removal), each twice in a row against mdp_stbmm."""
+    import torch
+    import midapack_b200 as mb
+    from midapack_b200 import synth
+    L = mb.lib()
+    if case == "white":
+        sizes, idv, lam = [5000, 7000], [0, 5000], 1
+        invtt = np.array([0.7, 2.5])
+    else:
+        sizes, idv, lam = [70000, 20000], [1000, 90000], 256
+        invtt = np.concatenate([synth.invtt_row(1 << 15, lam, fk) for fk in (1.0, 0.4)])
+    nrow = idv[-1] + sizes[-1]
+    N = mb.Noise(gpu_ctx, sizes, lam, invtt, idv=np.array(idv, dtype=np.int64))
+    rng = np.random.default_rng(23)
+    for call in range(2):
+        v = torch.from_numpy(rng.standard_normal(nrow) + 3.0 * call).cuda()
+        ref = torch.full_like(v, np.nan)
+        out = torch.full_like(v, np.nan)
+        N.apply(v, ref)
+        rc = L.mdp_stbmm_noalloc(gpu_ctx.h, N.h, ct.c_void_p(v.data_ptr()), ct.c_void_p(out.data_ptr()))
+        assert rc == 0, L.mdp_last_error().decode()
+        torch.cuda.synchronize()
+        o, r = out.cpu().numpy(), ref.cpu().numpy()
+        covered = np.zeros(nrow, dtype=bool)
+        for s0, n in zip(idv, sizes):
+            covered[s0:s0 + n] = True
+        assert np.isfinite(o[covered]).all() and _rel(o[covered], r[covered]) < TOL
+        assert np.array_equal(o[~covered], r[~covered]) and np.array_equal(o[~covered], v.cpu().numpy()[~covered])
+
+
 def test_noalloc_rejects_in_place_and_oversize(gpu_ctx):
     import torch
     import midapack_b200 as mb
