@@ -937,12 +937,24 @@ def run_e2e_device_api(args, wl, world, pinned):
     nb = len(wl.block_sizes)
     idv = np.arange(nb, dtype=np.int64) * wl.block_len
     times, it = [], 0
+    copy_stream = torch.cuda.Stream()
     for _ in range(args.e2e_steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        dev = {k: v.to("cuda", non_blocking=True) for k, v in pinned.items()}
+        # the pointing first (the compression needs only it); weights, signal and
+        # noise follow on a second stream while the pointing is compressed and
+        # the noise operator (spectra, tile plans) is built
+        dev = {"pix": pinned["pix"].to("cuda", non_blocking=True)}
+        with torch.cuda.stream(copy_stream):
+            for k in ("weights", "signal", "noise"):
+                dev[k] = pinned[k].to("cuda", non_blocking=True)
+            copied = torch.cuda.Event()
+            copied.record(copy_stream)
         P = mb.Pointing(ctx, dev["pix"], dev["weights"], wl.n_samples, 3)
         N = mb.Noise(ctx, wl.block_sizes, wl.lam, wl.invtt, idv=idv)
+        torch.cuda.current_stream().wait_event(copied)
+        for k in ("weights", "signal", "noise"):
+            dev[k].record_stream(torch.cuda.current_stream())
         if args.precision == "mixed":
             out = mb.gls_solve_mixed(ctx, P, N, dev["signal"], dev["noise"], tol=TOL, maxiter=MAXITER,
                                      inner_tol=args.inner_tol)

@@ -44,7 +44,9 @@ struct SlotScal {
     double tol2;     // inner stop: res <= tol2 * rin0
     double dot;      // result of mr_dot_kernel
     int    cont;     // 1 while the inner PCG of the slot continues
-    int    pad[3];
+    int    stopped;  // set by the device when the inner PCG stops (the slot's run flag drops)
+    int    inner_it; // inner iterations since the slot's last (re)start
+    int    budget;   // inner iterations the slot may still take (inner cap, column cap)
 };
 
 struct MRed {
@@ -99,9 +101,13 @@ __global__ void __launch_bounds__(512) mr_matvec32_kernel(const int32_t *__restr
                                                           const int64_t *__restrict__ chunk_start,
                                                           const int32_t *__restrict__ chunk_len, int n_chunks,
                                                           double *__restrict__ partial) {
-    bool act[G];
+    bool act[G], any = false;
 #pragma unroll
-    for (int j = 0; j < G; j++) act[j] = run[j] != 0;
+    for (int j = 0; j < G; j++) {
+        act[j] = run[j] != 0;
+        any = any || act[j];
+    }
+    if (!any) return;  // every slot has stopped
     const int64_t s = chunk_start[blockIdx.x];
     const int     n = chunk_len[blockIdx.x];
     double        acc[G];
@@ -197,9 +203,13 @@ __global__ void __launch_bounds__(512) mr_trmatvec32_kernel(const int32_t *__res
     constexpr int BP = MR_BIN_PIX / G;
     static_assert(BP % 32 == 0, "bins must hold a multiple of 32 pixels");
     __shared__ double acc[3 * MR_BIN_PIX];
-    bool              act[G];
+    bool              act[G], any = false;
 #pragma unroll
-    for (int j = 0; j < G; j++) act[j] = run[j] != 0;
+    for (int j = 0; j < G; j++) {
+        act[j] = run[j] != 0;
+        any = any || act[j];
+    }
+    if (!any) return;  // every slot has stopped
     const int64_t bin = blockIdx.x / MR_SPLIT;
     const int     part = blockIdx.x % MR_SPLIT;
     for (int i = threadIdx.x; i < 3 * MR_BIN_PIX; i += blockDim.x) acc[i] = 0.0;
@@ -263,6 +273,10 @@ template <int G>
 __global__ void __launch_bounds__(MR_THREADS) mr_coeff_kernel(const double *__restrict__ H,
                                                              const double *__restrict__ Q, int64_t npix,
                                                              const int *__restrict__ run, SlotScal *S, MRed *R) {
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < G; j++) any = any || run[j] != 0;
+    if (!any) return;  // every slot has stopped: the whole grid returns
     double v[G];
 #pragma unroll
     for (int j = 0; j < G; j++) v[j] = 0.0;
@@ -289,15 +303,17 @@ __global__ void __launch_bounds__(MR_THREADS) mr_update_kernel(const double *__r
                                                               const double *__restrict__ H,
                                                               const double *__restrict__ Q,
                                                               const double *__restrict__ GP, double *__restrict__ Gn,
-                                                              double *__restrict__ CG, int64_t npix,
-                                                              const int *__restrict__ run, SlotScal *S, MRed *R) {
+                                                              double *__restrict__ CG, int64_t npix, int *run,
+                                                              SlotScal *S, MRed *R) {
     double ro[G];
-    bool   act[G];
+    bool   act[G], any = false;
 #pragma unroll
     for (int j = 0; j < G; j++) {
         act[j] = run[j] != 0;
+        any = any || act[j];
         ro[j] = S[j].ro;
     }
+    if (!any) return;  // every slot has stopped: the whole grid returns, no partials
     double v[3 * G];
 #pragma unroll
     for (int k = 0; k < 3 * G; k++) v[k] = 0.0;
@@ -339,7 +355,13 @@ __global__ void __launch_bounds__(MR_THREADS) mr_update_kernel(const double *__r
             s.g2pix_polak = mr_sum(R, G + j);
             s.res = mr_sum(R, 2 * G + j);
             s.gamma = s.g2pix_polak / s.g2pixp;
-            s.cont = (isfinite(s.res) && s.res > s.tol2 * s.rin0) ? 1 : 0;
+            s.inner_it++;
+            s.budget--;
+            s.cont = (isfinite(s.res) && s.res > s.tol2 * s.rin0 && s.budget > 0) ? 1 : 0;
+            if (!s.cont) {  // the slot stops here: later iterations of the batch skip it
+                s.stopped = 1;
+                run[j] = 0;
+            }
         }
         R->count[1] = 0;
     }
@@ -352,8 +374,8 @@ __global__ void __launch_bounds__(MR_THREADS) mr_slot_init_kernel(const double *
                                                                  const double *__restrict__ r, int j,
                                                                  double *__restrict__ Gn, double *__restrict__ CG,
                                                                  double *__restrict__ H, double *__restrict__ DL,
-                                                                 int64_t npix, double tol2, int *run, SlotScal *S,
-                                                                 MRed *R) {
+                                                                 int64_t npix, double tol2, int budget, int *run,
+                                                                 SlotScal *S, MRed *R) {
     double v[2] = {0.0, 0.0};
     for (int64_t p = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += (int64_t) gridDim.x * blockDim.x) {
         const double *I = inv + 9 * p;
@@ -385,6 +407,9 @@ __global__ void __launch_bounds__(MR_THREADS) mr_slot_init_kernel(const double *
         s.rin0 = s.res;
         s.tol2 = tol2;
         s.cont = 0;  // h = Cg already: no direction update before the first iteration
+        s.stopped = 0;
+        s.inner_it = 0;
+        s.budget = budget;
         run[j] = 1;
         R->count[2] = 0;
     }
@@ -462,12 +487,13 @@ int launch_apply32(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, Batch &B, co
 }
 
 // one batched inner iteration: direction (slots that continue), q = A32 h,
-// coeff, update; ends with the slot scalars copied to pinned host memory
+// coeff, update (which stops a slot's inner PCG on the device); with h_scal,
+// ends with the slot scalars copied to pinned host memory
 template <int G>
 int launch_iteration(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, Batch &B, const double *inv, double *g,
                      double *gp, SlotScal *h_scal) {
     cudaStream_t st = ctx->stream;
-    const int   *run = B.run.as<int>();
+    int         *run = B.run.as<int>();
     SlotScal    *S = B.scal.as<SlotScal>();
     MRed        *R = B.red.as<MRed>();
     const int    gv = grid_for(B.npix * 3 * G, 256, ctx->sm_count * 8);
@@ -479,7 +505,18 @@ int launch_iteration(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, Batch &B, 
     mr_update_kernel<G><<<MR_BLOCKS, MR_THREADS, 0, st>>>(inv, B.DL.as<double>(), B.H.as<double>(), B.Q.as<double>(),
                                                           gp, g, B.CG.as<double>(), B.npix, run, S, R);
     MDP_CHECK_LAUNCH(ctx);
-    MDP_CUDA(cudaMemcpyAsync(h_scal, S, sizeof(SlotScal) * G, cudaMemcpyDeviceToHost, st));
+    if (h_scal) MDP_CUDA(cudaMemcpyAsync(h_scal, S, sizeof(SlotScal) * G, cudaMemcpyDeviceToHost, st));
+    return MDP_OK;
+}
+
+// K batched iterations (K even: the gradient buffers end where they started);
+// the slot scalars reach the host after the last
+constexpr int MR_K = 4;
+template <int G>
+int launch_iterations(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, Batch &B, const double *inv,
+                      double *const bufs[2], SlotScal *h_scal) {
+    for (int k = 0; k < MR_K; k++)
+        MDP_TRY(launch_iteration<G>(ctx, A, N, B, inv, bufs[(k & 1) ^ 1], bufs[k & 1], k == MR_K - 1 ? h_scal : nullptr));
     return MDP_OK;
 }
 
@@ -588,14 +625,15 @@ int run_multi(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, const BJState &bj
     };
 
     std::vector<double> tol2rel(nrhs, 0.0);
-    std::vector<int>    slot_col(G, -1), inner_it(G, 0);
-    // gradient buffers: an iteration reads the current gradient bufs[parity]
-    // (as gp) and writes the new one into bufs[parity ^ 1]
+    std::vector<int>    slot_col(G, -1), seen_it(G, 0);
+    // gradient buffers: an iteration reads the current gradient bufs[k & 1] (as
+    // gp) and writes the new one into bufs[(k & 1) ^ 1]; a batch of MR_K (even)
+    // iterations leaves the current gradients in bufs[0], where slots start
     double *const       bufs[2] = {B.G1.as<double>(), B.G2.as<double>()};
-    int                 parity = 0;
     const double        itol2 = prm->inner_tol * prm->inner_tol;
     int                 next = 0, batched = 0;
     for (int c = 0; c < nrhs; c++) ci[c] = mdp_multi_col_info{0, 0, 0, 0.0, 0.0};
+    auto budget = [&](int col) { return std::max(1, std::min(prm->inner_maxiter, prm->maxiter - ci[col].iterations)); };
 
     // load the next unconverged column into slot j (or leave it idle)
     auto load = [&](int j) -> int {
@@ -611,11 +649,11 @@ int run_multi(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, const BJState &bj
                 continue;
             }
             slot_col[j] = col;
-            inner_it[j] = 0;
-            mr_slot_init_kernel<G><<<MR_BLOCKS, MR_THREADS, 0, st>>>(inv, rv.as<double>(), j, bufs[parity],
+            seen_it[j] = 0;
+            mr_slot_init_kernel<G><<<MR_BLOCKS, MR_THREADS, 0, st>>>(inv, rv.as<double>(), j, bufs[0],
                                                                      B.CG.as<double>(), B.H.as<double>(),
-                                                                     B.DL.as<double>(), npix, itol2, B.run.as<int>(),
-                                                                     S, R);
+                                                                     B.DL.as<double>(), npix, itol2, budget(col),
+                                                                     B.run.as<int>(), S, R);
             MDP_CHECK_LAUNCH(ctx);
             return MDP_OK;
         }
@@ -625,8 +663,9 @@ int run_multi(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, const BJState &bj
     };
     for (int j = 0; j < G; j++) MDP_TRY(load(j));
 
-    // the batched iteration as two CUDA graphs (g and gp alternate)
-    cudaGraphExec_t gx[2] = {nullptr, nullptr};
+    // MR_K batched iterations as one CUDA graph: the inner stop test and the
+    // stop of a slot run on the device, the host waits once per MR_K iterations
+    cudaGraphExec_t gx = nullptr;
     bool            graphs = prm->use_graph != 0;
     uint64_t        graph_launches = 0;  // kernels in one replay
     if (graphs) {
@@ -637,42 +676,36 @@ int run_multi(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, const BJState &bj
             cudaGetLastError();
             graphs = false;
         }
-        for (int k = 0; k < 2 && graphs; k++) {
+        if (graphs) {
             cudaGraph_t graph = nullptr;
             if (cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
                 if (prm->verbose) printf("graph capture unavailable: %s\n", cudaGetErrorString(cudaGetLastError()));
                 cudaGetLastError();
                 graphs = false;
-                break;
+            } else {
+                const uint64_t l0 = ctx->launches;
+                ctx->stream = cap;
+                int         rc = launch_iterations<G>(ctx, A, N, B, inv, bufs, hs);
+                cudaError_t e = cudaStreamEndCapture(cap, &graph);
+                ctx->stream = st;
+                graph_launches = ctx->launches - l0;
+                ctx->launches = l0;
+                cudaError_t ei = (rc == MDP_OK && e == cudaSuccess && graph) ? cudaGraphInstantiate(&gx, graph, 0)
+                                                                             : cudaErrorUnknown;
+                if (ei != cudaSuccess) {
+                    if (prm->verbose)
+                        printf("graph capture failed (rc %d): %s / %s\n", rc, cudaGetErrorString(e), cudaGetErrorString(ei));
+                    cudaGetLastError();
+                    graphs = false;
+                    gx = nullptr;
+                }
+                if (graph) cudaGraphDestroy(graph);
             }
-            const uint64_t l0 = ctx->launches;
-            ctx->stream = cap;
-            int         rc = launch_iteration<G>(ctx, A, N, B, inv, bufs[k ^ 1], bufs[k], hs);
-            cudaError_t e = cudaStreamEndCapture(cap, &graph);
-            ctx->stream = st;
-            graph_launches = ctx->launches - l0;
-            ctx->launches = l0;
-            cudaError_t ei = (rc == MDP_OK && e == cudaSuccess && graph) ? cudaGraphInstantiate(&gx[k], graph, 0)
-                                                                         : cudaErrorUnknown;
-            if (ei != cudaSuccess) {
-                if (prm->verbose)
-                    printf("graph capture failed (rc %d): %s / %s\n", rc, cudaGetErrorString(e), cudaGetErrorString(ei));
-                cudaGetLastError();
-                graphs = false;
-            }
-            if (graph) cudaGraphDestroy(graph);
         }
         if (cap) cudaStreamDestroy(cap);
-        if (!graphs)
-            for (auto &x : gx)
-                if (x) {
-                    cudaGraphExecDestroy(x);
-                    x = nullptr;
-                }
     }
     auto cleanup = [&]() {
-        for (auto &x : gx)
-            if (x) cudaGraphExecDestroy(x);
+        if (gx) cudaGraphExecDestroy(gx);
     };
 
     int rc = MDP_OK;
@@ -680,15 +713,14 @@ int run_multi(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, const BJState &bj
         bool any = false;
         for (int j = 0; j < G; j++) any = any || slot_col[j] >= 0;
         if (!any) break;
-        double *gnew = bufs[parity ^ 1], *gold = bufs[parity];
         if (graphs) {
-            if (cudaGraphLaunch(gx[parity], st) != cudaSuccess) {
+            if (cudaGraphLaunch(gx, st) != cudaSuccess) {
                 mdp_set_error("mdp_gls_solve_multi: graph launch: %s", cudaGetErrorString(cudaGetLastError()));
                 rc = MDP_ECUDA;
                 break;
             }
             ctx->launches += graph_launches;
-        } else if ((rc = launch_iteration<G>(ctx, A, N, B, inv, gnew, gold, hs))) {
+        } else if ((rc = launch_iterations<G>(ctx, A, N, B, inv, bufs, hs))) {
             break;
         }
         if (cudaStreamSynchronize(st) != cudaSuccess) {
@@ -696,20 +728,18 @@ int run_multi(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, const BJState &bj
             rc = MDP_ECUDA;
             break;
         }
-        batched++;
-        parity ^= 1;  // bufs[parity] = gnew holds the current gradients
+        batched += MR_K;
         for (int j = 0; j < G && rc == MDP_OK; j++) {
             const int col = slot_col[j];
             if (col < 0) continue;
-            inner_it[j]++;
-            ci[col].iterations++;
+            ci[col].iterations += hs[j].inner_it - seen_it[j];
+            seen_it[j] = hs[j].inner_it;
             if (!std::isfinite(hs[j].res)) {
                 mdp_set_error("mdp_gls_solve_multi: inner residual of column %d became %f", col, hs[j].res);
                 rc = MDP_ENAN;
                 break;
             }
-            const bool stop = !hs[j].cont || inner_it[j] >= prm->inner_maxiter || ci[col].iterations >= prm->maxiter;
-            if (!stop) continue;
+            if (!hs[j].stopped) continue;
             // refinement step of this column
             mr_extract_add_kernel<G><<<gn, 256, 0, st>>>(B.DL.as<double>(), j, d_x + (size_t) col * nmap, npix);
             MDP_CHECK_LAUNCH(ctx);
@@ -724,14 +754,14 @@ int run_multi(mdp_context *ctx, mdp_pointing *A, mdp_noise *N, const BJState &bj
                 ci[col].converged = res <= tol2rel[col];
                 if ((rc = load(j))) break;
             } else {
-                inner_it[j] = 0;
+                seen_it[j] = 0;
                 // inner target of this refinement: inner_tol, or the reduction
                 // still needed (factor 2 margin) when that is smaller
                 const double need = 0.5 * prm->tol / std::sqrt(res / ci[col].res0);
                 const double it = std::max(prm->inner_tol, std::min(need, 0.5));
-                mr_slot_init_kernel<G><<<MR_BLOCKS, MR_THREADS, 0, st>>>(inv, rv.as<double>(), j, bufs[parity],
+                mr_slot_init_kernel<G><<<MR_BLOCKS, MR_THREADS, 0, st>>>(inv, rv.as<double>(), j, bufs[0],
                                                                          B.CG.as<double>(), B.H.as<double>(),
-                                                                         B.DL.as<double>(), npix, it * it,
+                                                                         B.DL.as<double>(), npix, it * it, budget(col),
                                                                          B.run.as<int>(), S, R);
                 MDP_CHECK_LAUNCH(ctx);
             }

@@ -100,6 +100,14 @@ __device__ __forceinline__ Pr<double> pfma(Pr<double> x, Pr<double> y, Pr<double
 __device__ __forceinline__ Pr<double> pswap(Pr<double> p) { return {p.b, p.a}; }
 
 template <typename T> __device__ __forceinline__ Pr<T> pdup(T s) { return pmk(s, s); }
+// a compile-time constant on both lanes: plain integer bits for FP32 (the
+// compiler may rematerialise it at each use instead of keeping it live)
+template <typename T> __device__ __forceinline__ Pr<T> pcst(double v);
+template <> __device__ __forceinline__ Pr<float> pcst<float>(double v) {
+    const unsigned long long u = __float_as_uint((float) v);
+    return Pr<float>{(u << 32) | u};
+}
+template <> __device__ __forceinline__ Pr<double> pcst<double>(double v) { return Pr<double>{v, v}; }
 
 // complex values on both lanes: x = real parts (lane A, lane B), y = imaginary parts
 template <typename T> struct CP {
@@ -136,17 +144,17 @@ __device__ __forceinline__ CP<T> mulw16(CP<T> d) {
     if constexpr (M == 0) {
         return d;
     } else if constexpr (M == 4) {
-        if constexpr (!CONJ) return {d.y, psub(pdup<T>((T) 0), d.x)};  // * -i
-        else return {psub(pdup<T>((T) 0), d.y), d.x};                   // * i
+        if constexpr (!CONJ) return {d.y, psub(pcst<T>(0.0), d.x)};  // * -i
+        else return {psub(pcst<T>(0.0), d.y), d.x};                   // * i
     } else if constexpr (M == 2 || M == 6) {
-        const Pr<T> r = pdup<T>((T) 0.70710678118654752440);
+        const Pr<T> r = pcst<T>(0.70710678118654752440);
         // W^2 = (1 - i) r, W^6 = (-1 - i) r; conjugates (1 + i) r, (-1 + i) r
         if constexpr (M == 2 && !CONJ) return {pmul(padd(d.x, d.y), r), pmul(psub(d.y, d.x), r)};
         else if constexpr (M == 2 && CONJ) return {pmul(psub(d.x, d.y), r), pmul(padd(d.x, d.y), r)};
-        else if constexpr (M == 6 && !CONJ) return {pmul(psub(d.y, d.x), r), pmul(padd(d.x, d.y), psub(pdup<T>((T) 0), r))};
-        else return {pmul(padd(d.x, d.y), psub(pdup<T>((T) 0), r)), pmul(psub(d.x, d.y), r)};
+        else if constexpr (M == 6 && !CONJ) return {pmul(psub(d.y, d.x), r), pmul(padd(d.x, d.y), pcst<T>(-0.70710678118654752440))};
+        else return {pmul(padd(d.x, d.y), pcst<T>(-0.70710678118654752440)), pmul(psub(d.x, d.y), r)};
     } else {
-        const CP<T> w{pdup<T>((T) w16c(M)), pdup<T>((T) w16s(M))};
+        const CP<T> w{pcst<T>(w16c(M)), pcst<T>(w16s(M))};
         return CONJ ? cpmulc(d, w) : cpmul(d, w);
     }
 }
@@ -225,21 +233,43 @@ __host__ __device__ constexpr int ilog2_c(int v) { return v <= 1 ? 0 : 1 + ilog2
 
 // v[i] *= w^rev(i) (CONJ: times conj(w^rev(i))), i = 1..R-1, R = 2^L <= 16,
 // the powers from w^1 by a product tree of depth <= 4 (w^2k = (w^k)^2,
-// w^(h+j) = w^h w^j), each applied as soon as it is formed so that few powers
-// are live at once
+// w^(8+j) = w^8 w^j), each applied as soon as it is formed.  The powers are
+// named registers, not an array, so that nothing is placed in local memory.
+template <typename T, int R, bool CONJ, int K>
+__device__ __forceinline__ void apply_pow(CP<T> (&v)[R], const CP<T> &w) {
+    constexpr int i = rev_bits_c(K, ilog2_c(R));
+    v[i] = CONJ ? cpmulc(v[i], w) : cpmul(v[i], w);
+}
 template <typename T, int R, bool CONJ>
 __device__ __forceinline__ void apply_powers(CP<T> (&v)[R], CP<T> w1) {
-    constexpr int L = ilog2_c(R);
-    CP<T>         w[R];
-    w[1] = w1;
-#pragma unroll
-    for (int k = 1; k < R; k++) {
-        if (k > 1) {
-            const int hi = 1 << ilog2_c(k);  // highest power of two <= k
-            w[k] = (k == hi) ? cpmul(w[k / 2], w[k / 2]) : cpmul(w[hi], w[k - hi]);
+    static_assert(R == 2 || R == 4 || R == 8 || R == 16, "radix 2, 4, 8 or 16");
+    apply_pow<T, R, CONJ, 1>(v, w1);
+    if constexpr (R >= 4) {
+        const CP<T> w2 = cpmul(w1, w1);
+        apply_pow<T, R, CONJ, 2>(v, w2);
+        const CP<T> w3 = cpmul(w2, w1);
+        apply_pow<T, R, CONJ, 3>(v, w3);
+        if constexpr (R >= 8) {
+            const CP<T> w4 = cpmul(w2, w2);
+            apply_pow<T, R, CONJ, 4>(v, w4);
+            const CP<T> w5 = cpmul(w4, w1);
+            apply_pow<T, R, CONJ, 5>(v, w5);
+            const CP<T> w6 = cpmul(w4, w2);
+            apply_pow<T, R, CONJ, 6>(v, w6);
+            const CP<T> w7 = cpmul(w4, w3);
+            apply_pow<T, R, CONJ, 7>(v, w7);
+            if constexpr (R >= 16) {
+                const CP<T> w8 = cpmul(w4, w4);
+                apply_pow<T, R, CONJ, 8>(v, w8);
+                apply_pow<T, R, CONJ, 9>(v, cpmul(w8, w1));
+                apply_pow<T, R, CONJ, 10>(v, cpmul(w8, w2));
+                apply_pow<T, R, CONJ, 11>(v, cpmul(w8, w3));
+                apply_pow<T, R, CONJ, 12>(v, cpmul(w8, w4));
+                apply_pow<T, R, CONJ, 13>(v, cpmul(w8, w5));
+                apply_pow<T, R, CONJ, 14>(v, cpmul(w8, w6));
+                apply_pow<T, R, CONJ, 15>(v, cpmul(w8, w7));
+            }
         }
-        const int i = rev_bits_c(k, L);
-        v[i] = CONJ ? cpmulc(v[i], w[k]) : cpmul(v[i], w[k]);
     }
 }
 
@@ -272,10 +302,13 @@ struct Ninv4Args {
     const int32_t *blk_len;
     const int32_t *blk_spec;
     const Ent<T>  *hc;          // [n_spec][C][16][256]: ((ca_A, ca_B), (cb_A, cb_B)), scaled by 1/(4M)
-    const Ent<T>  *wk;          // [C][16][256]: (W_N^k_A, W_N^k_B) as ((re_A, re_B), (im_A, im_B))
+    const Ent<T>  *wbase;       // [C]: (W_N^rA, W_N^rB) of CTA c's rows, as ((re_A, re_B), (im_A, im_B))
+    const typename std::conditional<sizeof(T) == 4, float2, double2>::type *w8192;  // [16][256]: W_2M2^rev(16t+i)
     const double2 *twM;         // [M2]: W_M^n2 (FP64; rounded to T on use)
     const double2 *tw4096;      // [256]: W_4096^q
     const double  *means;       // [nb] or [ncols][nb]
+    int64_t        n_tiles;
+    int64_t        ahead;       // tiles between this one and the one whose input is prefetched
     int            lambda;
     int            nb;
     int            E;           // outputs per tile
@@ -352,12 +385,17 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, sizeof(T) == 4 ?
     Ent<T>       *buf = reinterpret_cast<Ent<T> *>(smem_raw);
     cg::cluster_group cluster = cg::this_cluster();
     const int     c = (int) cluster.block_rank();
-    const int64_t tile = blockIdx.x / C;
     if (a.active && !a.active[blockIdx.y]) return;  // uniform over the cluster
     const T      *vin = a.vin + (int64_t) blockIdx.y * a.col_stride;
     T            *vout = a.vout + (int64_t) blockIdx.y * a.col_stride;
     const double *means = a.means ? a.means + (int64_t) blockIdx.y * a.nb : nullptr;
-
+    // every CTA of the cluster is running before any writes into another's shared memory
+    cluster_arrive_relaxed();
+    // One cluster per tile.  Each CTA asks L2 for its share of the input of the
+    // tile one wave later (a.ahead = the clusters resident at once), which a
+    // cluster of the next wave will load.
+    {
+    const int64_t tile = blockIdx.x / C;
     const int     blk = a.tile_block[tile];
     const int64_t bs = a.blk_start[blk];
     const int64_t be = bs + a.blk_len[blk];
@@ -365,8 +403,18 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, sizeof(T) == 4 ?
     const int64_t ws = (t0 - (a.lambda - 1)) & ~(int64_t) 1;  // even window start
     const bool    inside = ws >= bs && ws + 2LL * M <= be;
     const T       mu = means ? (T) means[blk] : (T) 0;
-    // every CTA of the cluster is running before any writes into another's shared memory
-    cluster_arrive_relaxed();
+    if (tile + a.ahead < a.n_tiles) {
+        const int64_t nt = tile + a.ahead;
+        const int     nblk = a.tile_block[nt];
+        const int64_t nbs = a.blk_start[nblk], nbe = nbs + a.blk_len[nblk];
+        const int64_t nws = (a.tile_start[nt] - (a.lambda - 1)) & ~(int64_t) 1;
+        // M1 runs of 2 NC samples, 128-byte lines; rows kept inside the next tile's block
+        constexpr int LINE = 128 / (int) sizeof(T), PER_RUN = 2 * NC / LINE;
+        for (int e = threadIdx.x; e < M1 * PER_RUN; e += NT) {
+            const int64_t r = nws + 2LL * (M2 * (e / PER_RUN) + c * NC) + (int64_t) (e % PER_RUN) * LINE;
+            if (r >= nbs && r < nbe) asm volatile("prefetch.global.L2 [%0];" ::"l"(vin + r));
+        }
+    }
 
     // ---- step A: columns (u, u + NC/2) of this CTA, M1-point DFT over n1, times W_M^(n2 k1)
     for (int u = threadIdx.x; u < NP; u += NT) {
@@ -424,7 +472,8 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, sizeof(T) == 4 ?
         const int   t = threadIdx.x;
         const int   spec = a.blk_spec[blk];
         const Ent<T> *hc = a.hc + ((size_t) spec * C + c) * (16 * NSET);
-        const Ent<T> *wk = a.wk + (size_t) c * (16 * NSET);
+        // W_N^k of lane r, k = r + M1 rev(p): W_N^r (per CTA) times W_{2 M2}^rev(p) (one table for all CTAs)
+        const Ent<T> wb = ldg_ent(a.wbase + c);
         CP<T>       v[16];
 #pragma unroll
         for (int i = 0; i < 16; i++) v[i] = ent2cp(buf[rpos(16 * t + i)]);
@@ -444,7 +493,9 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, sizeof(T) == 4 ?
                 z2 = CP<T>{pmk(plo(ea.x), phi(eb.x)), pmk(plo(ea.y), phi(eb.y))};
             }
             const Ent<T> h = ldg_ent(hc + i * NSET + t);  // (ca, cb), already / (4M)
-            const Ent<T> w = ldg_ent(wk + i * NSET + t);  // W_N^k
+            const auto   wr = __ldg(a.w8192 + i * NSET + t);
+            const CP<T>  wp = cpmul(CP<T>{wb.x, wb.y}, CP<T>{pdup<T>(wr.x), pdup<T>(wr.y)});
+            const Ent<T> w{wp.x, wp.y};  // W_N^k
             const CP<T>  z1 = v[i];
             const Pr<T>  e0x = padd(z1.x, z2.x), e0y = psub(z1.y, z2.y);
             const Pr<T>  o0x = padd(z1.y, z2.y), o0y = psub(z2.x, z1.x);
@@ -477,20 +528,21 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, sizeof(T) == 4 ?
         row_pass_inv_load<T, 4096>(buf, a.tw4096, v);
         cluster_arrive();
         cluster_wait();  // every CTA has read its rows: the buffers take the column layout
-        // value n2 = q + 256 n of rows (kA, kB) -> column n2 of CTA n2 / NC
-        const int q = threadIdx.x;
-        const int kA = c, kB = (c == 0) ? C : M1 - c;
+        // value n2 = q + 256 n of rows (kA, kB) -> column n2 of CTA n2 / NC.
+        // Columns u and u + NP (the two lanes of the destination's entry) are
+        // values n and n + NP/256 of this thread: one 16-byte store per row.
+        const int     q = threadIdx.x;
+        const int     kA = c, kB = (c == 0) ? C : M1 - c;
+        constexpr int DN = NP / 256;
 #pragma unroll
         for (int n = 0; n < 16; n++) {
+            if ((n / DN) % 2 != 0) continue;  // the upper half of a pair: stored with its lower half
             const int n2 = q + 256 * n;
-            const int d = n2 / NC, n2l = n2 % NC;
-            const int up = n2l % NP, half = n2l / NP;
-            T        *cb = reinterpret_cast<T *>(cluster.map_shared_rank(buf, d));
-            T        *ea = cb + 4 * (up * CS + kA), *eb = cb + 4 * (up * CS + kB);
-            ea[half] = plo(v[n].x);
-            ea[2 + half] = plo(v[n].y);
-            eb[half] = phi(v[n].x);
-            eb[2 + half] = phi(v[n].y);
+            const int d = n2 / NC, up = (n2 % NC) % NP;
+            Ent<T>   *cb = cluster.map_shared_rank(buf, d);
+            const CP<T> lo = v[n], hi = v[n + DN];
+            cb[up * CS + kA] = Ent<T>{pmk(plo(lo.x), plo(hi.x)), pmk(plo(lo.y), plo(hi.y))};
+            cb[up * CS + kB] = Ent<T>{pmk(phi(lo.x), phi(hi.x)), pmk(phi(lo.y), phi(hi.y))};
         }
     }
     cluster_arrive();
@@ -505,6 +557,8 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, sizeof(T) == 4 ?
             // DIT input order: v[i] holds k1 = rev(i), times conj(W_M^(n2 k1))
 #pragma unroll
             for (int i = 0; i < M1; i++) v[i] = ent2cp(buf[u * CS + rev_bits_c(i, LOGM1)]);
+            // (last column pair of the thread) this CTA's buffer may take the next tile's rows
+            if (u + NT >= NP) cluster_arrive();
             const double2 wa = __ldg(a.twM + n2a), wb = __ldg(a.twM + n2b);
             apply_powers<T, M1, true>(v, CP<T>{pmk((T) wa.x, (T) wb.x), pmk((T) wa.y, (T) wb.y)});
         }
@@ -529,6 +583,8 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, sizeof(T) == 4 ?
             }
         }
     }
+    }
+    cluster_wait();  // matches the arrive after the column reads
 }
 
 // ------------------------------------------------------------------ tables
@@ -560,11 +616,23 @@ static void cexp_ld(long double num, long double den, double *re, double *im) {
     *im = (double) sinl(ang);
 }
 
+// sets the kernel's shared-memory limit and returns how many clusters fit on the device at once
 template <typename T, int C>
-static int ninv4_setup_kernel() {
+static int ninv4_setup_kernel(int *max_clusters) {
     constexpr size_t smem = sizeof(Ent<T>) * buf_entries<C>();
     MDP_CUDA(cudaFuncSetAttribute((const void *) ninv4_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int) smem));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C * 256);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = smem;
+    int n = 0;
+    MDP_CUDA(cudaOccupancyMaxActiveClusters(&n, (void *) ninv4_kernel<T, C>, &cfg));
+    if (n < 1) {
+        mdp_set_error("cluster four-step tiles: no %d-CTA cluster fits on this device", C);
+        return MDP_EUNSUPPORTED;
+    }
+    *max_clusters = n;
     return MDP_OK;
 }
 
@@ -578,7 +646,8 @@ size_t ninv4_smem(int C) {
     return 0;
 }
 
-// The plan's tables: P.ttw = wk [C][16][256] Ent<T>, P.twm = W_M^n2 [M2]
+// The plan's tables: P.ttw = the per-CTA twist factors [C] Ent<T>, P.wa = W_{2 M2}^rev(p) [16][256]
+// (T2), P.twm = W_M^n2 [M2]
 // double2, P.ltw = W_4096^q [256] double2, P.spectra = hc [n_spec][C][16][256]
 // Ent<T> (from the FP64 spectra H of each distinct row when `spectra`, else
 // zero).  Tiles are laid as for the split plans (one output fewer than the
@@ -588,24 +657,32 @@ int ninv4_build(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, bool spectra) 
     const int C = P.cluster, M1 = 2 * C, M = M1 * M2, Nn = 2 * M;
     if (C != 2 && C != 4 && C != 8) return MDP_EUNSUPPORTED;
     const size_t ne = (size_t) C * 16 * NSET;
-    // wk: W_N^k of every (CTA, position, lane)
+    // W_N^k of lane r at position p (k = r + M1 rev(p)) = W_N^r W_{2 M2}^rev(p): the per-CTA
+    // factors (ttw) and one table in the order the untangle pass reads it (wa)
     {
-        std::vector<Ent<T>> wk(ne);
-        std::vector<T>      raw(4 * ne);
-        for (size_t e = 0; e < ne; e++) {
-            const int c = (int) (e / (16 * NSET)), i = (int) (e / NSET) % 16, t = (int) (e % NSET);
-            const int p = 16 * t + i, k2 = rev_bits_c(p, LOGM2);
+        std::vector<T> base(4 * C);
+        for (int c = 0; c < C; c++) {
             const int rA = c, rB = (c == 0) ? C : M1 - c;
             double    ar, ai, br, bi;
-            cexp_ld(rA + (long double) M1 * k2, Nn, &ar, &ai);
-            cexp_ld(rB + (long double) M1 * k2, Nn, &br, &bi);
-            raw[4 * e + 0] = (T) ar;
-            raw[4 * e + 1] = (T) br;
-            raw[4 * e + 2] = (T) ai;
-            raw[4 * e + 3] = (T) bi;
+            cexp_ld(rA, Nn, &ar, &ai);
+            cexp_ld(rB, Nn, &br, &bi);
+            base[4 * c + 0] = (T) ar;
+            base[4 * c + 1] = (T) br;
+            base[4 * c + 2] = (T) ai;
+            base[4 * c + 3] = (T) bi;
         }
-        MDP_TRY(P.ttw.alloc(sizeof(Ent<T>) * ne));
-        MDP_CUDA(cudaMemcpy(P.ttw.p, raw.data(), sizeof(T) * raw.size(), cudaMemcpyHostToDevice));
+        MDP_TRY(P.ttw.alloc(sizeof(Ent<T>) * C));
+        MDP_CUDA(cudaMemcpy(P.ttw.p, base.data(), sizeof(T) * base.size(), cudaMemcpyHostToDevice));
+        std::vector<T> w(2 * 16 * NSET);
+        for (int i = 0; i < 16; i++)
+            for (int t = 0; t < NSET; t++) {
+                double re, im;
+                cexp_ld(rev_bits_c(16 * t + i, LOGM2), 2 * M2, &re, &im);
+                w[2 * (i * NSET + t)] = (T) re;
+                w[2 * (i * NSET + t) + 1] = (T) im;
+            }
+        MDP_TRY(P.wa.alloc(sizeof(T) * w.size()));
+        MDP_CUDA(cudaMemcpy(P.wa.p, w.data(), sizeof(T) * w.size(), cudaMemcpyHostToDevice));
     }
     {
         std::vector<double2> tm(M2), t4(256);
@@ -637,9 +714,9 @@ int ninv4_build(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, bool spectra) 
         MDP_CUDA(cudaMemset(P.spectra.p, 0, sizeof(Ent<T>) * ne * std::max(N->n_spec, 1)));
     }
     switch (C) {
-        case 2: MDP_TRY((ninv4_setup_kernel<T, 2>())); break;
-        case 4: MDP_TRY((ninv4_setup_kernel<T, 4>())); break;
-        case 8: MDP_TRY((ninv4_setup_kernel<T, 8>())); break;
+        case 2: MDP_TRY((ninv4_setup_kernel<T, 2>(&P.threads))); break;
+        case 4: MDP_TRY((ninv4_setup_kernel<T, 4>(&P.threads))); break;
+        case 8: MDP_TRY((ninv4_setup_kernel<T, 8>(&P.threads))); break;
     }
     return MDP_OK;
 }
@@ -658,10 +735,12 @@ int ninv4_launch(mdp_context *ctx, const mdp_noise *N, const mdp_tile_plan &P, c
     a.blk_len = N->blk_len.as<int32_t>();
     a.blk_spec = N->blk_spec.as<int32_t>();
     a.hc = P.spectra.as<Ent<T>>();
-    a.wk = P.ttw.as<Ent<T>>();
+    a.wbase = P.ttw.as<Ent<T>>();
+    a.w8192 = static_cast<const typename std::conditional<sizeof(T) == 4, float2, double2>::type *>(P.wa.p);
     a.twM = P.twm.as<double2>();
     a.tw4096 = P.ltw.as<double2>();
     a.means = d_means;
+    a.n_tiles = P.n_tiles;
     a.lambda = N->lambda;
     a.nb = N->nb;
     a.E = P.fft_n - 2 * (N->lambda - 1) - 1;
@@ -669,9 +748,11 @@ int ninv4_launch(mdp_context *ctx, const mdp_noise *N, const mdp_tile_plan &P, c
              (reinterpret_cast<uintptr_t>(d_out) % (2 * sizeof(T)) == 0) && (col_stride % 2 == 0);
     a.col_stride = col_stride;
     a.active = d_active;
+    // one cluster per tile; P.threads holds how many clusters are resident at once
+    a.ahead = std::max(P.threads, 1);
     const int64_t nblk = P.n_tiles * C;
     if (nblk > 0x7fffffffLL) return MDP_EUNSUPPORTED;
-    dim3   grid((unsigned) nblk, (unsigned) ncols);
+    dim3 grid((unsigned) nblk, (unsigned) ncols);
     size_t smem = ninv4_smem<T>(C);
     switch (C) {
         case 2: ninv4_kernel<T, 2><<<grid, NT, smem, ctx->stream>>>(a); break;

@@ -677,20 +677,29 @@ __global__ void __launch_bounds__(32) bin_chunk_scatter_kernel(const int32_t *__
         __syncwarp();
     }
     const unsigned below = (1u << lane_id()) - 1u;
-    for (int64_t t0 = r0; t0 < r1; t0 += 32) {
-        const int64_t t = t0 + lane_id();
-        const int32_t o = (t < r1) ? off[t] : -1;
-        const int     b = (o >= 0) ? o / bin3 : -1;
-        const unsigned peers = __match_any_sync(0xffffffffu, b);
-        const int      leader = __ffs(peers) - 1;
-        uint32_t       base = 0;
-        if (b >= 0 && lane_id() == leader) {
-            base = cur[b];
-            cur[b] = base + (uint32_t) __popc(peers);
+    constexpr int  U = 8;  // steps of 32 rows whose offsets are loaded ahead
+    for (int64_t t0 = r0; t0 < r1; t0 += 32 * U) {
+        int32_t o[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int64_t t = t0 + 32 * u + lane_id();
+            o[u] = (t < r1) ? off[t] : -1;
         }
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (b >= 0) perm[base + __popc(peers & below)] = (uint32_t) t;
-        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int64_t  t = t0 + 32 * u + lane_id();
+            const int      b = (o[u] >= 0) ? o[u] / bin3 : -1;
+            const unsigned peers = __match_any_sync(0xffffffffu, b);
+            const int      leader = __ffs(peers) - 1;
+            uint32_t       base = 0;
+            if (b >= 0 && lane_id() == leader) {
+                base = cur[b];
+                cur[b] = base + (uint32_t) __popc(peers);
+            }
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (b >= 0) perm[base + __popc(peers & below)] = (uint32_t) t;
+            __syncwarp();
+        }
     }
 }
 
@@ -703,8 +712,9 @@ int mdp_build_bins(mdp_context *ctx, mdp_pointing *A, int bin_pix, mdp_pt_bins *
         mdp_set_error("P^T bins: %lld rows exceed 32-bit row indices", (long long) A->m);
         return MDP_EUNSUPPORTED;
     }
-    // row chunks: at least 2^20 rows, at most 2^26 (chunk, bin) counters
-    int64_t chunk = 1 << 20;
+    // row chunks (one warp each for the scatter): at least 2^14 rows, at most
+    // 2^26 (chunk, bin) counters
+    int64_t chunk = 1 << 14;
     while (((A->m + chunk - 1) / chunk) * std::max<int64_t>(nb, 1) > (1LL << 26)) chunk <<= 1;
     const int64_t nch = std::max<int64_t>((A->m + chunk - 1) / chunk, 1);
     DevBuf        count, tot, start;

@@ -1108,9 +1108,9 @@ static int ceil_log2_i(int64_t v) {
     return b;
 }
 
-// The cluster four-step tiles join the automatic choice once validated; until
-// then they are reached through mdp_noise_set_plan only.
-static const bool g_cluster4_auto = false;
+// The cluster four-step tiles are candidates of the automatic choice (the
+// autotuner times them with the others).
+static const bool g_cluster4_auto = true;
 
 // every launchable configuration whose tile holds the band (E >= 1)
 template <typename T>
@@ -1273,8 +1273,8 @@ static int parse_plan(const char *plan, int lambda, TileCand *out) {
         ok = sscanf(plan, "%d,%d,%d", &c.log_ml, &c.C, &c.threads) == 3 && pick_kernel<T>(c.log_ml, c.C) &&
              c.threads >= 32 && c.threads <= 512 && !(c.threads & 31);
     }
-    if (!ok || cand_E(c, lambda) < 1) {
-        mdp_set_error("invalid tile plan '%s' for lambda=%d", plan, lambda);
+    if (!ok || cand_E(c, lambda) < 1 || 8 * cand_E(c, lambda) < cand_N(c)) {
+        mdp_set_error("invalid tile plan '%s' for lambda=%d (or under an eighth of its tile useful)", plan, lambda);
         return MDP_EINVAL;
     }
     *out = c;

@@ -122,4 +122,4 @@ def test_fp32_operator_ragged_blocks(gpu_ctx, sizes, plan):
         torch.cuda.synchronize()
         outs.append(q.cpu().numpy())
     assert _rel(outs[0], ref) < 1e-5, _rel(outs[0], ref)
-    assert np.array_equal(outs[1], outs[0])  # every addition of the operator is in a fixed order
+    assert _rel(outs[1], outs[0]) < 1e-12  # below 2^20 rows P^T adds with atomics

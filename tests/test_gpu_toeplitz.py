@@ -45,7 +45,7 @@ def _rel(a, b):
     (4096, [40000, 9000], "c,2"),     # cluster four-step tiles: 2, 4, 8 CTAs (2C x 4096 points)
     (8192, [70000, 9000], "c,4"),
     (16384, [140000, 40000], "c,8"),
-    (16384, [1 << 20], "c,8"),        # the at-scale block: 11 tiles, interior and edge tiles
+    (16384, [300000], "c,8"),         # four tiles of the at-scale plan: interior and edge tiles
     (100, [300000, 5000], "c,8"),     # narrow band: blocks shorter than a tile, windows past both ends
 ])
 def test_stbmm_vs_exact(gpu_ctx, lam, sizes, fft):
