@@ -103,6 +103,15 @@ def parse():
     return ap.parse_args()
 
 
+_T0 = time.perf_counter()
+
+
+def log(msg: str):
+    """Progress of the run on stderr (the JSON line stays the only stdout)."""
+    sys.stderr.write(f"[bench +{time.perf_counter() - _T0:7.1f} s] {msg}\n")
+    sys.stderr.flush()
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -257,6 +266,7 @@ def bench_multi(args, device):
                                                       maxiter=MAXITER, slots=0, use_graph=True)
     torch.cuda.synchronize()
     t_multi = time.perf_counter() - t0
+    log(f"multi-RHS solve: {args.multi_rhs} columns in {t_multi:.2f} s")
     launches = ctx.launches - l0
     xs = x[: min(args.multi_fp64_cols, args.multi_rhs)].cpu().numpy()
     del x
@@ -275,6 +285,7 @@ def bench_multi(args, device):
         x1 = x1.cpu().numpy()
         # FP64 oracle of the column: the plain FP64 path at tol 1e-12 (untimed)
         xo = mb.gls_solve(ctx, P1, N1, sig, nz, tol=1e-12, maxiter=4 * MAXITER)[0].cpu().numpy()
+        log(f"multi-RHS part: FP64 column {c} and its oracle done")
         for tag, xv in (("multi_mixed", xs[c]), ("fp64_path", x1)):
             for k, name in enumerate("IQU"):
                 errs[tag][name] = max(errs[tag][name],
@@ -423,8 +434,11 @@ def bench_fknee(args, device):
 def run_part(fn, args, device):
     """One auxiliary part of the bench line; a part that fails is reported on
     the line (its error) instead of ending the run without a line."""
+    log(f"{fn.__name__}: start")
     try:
-        return fn(args, device)
+        out = fn(args, device)
+        log(f"{fn.__name__}: done")
+        return out
     except Exception as ex:  # noqa: BLE001
         import torch
         torch.cuda.synchronize()
@@ -650,6 +664,7 @@ def bench_serving(args, device):
         for tk in warm:
             tk.wait(1800.0)
     t_pre = time.perf_counter() - t0
+    log(f"serving: datasets preloaded, slots warm ({t_pre:.1f} s)")
     out = {"requests": n, "rate_per_s": args.serve_rate, "datasets": len(specs), "slots": args.serve_slots,
            "dataset_samples": [s.n_samples for s in specs], "preload_and_warmup_s": round(t_pre, 2)}
     res = {}
@@ -664,6 +679,7 @@ def bench_serving(args, device):
             st["error_samples"] = sorted({x.error for x in r if x.error})[:4]
         out[prec] = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in st.items()}
         res[prec] = r
+        log(f"serving: {prec} stream done")
     # the same stream offered at half the FP64 path's measured throughput, so that
     # p50/p99 measure service time rather than the growth of a queue
     rate2 = round(0.5 * out["fp64"]["solves_per_s"], 2)
@@ -727,8 +743,10 @@ def main():
     from midapack_b200 import synth
     cfg = dict(synth.CONFIGS[args.config])
     cfg["seed"] = cfg["seed"] + rank
+    log(f"workload {args.config}: generating")
     wl = synth.make_workload_torch(args.config, **cfg)
     torch.cuda.synchronize()
+    log("workload ready")
     ns = wl.n_samples
     nb = len(wl.block_sizes)
     idv = np.arange(nb, dtype=np.int64) * wl.block_len
@@ -747,9 +765,10 @@ def main():
     if world > 1 and not args.replicas:
         return run_sharded(args, wl, ctx, rank, world, local, idv)
 
-    for _ in range(args.warmup):
+    for k in range(args.warmup):
         one_solve()
-    torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        log(f"warm-up solve {k + 1}/{args.warmup} ({args.precision})")
     if world > 1:
         torch.distributed.barrier()
     launches0 = ctx.launches
@@ -767,6 +786,7 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
+    log(f"timed solves done ({args.steps})")
     ms = e0.elapsed_time(e1) / args.steps
     prof = ctx.profile_read()
     ctx.profile(False)
@@ -794,6 +814,7 @@ def main():
         e3.record(stream)
         torch.cuda.synchronize()
         oms = e2.elapsed_time(e3) / args.steps
+        log(f"timed solves done ({oprec})")
         if world > 1:
             t = torch.tensor([oms], device="cuda", dtype=torch.float64)
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -844,7 +865,9 @@ def main():
     # the reference's CPU path on a bounded sample (before any large host allocation)
     cpu = None
     if rank == 0 and not args.no_cpu and world == 1:
+        log("cpu baseline: start")
         cpu = run_cpu_baseline(wl, cpu_sample(wl), REFERENCE_ITERATIONS, ns)
+        log("cpu baseline: done")
     # pinned host inputs for the end-to-end run
     pinned = None
     if not args.no_e2e:
@@ -861,9 +884,12 @@ def main():
     e2e = None
     if pinned:
         try:
+            log("e2e: start")
             e2e = run_e2e_device_api(args, wl, world, pinned)
+            log("e2e (device API): done")
             # the reference's own entry point (MLmap: FP64, host maps out) on the same inputs
             e2e["mlmap_fp64"] = run_e2e(args, wl, world, pinned)
+            log("e2e (MLmap_b200): done")
         except Exception as ex:  # noqa: BLE001 - reported on the line
             sys.stderr.write(f"e2e failed: {type(ex).__name__}: {ex}\n")
             e2e = dict(e2e or {"value": None, "unit": "s"}, error=f"{type(ex).__name__}: {ex}")

@@ -32,14 +32,35 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
         "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
         "-I", os.path.join(ROOT, "include"), "-I", CSRC,
     ] + (extra or [])
-    objs = []
+    # an object is rebuilt when its source, a shared header or the flags changed
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    inc = os.path.join(ROOT, "include")
+    headers += [os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h")]
+    newest_header = max((os.path.getmtime(h) for h in headers), default=0.0)
+    flags_file = os.path.join(objdir, "flags.txt")
+    flags = " ".join(common)
+    same_flags = os.path.exists(flags_file) and open(flags_file).read() == flags
+    jobs, objs = [], []
     for src in SOURCES:
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
-        cmd = [nvcc(), "-c", os.path.join(CSRC, src), "-o", obj] + common
+        objs.append(obj)
+        path = os.path.join(CSRC, src)
+        if (same_flags and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(path)
+                and os.path.getmtime(obj) >= newest_header):
+            continue
+        jobs.append([nvcc(), "-c", path, "-o", obj] + common)
+
+    def run(cmd):
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-        objs.append(obj)
+
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(run, c) for c in jobs]:
+            f.result()
+    with open(flags_file, "w") as f:
+        f.write(flags)
     link = [nvcc(), "-shared", "-o", LIB] + objs + [
         "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "shared",
         "-Xlinker", "-rpath,/usr/local/cuda/lib64"]

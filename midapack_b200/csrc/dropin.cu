@@ -624,6 +624,18 @@ static void write_residuals(const char *outpath, const char *ref, const std::vec
     fclose(f);
 }
 
+// ECG_GLS's relative residuals (ecg.c:156-161): <outpath>/rel_res_<ref>_enlfac_<t>_o=<ortho_alg>.txt
+static void write_ecg_residuals(const char *outpath, const char *ref, const std::vector<double> &res, int iters,
+                                int enl_fac, int ortho_alg) {
+    if (!outpath || !ref) return;
+    char fn[4096];
+    snprintf(fn, sizeof(fn), "%s/rel_res_%s_enlfac_%d_o=%d.txt", outpath, ref, enl_fac, ortho_alg);
+    FILE *f = fopen(fn, "w");
+    if (!f) return;
+    for (int i = 0; i <= iters && i < (int) res.size(); i++) fprintf(f, "%.15e\n", res[i]);
+    fclose(f);
+}
+
 extern "C" int PCG_GLS_true(char *outpath, char *ref, Mat *A, Tpltz *Nm1, double *x, double *b, double *noise,
                             double *cond, int *lhits, double tol, int K, int precond, int Z_2lvl) {
     if (precond < 0 || precond > 2) {
@@ -713,15 +725,7 @@ extern "C" int ECG_GLS(char *outpath, char *ref, Mat *A, Tpltz *Nm1, double *x, 
     cudaMemcpy(lhits, bj.hits.p, 4 * bj.npix, cudaMemcpyDeviceToHost);
     printf("*** ECG: %d iterations, relative residual %e (%s)\n", info.iterations, std::sqrt(info.res / info.res0),
            info.converged ? "converged" : "not converged");
-    if (outpath && ref) {
-        char fn[4096];
-        snprintf(fn, sizeof(fn), "%s/rel_res_%s_enlfac_%d_o=%d.txt", outpath, ref, enlFac, ortho_alg);
-        FILE *f = fopen(fn, "w");
-        if (f) {
-            for (int i = 0; i <= info.iterations; i++) fprintf(f, "%.15e\n", res[i]);
-            fclose(f);
-        }
-    }
+    write_ecg_residuals(outpath, ref, res, info.iterations, enlFac, ortho_alg);
     return 0;
 }
 
@@ -750,7 +754,7 @@ static int mlmap_device(int m, int nb, const int *blocks, const int *pix, const 
                         int precond, int z_2lvl, int solver, int enl_fac, int ortho_alg, int bs_red,
                         std::vector<double> &x, std::vector<int> &lstid, std::vector<double> &cond,
                         std::vector<int> &hits, int *iters, double *res_rel,
-                        const mdp_template_scan *scan = nullptr) {
+                        const mdp_template_scan *scan = nullptr, std::vector<double> *res_hist = nullptr) {
     mdp_context *ctx = default_ctx();
     if (!ctx) return MDP_ECUDA;
     const int64_t n3 = 3LL * m;
@@ -819,6 +823,7 @@ static int mlmap_device(int m, int nb, const int *blocks, const int *pix, const 
         if (cudaStreamSynchronize(st) != cudaSuccess) rc = MDP_ECUDA;
         if (iters) *iters = info.iterations;
         if (res_rel) *res_rel = std::sqrt(info.res / info.res0);
+        if (res_hist) *res_hist = res;
     }
     mdp_pointing_destroy(P);
     mdp_noise_destroy(N);
@@ -940,7 +945,7 @@ extern "C" void MLmap(MPI_Comm comm, char *outpath, char *ref, int solver, int p
     }
     const int m = ((int *) data_size_proc)[0];
     printf("\n############# MAPPRAISER (midapack_b200, one GPU) ################\n");
-    std::vector<double> x, cond;
+    std::vector<double> x, cond, hist;
     std::vector<int>    lstid, hits;
     int                 it = 0;
     double              rr = 0;
@@ -949,12 +954,18 @@ extern "C" void MLmap(MPI_Comm comm, char *outpath, char *ref, int solver, int p
         std::lock_guard<std::mutex> lk(g_mu);
         rc = mlmap_device(m, nb_blocks_loc, (const int *) local_blocks_sizes, (const int *) pix,
                           (const double *) pixweights, (const double *) signal, noise, lambda, invtt, tol, maxiter, 1,
-                          precond, Z_2lvl, solver, enlFac, ortho_alg, bs_red, x, lstid, cond, hits, &it, &rr);
+                          precond, Z_2lvl, solver, enlFac, ortho_alg, bs_red, x, lstid, cond, hits, &it, &rr, nullptr,
+                          &hist);
     }
     if (rc) {
         fail("MLmap", rc);
         return;
     }
+    // the residual history the reference's solver writes (PCG_GLS_true,
+    // pcg_true.c:119-123,195: one double per iteration from k = 0; ECG_GLS,
+    // ecg.c:156-161: one line per iteration)
+    if (solver == 0) write_residuals(outpath, ref, hist, it < maxiter ? it : maxiter - 1);
+    else write_ecg_residuals(outpath, ref, hist, it, enlFac, ortho_alg);
     write_maps(outpath, ref, nside, x, lstid, cond, hits, "MLmap");
     printf("[midapack_b200] %d iterations, final res_rel %e\n", it, rr);
 }
@@ -1014,7 +1025,7 @@ extern "C" void MTmap(MPI_Comm comm, char *outpath, char *ref, int solver, int p
                               sw.data(), ground ? azf.data() : nullptr, ground ? az_min : nullptr,
                               ground ? az_max : nullptr, nhwp ? hwpf.data() : nullptr};
     printf("\n############# MAPPRAISER MTmap (midapack_b200, one GPU) ################\n");
-    std::vector<double> x, cond;
+    std::vector<double> x, cond, hist;
     std::vector<int>    lstid, hits;
     int                 it = 0;
     double              rr = 0;
@@ -1023,12 +1034,14 @@ extern "C" void MTmap(MPI_Comm comm, char *outpath, char *ref, int solver, int p
         std::lock_guard<std::mutex> lk(g_mu);
         rc = mlmap_device(m, nb_blocks_loc, blocks, (const int *) pix, (const double *) pixweights,
                           (const double *) signal, noise, 1, invtt, tol, maxiter, 1, 0, 0, 0, 1, 1, 0, x, lstid, cond,
-                          hits, &it, &rr, &scan);
+                          hits, &it, &rr, &scan, &hist);
     }
     if (rc) {
         fail("MTmap", rc);
         return;
     }
+    // PCG_GLS_templates' residual history (pcg_true.c:415-420,520-523)
+    write_residuals(outpath, ref, hist, it < maxiter ? it : maxiter - 1);
     write_maps(outpath, ref, nside, x, lstid, cond, hits, "MTmap");
     printf("[midapack_b200] %d iterations, final res_rel %e\n", it, rr);
 }

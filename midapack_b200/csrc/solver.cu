@@ -155,7 +155,12 @@ static int localW_launch(mdp_context *ctx, mdp_pointing *A, const mdp_noise *N, 
         MDP_CHECK_LAUNCH(ctx);
         return MDP_OK;
     }
-    MDP_TRY(localW_launch(ctx, A, N, d_W, d_hits));
+    MDP_CUDA(cudaMemsetAsync(d_W, 0, 72 * npix, st));
+    MDP_CUDA(cudaMemsetAsync(d_hits, 0, 4 * npix, st));
+    localW_kernel<<<grid_for(A->m, 256, ctx->sm_count * 16), 256, 0, st>>>(
+            A->off.as<int32_t>(), A->values, A->m, N->blk_start.as<int64_t>(), N->blk_len.as<int32_t>(),
+            N->blk_t0.as<double>(), N->nb, d_W, d_hits);
+    MDP_CHECK_LAUNCH(ctx);
     return MDP_OK;
 }
 
