@@ -98,6 +98,8 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=50.0, help="mean Poisson arrival rate, solves/s")
     ap.add_argument("--serve-datasets", type=int, default=16)
     ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--ninv-plan", default="", help="force the FP64 N^-1 tile plan of the headline solves (profiling)")
+    ap.add_argument("--ninv-plan32", default="", help="force the FP32 N^-1 tile plan of the headline solves (profiling)")
     ap.add_argument("--replicas", action="store_true",
                     help="with N > 1 ranks: N independent solves instead of one solve sharded over the ranks")
     return ap.parse_args()
@@ -755,6 +757,10 @@ def main():
     def one_solve(precision=args.precision):
         P = mb.Pointing(ctx, wl.pix, wl.weights, ns, 3)
         N = mb.Noise(ctx, wl.block_sizes, wl.lam, wl.invtt, idv=idv)
+        if args.ninv_plan:
+            N.set_plan(args.ninv_plan, fp32=False)
+        if args.ninv_plan32:
+            N.set_plan(args.ninv_plan32, fp32=True)
         if precision == "mixed":
             out = mb.gls_solve_mixed(ctx, P, N, wl.signal, wl.noise, tol=TOL, maxiter=MAXITER,
                                      inner_tol=args.inner_tol)

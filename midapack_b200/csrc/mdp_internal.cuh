@@ -244,6 +244,8 @@ int mdp_circulant_spectrum(mdp_context *ctx, const double *h_T, int lambda, int 
 // H[k], k = 0..Nn/2, of the Nn-point circulant embedding of the band T (device,
 // FP64); d_tw = exp(-2 pi i k / Nn), k < Nn/2
 int mdp_spectrum_H(mdp_context *ctx, const double *h_T, int lambda, int Nn, const double2 *d_tw, double *d_H);
+// exp(-2 pi i num / den) from long double (a table lookup for power-of-two den <= 2^19)
+void mdp_host_cexp(long double num, long double den, double *re, double *im);
 // cluster four-step tiles of N^-1 (ninv4.cu): tables of a plan, launch
 template <typename T>
 int ninv4_build(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, bool spectra);

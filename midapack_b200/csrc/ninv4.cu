@@ -610,11 +610,7 @@ __global__ void ninv4_hc_kernel(const double *__restrict__ H, int C, Ent<T> *__r
 }  // namespace
 
 // ------------------------------------------------------------------ host side
-static void cexp_ld(long double num, long double den, double *re, double *im) {
-    const long double ang = -2.0L * 3.14159265358979323846264338327950288L * num / den;
-    *re = (double) cosl(ang);
-    *im = (double) sinl(ang);
-}
+static void cexp_ld(long double num, long double den, double *re, double *im) { mdp_host_cexp(num, den, re, im); }
 
 // sets the kernel's shared-memory limit and returns how many clusters fit on the device at once
 template <typename T, int C>

@@ -904,13 +904,57 @@ __global__ void split_pairs_kernel(const double *__restrict__ H, int M, const in
 }
 
 // exp(-2 pi i num / den) in long double, rounded to V
-static inline void host_cexp(long double num, long double den, double2 *o) {
+// exp(-2 pi i k / 2^LOG_ROOTS), k < 2^LOG_ROOTS, in long double: computed once per
+// process, so that plan tables (all of them W_den^num with den a power of two
+// up to 2^LOG_ROOTS) are lookups.  The angle 2 pi num/den equals 2 pi k/2^LOG_ROOTS
+// exactly for k = num 2^LOG_ROOTS / den, so a lookup returns the same value
+// as evaluating cosl/sinl directly.
+constexpr int LOG_ROOTS = 19;
+struct RootTable {
+    std::vector<long double> re, im;
+    RootTable() : re(1u << LOG_ROOTS), im(1u << LOG_ROOTS) {
+        const long double two_pi = 2.0L * 3.14159265358979323846264338327950288L;
+        for (uint32_t k = 0; k < (1u << LOG_ROOTS); k++) {
+            const long double ang = -two_pi * (long double) k / (long double) (1u << LOG_ROOTS);
+            re[k] = cosl(ang);
+            im[k] = sinl(ang);
+        }
+    }
+};
+static const RootTable &root_table() {
+    static const RootTable t;  // thread-safe one-time initialisation
+    return t;
+}
+static inline void host_cexp_ld(long double num, long double den, long double *re, long double *im) {
+    if (den >= 1.0L && den <= (long double) (1u << LOG_ROOTS) && num >= 0.0L && num == floorl(num)) {
+        const uint64_t d = (uint64_t) den, n = (uint64_t) num;
+        if ((long double) d == den && (d & (d - 1)) == 0) {
+            const uint64_t   k = (n % d) * ((1ull << LOG_ROOTS) / d);
+            const RootTable &t = root_table();
+            *re = t.re[k];
+            *im = t.im[k];
+            return;
+        }
+    }
     const long double ang = -2.0L * 3.14159265358979323846264338327950288L * num / den;
-    *o = make_double2((double) cosl(ang), (double) sinl(ang));
+    *re = cosl(ang);
+    *im = sinl(ang);
+}
+void mdp_host_cexp(long double num, long double den, double *re, double *im) {
+    long double r, i;
+    host_cexp_ld(num, den, &r, &i);
+    *re = (double) r;
+    *im = (double) i;
+}
+static inline void host_cexp(long double num, long double den, double2 *o) {
+    long double re, im;
+    host_cexp_ld(num, den, &re, &im);
+    *o = make_double2((double) re, (double) im);
 }
 static inline void host_cexp(long double num, long double den, float2 *o) {
-    const long double ang = -2.0L * 3.14159265358979323846264338327950288L * num / den;
-    *o = make_float2((float) cosl(ang), (float) sinl(ang));
+    long double re, im;
+    host_cexp_ld(num, den, &re, &im);
+    *o = make_float2((float) re, (float) im);
 }
 
 int mdp_circulant_spectrum(mdp_context *ctx, const double *h_T, int lambda, int bs, double *h_F) {
