@@ -203,6 +203,9 @@ NINV_TRAFFIC_PER_TILE = {("f32", 256, 256): 1857072128 / 704,   # profiles/ninv_
 
 
 def ninv_kernel(t: dict, prec: str) -> str:
+    if t.get("cluster_four_step"):
+        m1, m2 = t["cluster_four_step"]
+        return f"ninv4_kernel<{prec}, {t['cluster']}> ({m1}x{m2} cluster four-step tiles)"
     if t.get("split"):
         m1, m2 = t["split"]
         return f"split_cols_kernel + split_rows_kernel + split_cols_kernel<{prec}> ({m1}x{m2} four-step tiles)"
@@ -840,14 +843,14 @@ def main():
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     achieved = ab[dom] / (per[dom] * 1e-3) / 1e9
     kname = {"P": "matvec_chunk_sums_kernel", "Ninv": ninv_kernel(tile, "double"),
-             "Pt": "trmatvec_binned_kernel"}
+             "Pt": "trmatvec_slices_kernel<double, double> + pt_partial_sum_kernel"}
     ninv_tile, ninv_prec = tile, "f64"
     if args.precision == "mixed":
         t32 = N.tile_fp32()
         ab = algorithmic_bytes32(ns, n_map, (t32["n_tiles"], t32["fft_n"] // 2))
         tile = {"fp64": tile, "fp32": t32}
         kname = {"P": "matvec32_chunk_sums4_kernel", "Ninv": ninv_kernel(t32, "float"),
-                 "Pt": "trmatvec32_binned_kernel"}
+                 "Pt": "trmatvec_slices_kernel<float, float> + pt_partial_sum_kernel"}
         ninv_tile, ninv_prec = t32, "f32"
         dom = max(("P", "Ninv", "Pt"), key=lambda k: per[k])
         achieved = ab[dom] / (per[dom] * 1e-3) / 1e9
@@ -866,7 +869,7 @@ def main():
         roofline["limiter"] = ("not DRAM (1.8-2.7 TB/s of DRAM traffic, ~3x the algorithmic bytes from the "
                                "four-step scratch): instruction issue in the row and inverse-column passes (issue "
                                "slot ~65 % busy, top stall 'not selected') and load latency in the forward-column "
-                               "pass; profiles/ninv_split_fp32_256x512_sections.md")
+                               "pass (ncu)")
 
     # the reference's CPU path on a bounded sample (before any large host allocation)
     cpu = None

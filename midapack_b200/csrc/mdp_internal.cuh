@@ -112,6 +112,20 @@ struct mdp_pt_bins {
     int64_t nbins = 0;
     DevBuf  start;   // int64 [nbins+1] offsets into perm
     DevBuf  perm;    // uint32 [valid rows] sample index, grouped by bin
+    // slices of the bins' lists (P^T): every bin's list cut into runs of at
+    // most slice_len rows (one run for an empty bin); a bin of one slice is
+    // written by it, the slices of a longer bin write partial maps that are
+    // then summed in slice order.  The partial buffer belongs to the pointing:
+    // two P^T of one pointing must not run at the same time.
+    int64_t nslices = 0, nmulti = 0, slice_len = 0;
+    DevBuf  slice_bin;    // int32 [nslices]
+    DevBuf  slice_lo;     // uint32 [nslices] first list entry
+    DevBuf  slice_hi;     // uint32 [nslices] one past the last
+    DevBuf  slice_out;    // int32 [nslices] -1: the bin's map entries, else its row of `partial`
+    DevBuf  multi_bin;    // int32 [nmulti] bins of several slices
+    DevBuf  multi_first;  // int32 [nmulti] their first row of `partial`
+    DevBuf  multi_n;      // int32 [nmulti] and how many
+    DevBuf  partial;      // double [rows][3 bin_pix]
 };
 
 struct mdp_pointing {
@@ -252,6 +266,10 @@ int ninv4_build(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, bool spectra);
 template <typename T>
 int ninv4_launch(mdp_context *ctx, const mdp_noise *N, const mdp_tile_plan &P, const T *d_in, T *d_out,
                  const double *d_means, int ncols, int64_t col_stride, const int *d_active);
+// dynamic shared memory of a cluster four-step CTA, and the largest a B200 CTA may use
+template <typename T>
+size_t ninv4_smem(int C);
+#define NINV4_SMEM_MAX ((size_t) 227 * 1024)
 int mdp_matvec_blockmeans(mdp_context *ctx, const mdp_pointing *A, const mdp_noise *N, const double *d_x,
                           double *d_y);
 // FP32 operator pieces (mixed precision)
@@ -275,7 +293,7 @@ inline int grid_for(int64_t n, int threads, int max_blocks = 148 * 16) {
 }
 
 // sample lists of the pointing's rows grouped by bins of bin_pix pixels
-int mdp_build_bins(mdp_context *ctx, mdp_pointing *A, int bin_pix, mdp_pt_bins *B);
+int mdp_build_bins(mdp_context *ctx, mdp_pointing *A, int bin_pix, mdp_pt_bins *B, bool slices = false);
 // P^T and the block-Jacobi sums run over bins of MDP_PT_BIN_PIX pixels when the
 // pointing is a triplet pointing of 2^20 rows or more (pointing.cu)
 #define MDP_PT_BIN_PIX 256

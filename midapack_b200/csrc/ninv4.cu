@@ -138,6 +138,17 @@ __host__ __device__ constexpr double w16s(int m) {  // imaginary part of W_16^m 
          : m == 6 ? -0.70710678118654752440 : -0.38268343236508977173;
 }
 
+// cos and -sin of 2 pi m / 32, m < 16
+__host__ __device__ constexpr double w32c(int m) {
+    return m == 0 ? 1.0 : m == 1 ? 0.98078528040323044913 : m == 2 ? 0.92387953251128675613
+         : m == 3 ? 0.83146961230254523708 : m == 4 ? 0.70710678118654752440 : m == 5 ? 0.55557023301960222474
+         : m == 6 ? 0.38268343236508977173 : m == 7 ? 0.19509032201612826785 : m == 8 ? 0.0
+         : m == 9 ? -0.19509032201612826785 : m == 10 ? -0.38268343236508977173 : m == 11 ? -0.55557023301960222474
+         : m == 12 ? -0.70710678118654752440 : m == 13 ? -0.83146961230254523708 : m == 14 ? -0.92387953251128675613
+         : -0.98078528040323044913;
+}
+__host__ __device__ constexpr double w32s(int m) { return -w32c((m + 24) % 32 < 16 ? (m + 24) % 32 : 32 - (m + 24) % 32); }
+
 // d * W_16^m (CONJ: d * conj(W_16^m)), m known at compile time
 template <typename T, int M, bool CONJ>
 __device__ __forceinline__ CP<T> mulw16(CP<T> d) {
@@ -286,6 +297,11 @@ template <int C> __host__ __device__ constexpr int col_entries() { return (M2 / 
 template <int C> __host__ __device__ constexpr int buf_entries() {
     return row_entries() > col_entries<C>() ? row_entries() : col_entries<C>();
 }
+// the spectrum values of a CTA's two rows staged in shared memory as lane
+// pairs (H[rA + M1 k2], H[rB + M1 k2]), k2 = rev(p), position p at entry
+// hpos(p) = p + p / 16 (spread over all banks for the pass's strided reads)
+__host__ __device__ constexpr int hpos(int p) { return p + (p >> 4); }
+constexpr int HENT = M2 + M2 / 16;  // staged pairs
 
 template <typename T>
 struct alignas(16) Ent {  // one shared-memory position: (x_A, x_B), (y_A, y_B)
@@ -301,9 +317,10 @@ struct Ninv4Args {
     const int64_t *blk_start;
     const int32_t *blk_len;
     const int32_t *blk_spec;
-    const Ent<T>  *hc;          // [n_spec][C][16][256]: ((ca_A, ca_B), (cb_A, cb_B)), scaled by 1/(4M)
+    const T       *hrow;        // [n_spec][M + 4]: pairs (H[rA + M1 rev(p)], H[rB + M1 rev(p)]) / (4M) of CTA c
+                                //   at 2 (c M2 + p), then H[M] / (4M)
     const Ent<T>  *wbase;       // [C]: (W_N^rA, W_N^rB) of CTA c's rows, as ((re_A, re_B), (im_A, im_B))
-    const typename std::conditional<sizeof(T) == 4, float2, double2>::type *w8192;  // [16][256]: W_2M2^rev(16t+i)
+    const typename std::conditional<sizeof(T) == 4, float2, double2>::type *wlo;  // [256]: W_2M2^rev8(t)
     const double2 *twM;         // [M2]: W_M^n2 (FP64; rounded to T on use)
     const double2 *tw4096;      // [256]: W_4096^q
     const double  *means;       // [nb] or [ncols][nb]
@@ -329,6 +346,22 @@ __device__ __forceinline__ Ent<double> ldg_ent(const Ent<double> *p) {
 template <typename T>
 __device__ __forceinline__ CP<T> ent2cp(Ent<T> e) {
     return {e.x, e.y};
+}
+
+// a staged spectrum pair from shared memory, in program order (the untangle
+// pass reads one position at a time; letting the compiler hoist all sixteen
+// costs registers the kernel does not have)
+__device__ __forceinline__ Pr<float> lds_pair(const Pr<float> *p) {
+    Pr<float>      r;
+    const unsigned a = (unsigned) __cvta_generic_to_shared(p);
+    asm volatile("ld.shared.b64 %0, [%1];" : "=l"(r.v) : "r"(a) : "memory");
+    return r;
+}
+__device__ __forceinline__ Pr<double> lds_pair(const Pr<double> *p) {
+    Pr<double>     r;
+    const unsigned a = (unsigned) __cvta_generic_to_shared(p);
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(r.a), "=d"(r.b) : "r"(a) : "memory");
+    return r;
 }
 
 // cluster barriers (all threads of every CTA of the cluster)
@@ -459,42 +492,72 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, sizeof(T) == 4 ?
     cluster_arrive();
     cluster_wait();  // every row of this CTA is in place
 
+    // this CTA's two spectrum rows (rA, rB) into shared memory, in flight
+    // during the forward row passes
+    // (after the row layout: the column layout's tail, used only once the
+    // untangle pass has read the spectrum)
+    Pr<T> *sH = reinterpret_cast<Pr<T> *>(smem_raw + sizeof(Ent<T>) * row_entries());
+    {
+        const T *hs = a.hrow + (size_t) a.blk_spec[blk] * (M + 4) + (size_t) 2 * c * M2;
+#pragma unroll 1
+        for (int p = threadIdx.x; p < M2; p += NT) {
+            const unsigned dst = (unsigned) __cvta_generic_to_shared(sH + hpos(p));
+            if constexpr (sizeof(T) == 4)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(hs + 2 * p) : "memory");
+            else
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(hs + 2 * p) : "memory");
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+
     // ---- step B forward: three radix-16 DIF passes per row (both rows on the lanes)
     row_pass_fwd<T, 4096>(buf, a.tw4096);
     __syncthreads();
     row_pass_fwd<T, 256>(buf, a.tw4096);
     __syncthreads();
     row_pass_fwd<T, 16>(buf, a.tw4096);
+    asm volatile("cp.async.wait_all;\n" ::: "memory");  // this thread's spectrum copies
     __syncthreads();
 
     // ---- untangle, spectrum product, re-tangle; then the first inverse pass
     {
         const int   t = threadIdx.x;
-        const int   spec = a.blk_spec[blk];
-        const Ent<T> *hc = a.hc + ((size_t) spec * C + c) * (16 * NSET);
-        // W_N^k of lane r, k = r + M1 rev(p): W_N^r (per CTA) times W_{2 M2}^rev(p) (one table for all CTAs)
+        // W_N^k of lane r = W_N^r W_2M2^k2, k2 = rev4(i) 2^8 + rev8(t): W_N^r W_2M2^rev8(t) once per
+        // thread, times the constant W_32^rev4(i) per position
         const Ent<T> wb = ldg_ent(a.wbase + c);
-        CP<T>       v[16];
+        const auto   wl = __ldg(a.wlo + t);
+        const CP<T>  wt = cpmul(CP<T>{wb.x, wb.y}, CP<T>{pdup<T>(wl.x), pdup<T>(wl.y)});
+        const T      hM = (c == 0) ? a.hrow[(size_t) a.blk_spec[blk] * (M + 4) + M] : (T) 0;
+        CP<T>        v[16];
 #pragma unroll
         for (int i = 0; i < 16; i++) v[i] = ent2cp(buf[rpos(16 * t + i)]);
 #pragma unroll
         for (int i = 0; i < 16; i++) {
             const int p = 16 * t + i;
             CP<T>     z2;
+            // (H[kA], H[kB]) and (H[M - kA], H[M - kB]): M - k of one lane lies
+            // in the other lane's row at position M2-1-p (rows c and M1 - c);
+            // on CTA 0 lane B (row C) pairs with itself there, and lane A (row
+            // 0) with row 0 at rev(M2 - k2), or H[M] for k2 = 0
+            const Pr<T> hk = lds_pair(sH + hpos(p));
+            Pr<T>       hm;
             if (c != 0) {
                 // lane A pairs with lane B of position M2-1-p and vice versa
                 const Ent<T> e = buf[rpos(M2 - 1 - p)];
                 z2 = CP<T>{pswap(e.x), pswap(e.y)};
+                hm = pswap(lds_pair(sH + hpos(M2 - 1 - p)));
             } else {
                 // row 0 (lane A): k2 = rev(p) pairs with M2 - k2; row C (lane B): position M2-1-p
                 const int k2 = (int) (__brev((unsigned) p) >> (32 - LOGM2));
                 const int pp = (int) (__brev((unsigned) ((M2 - k2) & (M2 - 1))) >> (32 - LOGM2));
                 const Ent<T> ea = buf[rpos(pp)], eb = buf[rpos(M2 - 1 - p)];
                 z2 = CP<T>{pmk(plo(ea.x), phi(eb.x)), pmk(plo(ea.y), phi(eb.y))};
+                hm = pmk(k2 == 0 ? hM : plo(lds_pair(sH + hpos(pp))), phi(lds_pair(sH + hpos(M2 - 1 - p))));
             }
-            const Ent<T> h = ldg_ent(hc + i * NSET + t);  // (ca, cb), already / (4M)
-            const auto   wr = __ldg(a.w8192 + i * NSET + t);
-            const CP<T>  wp = cpmul(CP<T>{wb.x, wb.y}, CP<T>{pdup<T>(wr.x), pdup<T>(wr.y)});
+            // (ca, cb) = (H[k] + H[M-k], H[k] - H[M-k]), already / (4M)
+            const Ent<T> h{padd(hk, hm), psub(hk, hm)};
+            const int    m = rev_bits_c(i, 4);
+            const CP<T>  wp = cpmul(wt, CP<T>{pcst<T>(w32c(m)), pcst<T>(w32s(m))});
             const Ent<T> w{wp.x, wp.y};  // W_N^k
             const CP<T>  z1 = v[i];
             const Pr<T>  e0x = padd(z1.x, z2.x), e0y = psub(z1.y, z2.y);
@@ -588,22 +651,25 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, sizeof(T) == 4 ?
 }
 
 // ------------------------------------------------------------------ tables
-// hc and wk tables of one spectrum H[0..M] (FP64, N = 2M point circulant
-// spectrum) in the order the untangle pass reads them: entry (c, i, t) is
-// position p = 16 t + i of CTA c, lanes A/B = rows (c, M1 - c) or (0, C).
+// the staged spectrum table of one spectrum H[0..M] (FP64, N = 2M point
+// circulant spectrum), scaled by 1/(4M) (a power of two, exact): for CTA c,
+// position p, the lane pair (H[rA + M1 k2], H[rB + M1 k2]), k2 = rev(p), rows
+// (rA, rB) = (c, M1 - c), (0, C) on CTA 0, in the order the untangle pass
+// reads them; H[M] follows
 template <typename T>
-__global__ void ninv4_hc_kernel(const double *__restrict__ H, int C, Ent<T> *__restrict__ out) {
-    const int M1 = 2 * C, M = M1 * M2, n = C * 16 * NSET;
+__global__ void ninv4_hrow_kernel(const double *__restrict__ H, int C, T *__restrict__ out) {
+    const int    M1 = 2 * C, M = M1 * M2;
     const double s = 1.0 / (4.0 * (double) M);
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        const int c = e / (16 * NSET), i = (e / NSET) % 16, t = e % NSET;
-        const int p = 16 * t + i;
-        const int k2 = (int) (__brev((unsigned) p) >> (32 - LOGM2));
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e <= C * M2; e += gridDim.x * blockDim.x) {
+        if (e == C * M2) {
+            out[M] = (T) (H[M] * s);
+            continue;
+        }
+        const int c = e / M2, p = e % M2;
         const int rA = c, rB = (c == 0) ? C : M1 - c;
-        const int kA = rA + M1 * k2, kB = rB + M1 * k2;
-        const double caA = (H[kA] + H[M - kA]) * s, cbA = (H[kA] - H[M - kA]) * s;
-        const double caB = (H[kB] + H[M - kB]) * s, cbB = (H[kB] - H[M - kB]) * s;
-        out[e] = Ent<T>{pmk((T) caA, (T) caB), pmk((T) cbA, (T) cbB)};
+        const int k2 = (int) (__brev((unsigned) p) >> (32 - LOGM2));
+        out[2 * e] = (T) (H[rA + M1 * k2] * s);
+        out[2 * e + 1] = (T) (H[rB + M1 * k2] * s);
     }
 }
 
@@ -614,8 +680,14 @@ static void cexp_ld(long double num, long double den, double *re, double *im) { 
 
 // sets the kernel's shared-memory limit and returns how many clusters fit on the device at once
 template <typename T, int C>
+static constexpr size_t ninv4_smem_c() {
+    const size_t rows = sizeof(Ent<T>) * row_entries() + sizeof(Pr<T>) * HENT;
+    return rows > sizeof(Ent<T>) * buf_entries<C>() ? rows : sizeof(Ent<T>) * buf_entries<C>();
+}
+
+template <typename T, int C>
 static int ninv4_setup_kernel(int *max_clusters) {
-    constexpr size_t smem = sizeof(Ent<T>) * buf_entries<C>();
+    constexpr size_t smem = ninv4_smem_c<T, C>();
     MDP_CUDA(cudaFuncSetAttribute((const void *) ninv4_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int) smem));
     cudaLaunchConfig_t cfg = {};
@@ -635,26 +707,25 @@ static int ninv4_setup_kernel(int *max_clusters) {
 template <typename T>
 size_t ninv4_smem(int C) {
     switch (C) {
-        case 2: return sizeof(Ent<T>) * buf_entries<2>();
-        case 4: return sizeof(Ent<T>) * buf_entries<4>();
-        case 8: return sizeof(Ent<T>) * buf_entries<8>();
+        case 2: return ninv4_smem_c<T, 2>();
+        case 4: return ninv4_smem_c<T, 4>();
+        case 8: return ninv4_smem_c<T, 8>();
     }
     return 0;
 }
 
-// The plan's tables: P.ttw = the per-CTA twist factors [C] Ent<T>, P.wa = W_{2 M2}^rev(p) [16][256]
-// (T2), P.twm = W_M^n2 [M2]
-// double2, P.ltw = W_4096^q [256] double2, P.spectra = hc [n_spec][C][16][256]
-// Ent<T> (from the FP64 spectra H of each distinct row when `spectra`, else
-// zero).  Tiles are laid as for the split plans (one output fewer than the
-// band allows, even window starts).
+// The plan's tables: P.ttw = the per-CTA twist factors [C] Ent<T>, P.wa = W_{2 M2}^rev8(t) [256]
+// (T2), P.twm = W_M^n2 [M2] double2, P.ltw = W_4096^q [256] double2, P.spectra = the staged
+// spectrum tables [n_spec][M + 4] T (ninv4_hrow_kernel, from the FP64 spectra H of each
+// distinct row when `spectra`, else zero).  Tiles are laid as for the split plans (one
+// output fewer than the band allows, even window starts).
 template <typename T>
 int ninv4_build(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, bool spectra) {
     const int C = P.cluster, M1 = 2 * C, M = M1 * M2, Nn = 2 * M;
     if (C != 2 && C != 4 && C != 8) return MDP_EUNSUPPORTED;
-    const size_t ne = (size_t) C * 16 * NSET;
-    // W_N^k of lane r at position p (k = r + M1 rev(p)) = W_N^r W_{2 M2}^rev(p): the per-CTA
-    // factors (ttw) and one table in the order the untangle pass reads it (wa)
+    const size_t ne = (size_t) M + 4;  // staged spectrum table entries per spectrum
+    // W_N^k of lane r at position p = 16 t + i (k = r + M1 rev(p)) = W_N^r W_{2 M2}^rev8(t) W_32^rev4(i):
+    // the per-CTA factors (ttw) and W_{2 M2}^rev8(t) by thread (wa; W_32 are constants)
     {
         std::vector<T> base(4 * C);
         for (int c = 0; c < C; c++) {
@@ -669,14 +740,13 @@ int ninv4_build(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, bool spectra) 
         }
         MDP_TRY(P.ttw.alloc(sizeof(Ent<T>) * C));
         MDP_CUDA(cudaMemcpy(P.ttw.p, base.data(), sizeof(T) * base.size(), cudaMemcpyHostToDevice));
-        std::vector<T> w(2 * 16 * NSET);
-        for (int i = 0; i < 16; i++)
-            for (int t = 0; t < NSET; t++) {
-                double re, im;
-                cexp_ld(rev_bits_c(16 * t + i, LOGM2), 2 * M2, &re, &im);
-                w[2 * (i * NSET + t)] = (T) re;
-                w[2 * (i * NSET + t) + 1] = (T) im;
-            }
+        std::vector<T> w(2 * NSET);
+        for (int t = 0; t < NSET; t++) {
+            double re, im;
+            cexp_ld(rev_bits_c(t, 8), 2 * M2, &re, &im);
+            w[2 * t] = (T) re;
+            w[2 * t + 1] = (T) im;
+        }
         MDP_TRY(P.wa.alloc(sizeof(T) * w.size()));
         MDP_CUDA(cudaMemcpy(P.wa.p, w.data(), sizeof(T) * w.size(), cudaMemcpyHostToDevice));
     }
@@ -689,7 +759,7 @@ int ninv4_build(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, bool spectra) 
         MDP_CUDA(cudaMemcpy(P.twm.p, tm.data(), sizeof(double2) * M2, cudaMemcpyHostToDevice));
         MDP_CUDA(cudaMemcpy(P.ltw.p, t4.data(), sizeof(double2) * 256, cudaMemcpyHostToDevice));
     }
-    MDP_TRY(P.spectra.alloc(sizeof(Ent<T>) * ne * std::max(N->n_spec, 1)));
+    MDP_TRY(P.spectra.alloc(sizeof(T) * ne * std::max(N->n_spec, 1)));
     if (spectra) {
         // H[k], k <= M, in FP64 from exp(-2 pi i k / N), k < M (long double on the host)
         std::vector<double2> tw(M);
@@ -701,13 +771,13 @@ int ninv4_build(mdp_context *ctx, mdp_noise *N, mdp_tile_plan &P, bool spectra) 
         for (int u = 0; u < N->n_spec; u++) {
             MDP_TRY(mdp_spectrum_H(ctx, N->h_Tuniq.data() + (size_t) u * N->lambda, N->lambda, Nn,
                                    dtw.as<double2>(), dH.as<double>()));
-            ninv4_hc_kernel<T><<<grid_for((int64_t) ne, 256, 1024), 256, 0, ctx->stream>>>(
-                    dH.as<double>(), C, P.spectra.as<Ent<T>>() + (size_t) u * ne);
+            ninv4_hrow_kernel<T><<<grid_for((int64_t) ne, 256, 1024), 256, 0, ctx->stream>>>(
+                    dH.as<double>(), C, P.spectra.as<T>() + (size_t) u * ne);
             MDP_CHECK_LAUNCH(ctx);
             MDP_CUDA(cudaStreamSynchronize(ctx->stream));
         }
     } else {
-        MDP_CUDA(cudaMemset(P.spectra.p, 0, sizeof(Ent<T>) * ne * std::max(N->n_spec, 1)));
+        MDP_CUDA(cudaMemset(P.spectra.p, 0, sizeof(T) * ne * std::max(N->n_spec, 1)));
     }
     switch (C) {
         case 2: MDP_TRY((ninv4_setup_kernel<T, 2>(&P.threads))); break;
@@ -730,9 +800,9 @@ int ninv4_launch(mdp_context *ctx, const mdp_noise *N, const mdp_tile_plan &P, c
     a.blk_start = N->blk_start.as<int64_t>();
     a.blk_len = N->blk_len.as<int32_t>();
     a.blk_spec = N->blk_spec.as<int32_t>();
-    a.hc = P.spectra.as<Ent<T>>();
+    a.hrow = P.spectra.as<T>();
     a.wbase = P.ttw.as<Ent<T>>();
-    a.w8192 = static_cast<const typename std::conditional<sizeof(T) == 4, float2, double2>::type *>(P.wa.p);
+    a.wlo = static_cast<const typename std::conditional<sizeof(T) == 4, float2, double2>::type *>(P.wa.p);
     a.twM = P.twm.as<double2>();
     a.tw4096 = P.ltw.as<double2>();
     a.means = d_means;

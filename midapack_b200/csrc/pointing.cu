@@ -613,12 +613,16 @@ __global__ void trmatvec_general_kernel(const int32_t *__restrict__ local, const
 // the rows by bin, so the list is the same on every build): counts per
 // (row chunk, bin), bin totals, an exclusive scan over the bins, per-chunk
 // offsets within each bin, then one warp per row chunk writes its rows in
-// order.  One warp then owns one bin: it walks the bin's list in order, 32
-// rows a step, and adds each row's three products into its shared-memory copy
-// of the bin's map; rows of one step that hit the same pixel are added in
-// lane order.  Every map entry is written once, by its bin's warp: the sums
-// are reproducible bit for bit (the order of every addition is fixed) and no
-// atomic operation touches the map.
+// order.  Each bin's list is cut into slices of a fixed length (a function of
+// the row count only), and one warp owns one slice: it walks the slice in
+// order, 32 rows a step, and adds each row's three products into its
+// shared-memory copy of the bin's map; rows of one step that hit the same
+// pixel are added in lane order.  A bin of one slice is written by that warp;
+// the slices of a longer bin write partial maps, summed in slice order by one
+// thread per map entry.  The order of every addition is fixed, so the sums
+// are reproducible bit for bit, and no atomic operation touches the map.
+// Slicing keeps the work per warp bounded: small maps (few bins) still fill
+// the device.
 #define PT_BIN_PIX MDP_PT_BIN_PIX
 #define PT_WARPS 8
 
@@ -703,7 +707,19 @@ __global__ void __launch_bounds__(32) bin_chunk_scatter_kernel(const int32_t *__
     }
 }
 
-int mdp_build_bins(mdp_context *ctx, mdp_pointing *A, int bin_pix, mdp_pt_bins *B) {
+// rows per slice of the P^T bin lists: about 2^14 slices, enough to fill the
+// device whatever the map size, at least 512 and at most 2^16 rows each; a
+// function of the row count alone, so that the sums are the same on every
+// device.  Longer slices would leave a small map's few bins to a few warps;
+// shorter ones write more partial maps (3 bin_pix doubles per slice of a bin
+// cut in several).
+static int64_t pt_slice_len(int64_t m) {
+    int64_t len = 512;
+    while (len < (1 << 16) && m / len > (1 << 14)) len <<= 1;
+    return len;
+}
+
+int mdp_build_bins(mdp_context *ctx, mdp_pointing *A, int bin_pix, mdp_pt_bins *B, bool slices) {
     const int64_t npix = A->n_map() / 3;
     const int     bin3 = 3 * bin_pix;
     const int64_t nb = (npix + bin_pix - 1) / bin_pix;
@@ -756,32 +772,76 @@ int mdp_build_bins(mdp_context *ctx, mdp_pointing *A, int bin_pix, mdp_pt_bins *
     for (int64_t i = 0; i <= nb; i++) hs64[i] = hs[i];
     MDP_TRY(B->start.alloc(8 * (nb + 1)));
     MDP_CUDA(cudaMemcpy(B->start.p, hs64.data(), 8 * (nb + 1), cudaMemcpyHostToDevice));
+    B->nslices = B->nmulti = 0;
+    if (slices && nb > 0) {
+        const int64_t        len = pt_slice_len(A->m);
+        std::vector<int32_t> sb, so, mb, mf, mn;
+        std::vector<uint32_t> lo, hi;
+        int32_t              rows = 0;
+        for (int64_t b = 0; b < nb; b++) {
+            const int64_t n = hs64[b + 1] - hs64[b];
+            const int64_t k = std::max<int64_t>((n + len - 1) / len, 1);
+            if (k > 1) {
+                mb.push_back((int32_t) b);
+                mf.push_back(rows);
+                mn.push_back((int32_t) k);
+            }
+            for (int64_t j = 0; j < k; j++) {
+                sb.push_back((int32_t) b);
+                lo.push_back((uint32_t) (hs64[b] + j * len));
+                hi.push_back((uint32_t) std::min<int64_t>(hs64[b] + (j + 1) * len, hs64[b + 1]));
+                so.push_back(k > 1 ? rows++ : -1);
+            }
+        }
+        B->nslices = (int64_t) sb.size();
+        B->nmulti = (int64_t) mb.size();
+        B->slice_len = len;
+        MDP_TRY(B->slice_bin.alloc(4 * sb.size()));
+        MDP_TRY(B->slice_lo.alloc(4 * sb.size()));
+        MDP_TRY(B->slice_hi.alloc(4 * sb.size()));
+        MDP_TRY(B->slice_out.alloc(4 * sb.size()));
+        MDP_CUDA(cudaMemcpy(B->slice_bin.p, sb.data(), 4 * sb.size(), cudaMemcpyHostToDevice));
+        MDP_CUDA(cudaMemcpy(B->slice_lo.p, lo.data(), 4 * lo.size(), cudaMemcpyHostToDevice));
+        MDP_CUDA(cudaMemcpy(B->slice_hi.p, hi.data(), 4 * hi.size(), cudaMemcpyHostToDevice));
+        MDP_CUDA(cudaMemcpy(B->slice_out.p, so.data(), 4 * so.size(), cudaMemcpyHostToDevice));
+        if (!mb.empty()) {
+            MDP_TRY(B->multi_bin.alloc(4 * mb.size()));
+            MDP_TRY(B->multi_first.alloc(4 * mf.size()));
+            MDP_TRY(B->multi_n.alloc(4 * mn.size()));
+            MDP_TRY(B->partial.alloc(sizeof(double) * 3 * (size_t) bin_pix * (size_t) rows));
+            MDP_CUDA(cudaMemcpy(B->multi_bin.p, mb.data(), 4 * mb.size(), cudaMemcpyHostToDevice));
+            MDP_CUDA(cudaMemcpy(B->multi_first.p, mf.data(), 4 * mf.size(), cudaMemcpyHostToDevice));
+            MDP_CUDA(cudaMemcpy(B->multi_n.p, mn.data(), 4 * mn.size(), cudaMemcpyHostToDevice));
+        }
+    }
     B->nbins = nb;
     B->bin_pix = bin_pix;
     B->valid = 1;
     return MDP_OK;
 }
 
-// x = P^T y over the bins: warp k of a CTA owns bin PT_WARPS*blockIdx.x + k.
-// TY/TW: TOD and weight types (double, or float for the mixed solver's FP32
-// operator); products and sums in FP64.  U steps of 32 rows are loaded before
-// they are added, for memory-level parallelism.
+// x = P^T y over the slices of the bins' lists: warp k of a CTA owns slice
+// PT_WARPS*blockIdx.x + k.  TY/TW: TOD and weight types (double, or float for
+// the mixed solver's FP32 operator); products and sums in FP64.  U steps of 32
+// rows are loaded before they are added, for memory-level parallelism.  The
+// warp's sums go to the bin's map entries (a bin of one slice) or to the
+// slice's row of `partial`, summed by pt_partial_sum_kernel.
 template <typename TY, typename TW>
-__global__ void __launch_bounds__(32 * PT_WARPS) trmatvec_bins_kernel(const int32_t *__restrict__ off,
-                                                                      const TW *__restrict__ w,
-                                                                      const TY *__restrict__ y, double *__restrict__ x,
-                                                                      const int64_t *__restrict__ bin_start,
-                                                                      const uint32_t *__restrict__ perm, int64_t nbins,
-                                                                      int64_t n_map) {
+__global__ void __launch_bounds__(32 * PT_WARPS) trmatvec_slices_kernel(
+        const int32_t *__restrict__ off, const TW *__restrict__ w, const TY *__restrict__ y, double *__restrict__ x,
+        const uint32_t *__restrict__ perm, const int32_t *__restrict__ slice_bin, const uint32_t *__restrict__ slice_lo,
+        const uint32_t *__restrict__ slice_hi, const int32_t *__restrict__ slice_out, int64_t nslices,
+        double *__restrict__ partial, int64_t n_map) {
     constexpr int U = 4;
     __shared__ double acc_s[PT_WARPS][3 * PT_BIN_PIX];
     const int     wid = threadIdx.x >> 5, lane = lane_id();
-    const int64_t bin = (int64_t) blockIdx.x * PT_WARPS + wid;
-    if (bin >= nbins) return;  // whole warps only; no CTA-wide barrier follows
+    const int64_t sl = (int64_t) blockIdx.x * PT_WARPS + wid;
+    if (sl >= nslices) return;  // whole warps only; no CTA-wide barrier follows
     double *acc = acc_s[wid];
     for (int i = lane; i < 3 * PT_BIN_PIX; i += 32) acc[i] = 0.0;
     __syncwarp();
-    const int64_t s0 = bin_start[bin], s1 = bin_start[bin + 1];
+    const int64_t bin = slice_bin[sl];
+    const int64_t s0 = slice_lo[sl], s1 = slice_hi[sl];
     const int64_t base = bin * 3 * PT_BIN_PIX;
     for (int64_t i0 = s0; i0 < s1; i0 += 32 * U) {
         int    o[U];
@@ -826,8 +886,52 @@ __global__ void __launch_bounds__(32 * PT_WARPS) trmatvec_bins_kernel(const int3
             __syncwarp();
         }
     }
-    const int64_t lim = min((int64_t) 3 * PT_BIN_PIX, n_map - base);
-    for (int i = lane; i < lim; i += 32) x[base + i] = acc[i];
+    const int out = slice_out[sl];
+    if (out < 0) {
+        const int64_t lim = min((int64_t) 3 * PT_BIN_PIX, n_map - base);
+        for (int i = lane; i < lim; i += 32) x[base + i] = acc[i];
+    } else {
+        double *pr = partial + (int64_t) out * 3 * PT_BIN_PIX;
+        for (int i = lane; i < 3 * PT_BIN_PIX; i += 32) pr[i] = acc[i];
+    }
+}
+
+// map entries of the bins of several slices: their partial maps summed in slice order
+__global__ void pt_partial_sum_kernel(const double *__restrict__ partial, const int32_t *__restrict__ multi_bin,
+                                      const int32_t *__restrict__ multi_first, const int32_t *__restrict__ multi_n,
+                                      int64_t nmulti, double *__restrict__ x, int64_t n_map) {
+    constexpr int E = 3 * PT_BIN_PIX;
+    for (int64_t idx = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; idx < nmulti * E;
+         idx += (int64_t) gridDim.x * blockDim.x) {
+        const int64_t k = idx / E, e = idx % E;
+        const int64_t xi = (int64_t) multi_bin[k] * E + e;
+        if (xi >= n_map) continue;
+        const double *pr = partial + (int64_t) multi_first[k] * E + e;
+        double        s = 0.0;
+        for (int j = 0; j < multi_n[k]; j++) s += pr[(int64_t) j * E];
+        x[xi] = s;
+    }
+}
+
+// P^T over the slices (both kernels), FP64 or FP32 TOD and weights
+template <typename TY, typename TW>
+static int trmatvec_slices(mdp_context *ctx, const mdp_pointing *A, const TW *w, const TY *d_y, double *d_x) {
+    const mdp_pt_bins &B = A->bins;
+    if (B.nslices > 0) {
+        trmatvec_slices_kernel<TY, TW><<<(unsigned) ((B.nslices + PT_WARPS - 1) / PT_WARPS), 32 * PT_WARPS, 0,
+                                         ctx->stream>>>(
+                A->off.as<int32_t>(), w, d_y, d_x, B.perm.as<uint32_t>(), B.slice_bin.as<int32_t>(),
+                B.slice_lo.as<uint32_t>(), B.slice_hi.as<uint32_t>(), B.slice_out.as<int32_t>(), B.nslices,
+                B.partial.as<double>(), A->n_map());
+        MDP_CHECK_LAUNCH(ctx);
+    }
+    if (B.nmulti > 0) {
+        pt_partial_sum_kernel<<<grid_for(B.nmulti * 3 * PT_BIN_PIX, 256, ctx->sm_count * 8), 256, 0, ctx->stream>>>(
+                B.partial.as<double>(), B.multi_bin.as<int32_t>(), B.multi_first.as<int32_t>(),
+                B.multi_n.as<int32_t>(), B.nmulti, d_x, A->n_map());
+        MDP_CHECK_LAUNCH(ctx);
+    }
+    return MDP_OK;
 }
 
 __global__ void trmatvec32_kernel(const int32_t *__restrict__ off, const float *__restrict__ w,
@@ -863,22 +967,16 @@ int mdp_pointing_prepare_fp32(mdp_context *ctx, mdp_pointing *A) {
 static bool use_bins(const mdp_pointing *A) { return A->triplet && A->m >= (1 << 20); }
 bool mdp_pointing_binned(const mdp_pointing *A) { return use_bins(A); }
 int  mdp_pointing_bins(mdp_context *ctx, mdp_pointing *A) {
-    if (!A->bins.valid || A->bins.bin_pix != PT_BIN_PIX) MDP_TRY(mdp_build_bins(ctx, A, PT_BIN_PIX, &A->bins));
+    if (!A->bins.valid || A->bins.bin_pix != PT_BIN_PIX) MDP_TRY(mdp_build_bins(ctx, A, PT_BIN_PIX, &A->bins, true));
     return MDP_OK;
 }
 
 int mdp_trmatvec_launch(mdp_context *ctx, const mdp_pointing *A, const double *d_y, double *d_x) {
     if (use_bins(A)) {
         mdp_pointing *Am = const_cast<mdp_pointing *>(A);  // the bin list is a cache of the pointing
-        if (!Am->bins.valid || Am->bins.bin_pix != PT_BIN_PIX) MDP_TRY(mdp_build_bins(ctx, Am, PT_BIN_PIX, &Am->bins));
-        if (A->bins.nbins > 0) {  // every map entry is written by its bin's warp
-            trmatvec_bins_kernel<double, double><<<(unsigned) ((A->bins.nbins + PT_WARPS - 1) / PT_WARPS), 32 * PT_WARPS,
-                                                   0, ctx->stream>>>(
-                    A->off.as<int32_t>(), A->values, d_y, d_x, A->bins.start.as<int64_t>(), A->bins.perm.as<uint32_t>(),
-                    A->bins.nbins, A->n_map());
-            MDP_CHECK_LAUNCH(ctx);
-        }
-        return MDP_OK;
+        MDP_TRY(mdp_pointing_bins(ctx, Am));
+        // every map entry is written by its bin's slice or by the partial sums
+        return trmatvec_slices<double, double>(ctx, A, A->values, d_y, d_x);
     }
     MDP_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * A->n_map(), ctx->stream));
     if (A->triplet && !aligned16(A->values, d_y)) {
@@ -905,15 +1003,8 @@ extern "C" int mdp_trmatvec(mdp_context *ctx, const mdp_pointing *A, const doubl
 int mdp_trmatvec32_launch(mdp_context *ctx, mdp_pointing *A, const float *d_y, double *d_x) {
     MDP_TRY(mdp_pointing_prepare_fp32(ctx, A));
     if (use_bins(A)) {
-        if (!A->bins.valid || A->bins.bin_pix != PT_BIN_PIX) MDP_TRY(mdp_build_bins(ctx, A, PT_BIN_PIX, &A->bins));
-        if (A->bins.nbins > 0) {
-            trmatvec_bins_kernel<float, float><<<(unsigned) ((A->bins.nbins + PT_WARPS - 1) / PT_WARPS), 32 * PT_WARPS,
-                                                 0, ctx->stream>>>(
-                    A->off.as<int32_t>(), A->w32.as<float>(), d_y, d_x, A->bins.start.as<int64_t>(),
-                    A->bins.perm.as<uint32_t>(), A->bins.nbins, A->n_map());
-            MDP_CHECK_LAUNCH(ctx);
-        }
-        return MDP_OK;
+        MDP_TRY(mdp_pointing_bins(ctx, A));
+        return trmatvec_slices<float, float>(ctx, A, A->w32.as<float>(), d_y, d_x);
     }
     MDP_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * A->n_map(), ctx->stream));
     trmatvec32_kernel<<<grid_for(A->m, 256, ctx->sm_count * 16), 256, 0, ctx->stream>>>(

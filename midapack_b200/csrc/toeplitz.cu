@@ -1178,7 +1178,7 @@ static std::vector<TileCand> tile_candidates(int lambda) {
     if (g_cluster4_auto)
         for (int C = 2; C <= 8; C <<= 1) {  // cluster four-step tiles of 2C x 4096 points
             TileCand c{13, C, 256, 2, 0, 12};
-            if (cand_E(c, lambda) < 1) continue;
+            if (cand_E(c, lambda) < 1 || ninv4_smem<T>(C) > NINV4_SMEM_MAX) continue;
             out.push_back(c);
         }
     return out;
@@ -1312,7 +1312,8 @@ static int parse_plan(const char *plan, int lambda, TileCand *out) {
              c.log_m1 <= SplitShape<T>::M1MAX && c.log_m2 >= 5 && c.log_m2 <= 9;
     } else if (plan[0] == 'c') {
         c = TileCand{13, 0, 256, 2, 0, 12};
-        ok = sscanf(plan + 1, ",%d", &c.C) == 1 && (c.C == 2 || c.C == 4 || c.C == 8);
+        ok = sscanf(plan + 1, ",%d", &c.C) == 1 && (c.C == 2 || c.C == 4 || c.C == 8) &&
+             ninv4_smem<T>(c.C) <= NINV4_SMEM_MAX;
     } else {
         ok = sscanf(plan, "%d,%d,%d", &c.log_ml, &c.C, &c.threads) == 3 && pick_kernel<T>(c.log_ml, c.C) &&
              c.threads >= 32 && c.threads <= 512 && !(c.threads & 31);
