@@ -94,6 +94,8 @@ def parse():
                     help="operator part: ';'-separated N^-1 tile plans (mdp_noise_set_plan names); empty: auto")
     ap.add_argument("--multi-rhs", type=int, default=128, help="right-hand sides of the multi-RHS part")
     ap.add_argument("--multi-fp64-cols", type=int, default=2, help="columns timed with the plain FP64 path")
+    ap.add_argument("--multi-inner-tol", type=float, default=1e-4,
+                    help="relative residual of the multi-RHS inner (FP32) solves between FP64 refinements")
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-rate", type=float, default=50.0, help="mean Poisson arrival rate, solves/s")
     ap.add_argument("--serve-datasets", type=int, default=16)
@@ -268,7 +270,8 @@ def bench_multi(args, device):
     l0 = ctx.launches
     t0 = time.perf_counter()
     x, lst, cond, hits, ci, info = mb.gls_solve_multi(ctx, P, N, noise, signal=wl.signal, signal_col=0, tol=MULTI_TOL,
-                                                      maxiter=MAXITER, slots=0, use_graph=True)
+                                                      maxiter=MAXITER, inner_tol=args.multi_inner_tol, slots=0,
+                                                      use_graph=True)
     torch.cuda.synchronize()
     t_multi = time.perf_counter() - t0
     log(f"multi-RHS solve: {args.multi_rhs} columns in {t_multi:.2f} s")
@@ -297,7 +300,7 @@ def bench_multi(args, device):
                                       float(np.linalg.norm(xv[k::3] - xo[k::3]) / np.linalg.norm(xo[k::3])))
         del P1, N1, nz, sig
     t64 = float(np.mean([f[0] for f in fp64]))
-    out = {"workload": MULTI_CONFIG, "tol": MULTI_TOL, "rhs": args.multi_rhs, "columns": "1 signal+noise + "
+    out = {"workload": MULTI_CONFIG, "tol": MULTI_TOL, "inner_tol": args.multi_inner_tol, "rhs": args.multi_rhs, "columns": "1 signal+noise + "
            f"{args.multi_rhs - 1} Monte-Carlo noise realisations (FP32 values)",
            "time_s": round(t_multi, 3), "solves_per_s": round(args.multi_rhs / t_multi, 3),
            "fp64_path": {"seconds_per_solve": round(t64, 4), "solves_per_s": round(1.0 / t64, 3),

@@ -709,13 +709,17 @@ __global__ void __launch_bounds__(32) bin_chunk_scatter_kernel(const int32_t *__
 
 // rows per slice of the P^T bin lists: about 2^14 slices, enough to fill the
 // device whatever the map size, at least 512 and at most 2^16 rows each; a
-// function of the row count alone, so that the sums are the same on every
-// device.  Longer slices would leave a small map's few bins to a few warps;
+// function of the pointing alone (rows and bins), so that the sums are the
+// same on every device.  Longer slices would leave a small map's few bins to a few warps;
 // shorter ones write more partial maps (3 bin_pix doubles per slice of a bin
 // cut in several).
-static int64_t pt_slice_len(int64_t m) {
+static int64_t pt_slice_len(int64_t m, int64_t nbins) {
     int64_t len = 512;
     while (len < (1 << 16) && m / len > (1 << 14)) len <<= 1;
+    // bins enough to fill the device by themselves: cut only the bins longer
+    // than the average (fewer partial maps to write and sum)
+    if (nbins >= 4096)
+        while (len < (1 << 16) && len < m / nbins) len <<= 1;
     return len;
 }
 
@@ -774,7 +778,7 @@ int mdp_build_bins(mdp_context *ctx, mdp_pointing *A, int bin_pix, mdp_pt_bins *
     MDP_CUDA(cudaMemcpy(B->start.p, hs64.data(), 8 * (nb + 1), cudaMemcpyHostToDevice));
     B->nslices = B->nmulti = 0;
     if (slices && nb > 0) {
-        const int64_t        len = pt_slice_len(A->m);
+        const int64_t        len = pt_slice_len(A->m, nb);
         std::vector<int32_t> sb, so, mb, mf, mn;
         std::vector<uint32_t> lo, hi;
         int32_t              rows = 0;
@@ -843,7 +847,22 @@ __global__ void __launch_bounds__(32 * PT_WARPS) trmatvec_slices_kernel(
     const int64_t bin = slice_bin[sl];
     const int64_t s0 = slice_lo[sl], s1 = slice_hi[sl];
     const int64_t base = bin * 3 * PT_BIN_PIX;
+    // the row numbers of the next U steps are loaded while the current ones are
+    // gathered and added: one memory latency per U steps on the warp's path
+    uint32_t tn[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        const int64_t i = s0 + 32 * u + lane;
+        tn[u] = (i < s1) ? perm[i] : 0u;
+    }
     for (int64_t i0 = s0; i0 < s1; i0 += 32 * U) {
+        uint32_t tc[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            tc[u] = tn[u];
+            const int64_t i = i0 + 32 * (U + u) + lane;
+            tn[u] = (i < s1) ? perm[i] : 0u;
+        }
         int    o[U];
         double c0[U], c1[U], c2[U];
 #pragma unroll
@@ -852,7 +871,7 @@ __global__ void __launch_bounds__(32 * PT_WARPS) trmatvec_slices_kernel(
             o[u] = -1;
             c0[u] = c1[u] = c2[u] = 0.0;
             if (i < s1) {
-                const int64_t t = perm[i];
+                const int64_t t = tc[u];
                 const double  v = (double) y[t];
                 o[u] = (int) (off[t] - base);
                 c0[u] = (double) w[3 * t] * v;
