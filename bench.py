@@ -197,11 +197,13 @@ def algorithmic_bytes32(ns: int, n_map: int, t32):
 
 
 # DRAM bytes per tile of one N^-1 application, measured with ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum of the three split kernels over
-# 704 tiles, lambda 2^14, 2^20-sample blocks; see profiles/), keyed by
-# (precision, M1, M2); scaled to a launch by the tile count
-NINV_TRAFFIC_PER_TILE = {("f32", 256, 256): 1857072128 / 704,   # profiles/ninv_split_fp32_256x256_lambda16384.md
-                         ("f32", 256, 512): 1728509184 / 320}   # profiles/op32_split_256x512_lambda16384.md
+# (dram__bytes_read.sum + dram__bytes_write.sum of the three split kernels,
+# lambda 2^14, 2^20-sample blocks), keyed by (precision, M1, M2); scaled to a
+# launch by the tile count.  256 x 256: 704 tiles in one application; 256 x 512:
+# three applications of 160 tiles, the split_pairs_kernel's 1.3 MB taken out
+# (profiles/ninv_split_fp32_256x256_lambda16384.md, operator_p_pt_ninv_dram_2p25.md)
+NINV_TRAFFIC_PER_TILE = {("f32", 256, 256): 1857072128 / 704,
+                         ("f32", 256, 512): (2370306304 - 1314000) / (3 * 160)}
 
 
 def ninv_kernel(t: dict, prec: str) -> str:
@@ -868,7 +870,7 @@ def main():
                 "per_application_ms": {k: round(v, 4) for k, v in per.items()},
                 "algorithmic_bytes": ab}
     if dom == "Ninv" and ninv_tile.get("split"):
-        # what the ncu captures show about the split kernels (profiles/)
+        # what the ncu captures show about the split kernels
         roofline["limiter"] = ("not DRAM (1.8-2.7 TB/s of DRAM traffic, ~3x the algorithmic bytes from the "
                                "four-step scratch): instruction issue in the row and inverse-column passes (issue "
                                "slot ~65 % busy, top stall 'not selected') and load latency in the forward-column "
