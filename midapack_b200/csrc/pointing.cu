@@ -617,7 +617,8 @@ __global__ void trmatvec_general_kernel(const int32_t *__restrict__ local, const
 // the row count only), and one warp owns one slice: it walks the slice in
 // order, 32 rows a step, and adds each row's three products into its
 // shared-memory copy of the bin's map; rows of one step that hit the same
-// pixel are added in lane order.  A bin of one slice is written by that warp;
+// pixel are summed in lane order by the group's lowest lane, which adds the
+// sum.  A bin of one slice is written by that warp;
 // the slices of a longer bin write partial maps, summed in slice order by one
 // thread per map entry.  The order of every addition is fixed, so the sums
 // are reproducible bit for bit, and no atomic operation touches the map.
@@ -890,16 +891,29 @@ __global__ void __launch_bounds__(32 * PT_WARPS) trmatvec_slices_kernel(
                     acc[o[u] + 2] += c2[u];
                 }
             } else {
-                for (int src = 0; src < 32; src++) {  // rows in lane order
-                    const int    oo = __shfl_sync(0xffffffffu, o[u], src);
+                // rows of one pixel in this step: the lowest lane of each group sums
+                // the others' products in lane order, then adds the group's sum
+                // (groups hit distinct pixels, so their adds do not collide)
+                const bool lead = o[u] >= 0 && (__ffs(peers) - 1) == lane;
+                unsigned   rest = lead ? (peers & ~(1u << lane)) : 0u;
+                double     s0 = c0[u], s1 = c1[u], s2 = c2[u];
+                const int  steps = (int) __reduce_max_sync(0xffffffffu, (unsigned) __popc(rest));
+                for (int k = 0; k < steps; k++) {
+                    const int    src = rest ? __ffs(rest) - 1 : lane;
                     const double d0 = __shfl_sync(0xffffffffu, c0[u], src);
                     const double d1 = __shfl_sync(0xffffffffu, c1[u], src);
                     const double d2 = __shfl_sync(0xffffffffu, c2[u], src);
-                    if (lane == 0 && oo >= 0) {
-                        acc[oo] += d0;
-                        acc[oo + 1] += d1;
-                        acc[oo + 2] += d2;
+                    if (rest) {
+                        s0 += d0;
+                        s1 += d1;
+                        s2 += d2;
+                        rest &= rest - 1u;
                     }
+                }
+                if (lead) {
+                    acc[o[u]] += s0;
+                    acc[o[u] + 1] += s1;
+                    acc[o[u] + 2] += s2;
                 }
             }
             __syncwarp();
