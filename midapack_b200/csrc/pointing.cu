@@ -832,7 +832,7 @@ int mdp_build_bins(mdp_context *ctx, mdp_pointing *A, int bin_pix, mdp_pt_bins *
 // warp's sums go to the bin's map entries (a bin of one slice) or to the
 // slice's row of `partial`, summed by pt_partial_sum_kernel.
 template <typename TY, typename TW>
-__global__ void __launch_bounds__(32 * PT_WARPS) trmatvec_slices_kernel(
+__global__ void __launch_bounds__(32 * PT_WARPS, 4) trmatvec_slices_kernel(
         const int32_t *__restrict__ off, const TW *__restrict__ w, const TY *__restrict__ y, double *__restrict__ x,
         const uint32_t *__restrict__ perm, const int32_t *__restrict__ slice_bin, const uint32_t *__restrict__ slice_lo,
         const uint32_t *__restrict__ slice_hi, const int32_t *__restrict__ slice_out, int64_t nslices,
@@ -882,8 +882,17 @@ __global__ void __launch_bounds__(32 * PT_WARPS) trmatvec_slices_kernel(
         }
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            const unsigned peers = __match_any_sync(0xffffffffu, o[u]);
-            const bool     alone = o[u] < 0 || peers == (1u << lane);
+            // distinct pixels for certain when the step's offsets run strictly up
+            // or down the lanes (a scan crossing the bin; the rows past the slice
+            // end, o < 0, are the last lanes and are given keys that continue
+            // either run); otherwise the lanes are grouped by pixel
+            const int  ku = o[u] >= 0 ? o[u] : (1 << 20) + lane, kd = o[u] >= 0 ? o[u] : -1 - lane;
+            const int  nu = __shfl_down_sync(0xffffffffu, ku, 1), nd = __shfl_down_sync(0xffffffffu, kd, 1);
+            const bool up = __all_sync(0xffffffffu, lane == 31 || ku < nu);
+            const bool down = __all_sync(0xffffffffu, lane == 31 || kd > nd);
+            unsigned   peers = 1u << lane;
+            if (!up && !down) peers = __match_any_sync(0xffffffffu, o[u]);
+            const bool alone = o[u] < 0 || peers == (1u << lane);
             if (__all_sync(0xffffffffu, alone)) {
                 if (o[u] >= 0) {  // distinct pixels: one add per entry
                     acc[o[u]] += c0[u];
