@@ -614,11 +614,12 @@ __global__ void trmatvec_general_kernel(const int32_t *__restrict__ local, const
 // (row chunk, bin), bin totals, an exclusive scan over the bins, per-chunk
 // offsets within each bin, then one warp per row chunk writes its rows in
 // order.  Each bin's list is cut into slices of a fixed length (a function of
-// the row count only), and one warp owns one slice: it walks the slice in
-// order, 32 rows a step, and adds each row's three products into its
-// shared-memory copy of the bin's map; rows of one step that hit the same
-// pixel are summed in lane order by the group's lowest lane, which adds the
-// sum.  A bin of one slice is written by that warp;
+// the row and bin counts only), and one warp owns one slice: it walks the
+// slice in order, 32 rows a step, and adds each row's three products into its
+// shared-memory copy of the bin's map.  A step whose offsets run strictly up
+// or down the lanes hits distinct pixels; in any other step the rows that hit
+// the same pixel are summed in lane order by the group's lowest lane, which
+// adds the sum.  A bin of one slice is written by that warp;
 // the slices of a longer bin write partial maps, summed in slice order by one
 // thread per map entry.  The order of every addition is fixed, so the sums
 // are reproducible bit for bit, and no atomic operation touches the map.
